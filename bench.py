@@ -1,0 +1,387 @@
+#!/usr/bin/env python
+"""Throughput of the SH9 lightmap bake on B200 (texel-samples/s).
+
+One step = one BakeSHLightMap pass (BVH build + path tracing + SH9
+projection, the region src/main.cpp:131-136 times) over the whole
+supersampled G-buffer of the workload, inputs resident in HBM.  `e2e` is the
+same metric through the public C ABI from pinned host buffers: scene upload,
+raster, bake, masks, downsample, dilation and the read-back of the final
+lightmap.  The CPU baseline is the oracle restatement on the host cores.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "texel-samples/s on 1 B200 at ≤1% rel. RMSE; batched and adjoint vs plain bake"
+UNIT = "texel-samples/s"
+
+WORKLOADS = {
+    # procedural room: 12-triangle closed room + 200 boxes (2,412 triangles),
+    # lightmap 1024^2, supersample 3, 128 spp, 3 bounces, dilation 2
+    "room": dict(kind="room", width=1024, height=1024, ss=3, spp=128, bounces=3, dilation=2, seed=2),
+    "room_small": dict(kind="room", width=256, height=256, ss=2, spp=32, bounces=3, dilation=2, seed=2),
+    "unit_quad": dict(kind="unit_quad", width=256, height=256, ss=1, spp=64, bounces=3, dilation=0, seed=1),
+}
+
+
+def make_scene(w):
+    from sh_baker_b200 import scenes
+    if w["kind"] == "room":
+        return scenes.procedural_room(seed=w["seed"], res=w["width"])
+    if w["kind"] == "unit_quad":
+        return scenes.unit_quad()
+    raise ValueError(w["kind"])
+
+
+def bytes_per_ray(n_tris: int) -> int:
+    """Algorithmic bytes of one ray: L node fetches of an 80-byte 8-wide
+    node plus one leaf of four 48-byte triangles, L = ceil(log8(ceil(N/4)))."""
+    leaves = max(1, math.ceil(n_tris / 4))
+    L = max(1, math.ceil(math.log(leaves, 8) - 1e-12))
+    return L * 80 + 4 * 48
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    try:
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "200"], stdout=self.file,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.file.flush()
+        rows = [r.split(",") for r in Path(self.file.name).read_text().splitlines() if r.count(",") >= 8]
+        os.unlink(self.file.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_baseline(scene, pts, w, seconds: float, threads: int, rng_seed: int = 1):
+    """The oracle (float, the reference's mt19937 stream) on a seeded random
+    subset of valid texels at full spp, sized to about `seconds` of work."""
+    import numpy as np
+
+    from oracle import pyoracle as O
+    osc = O.OracleScene(scene)
+    valid = np.flatnonzero(pts["material_id"] >= 0)
+    rng = np.random.default_rng(rng_seed)
+    probe = rng.choice(valid, size=min(len(valid), 64), replace=False)
+    t0 = time.perf_counter()
+    r = osc.bake(pts, w["width"], w["height"], w["ss"], samples=w["spp"], bounces=w["bounces"], rng=O.RNG_MT19937,
+                 subset=probe, threads=threads)
+    dt = max(time.perf_counter() - t0, 1e-3)
+    rate = r["texel_samples"] / dt
+    n = int(min(len(valid), max(64, rate * seconds / w["spp"])))
+    sub = rng.choice(valid, size=n, replace=False)
+    t0 = time.perf_counter()
+    r = osc.bake(pts, w["width"], w["height"], w["ss"], samples=w["spp"], bounces=w["bounces"], rng=O.RNG_MT19937,
+                 subset=sub, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": r["texel_samples"] / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} random valid texels of the workload at {w['spp']} spp (oracle restatement, "
+                      f"std::mt19937 stream, {r['rays']} rays, {dt:.1f} s)"}
+
+
+def run_reference(args, w):
+    """CPU arm: the reference algorithm as restated by the oracle (the
+    reference itself cannot be compiled here), all host threads."""
+    import numpy as np
+
+    from oracle import pyoracle as O
+    from sh_baker_b200 import scenes  # noqa: F401
+    scene = make_scene(w)
+    osc = O.OracleScene(scene)
+    pts = osc.rasterize(w["width"], w["height"], w["ss"])
+    threads = os.cpu_count() or 1
+    valid = np.flatnonzero(pts["material_id"] >= 0)
+    rng = np.random.default_rng(7)
+    probe = rng.choice(valid, size=min(len(valid), 64), replace=False)
+    t0 = time.perf_counter()
+    r = osc.bake(pts, w["width"], w["height"], w["ss"], samples=w["spp"], bounces=w["bounces"], rng=O.RNG_MT19937,
+                 subset=probe, threads=threads)
+    rate = r["texel_samples"] / max(time.perf_counter() - t0, 1e-3)
+    n = int(min(len(valid), max(64, rate * args.ref_step_seconds / w["spp"])))
+    times, ts = [], 0
+    for step in range(args.warmup + args.steps):
+        sub = rng.choice(valid, size=n, replace=False)
+        t0 = time.perf_counter()
+        r = osc.bake(pts, w["width"], w["height"], w["ss"], samples=w["spp"], bounces=w["bounces"],
+                     rng=O.RNG_MT19937, subset=sub, threads=threads)
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            times.append(dt)
+            ts += r["texel_samples"]
+    total = sum(times)
+    value = ts / total
+    sample = f"{n} random valid texels per step at {w['spp']} spp (oracle restatement of the reference, mt19937)"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_of(w, scene),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def pinned_scene(scene, pin):
+    """Copy of the scene whose arrays live in pinned (page-locked) memory."""
+    import copy
+
+    import numpy as np
+    import torch
+
+    def p(a, dt):
+        if a is None:
+            return None
+        a = np.ascontiguousarray(a, dtype=dt)
+        out = pin(a.shape, {np.float32: torch.float32, np.uint32: torch.int32, np.uint8: torch.uint8}[dt])
+        out = out.view(dt) if dt == np.uint32 else out
+        out[...] = a
+        return out
+
+    s = copy.deepcopy(scene)
+    for g in s.geometries:
+        g.vertices, g.normals = p(g.vertices, np.float32), p(g.normals, np.float32)
+        g.texture_uvs, g.lightmap_uvs = p(g.texture_uvs, np.float32), p(g.lightmap_uvs, np.float32)
+        g.tangents, g.indices = p(g.tangents, np.float32), p(g.indices, np.uint32)
+    for m in s.materials:
+        m.albedo.pixel_data = p(m.albedo.pixel_data, np.uint8)
+    return s
+
+
+def config_of(w, scene):
+    return {"workload": f"procedural {w['kind']}: {scene.triangle_count} triangles, lightmap {w['width']}x{w['height']}"
+                        f" supersample {w['ss']}, {w['spp']} spp, {w['bounces']} bounces, dilation {w['dilation']}",
+            "triangles": scene.triangle_count, "width": w["width"], "height": w["height"],
+            "supersample_scale": w["ss"], "samples": w["spp"], "bounces": w["bounces"], "dilation": w["dilation"],
+            "l2": "inputs larger than L2: G-buffer %.0f MB + outputs %.0f MB per step" % (
+                w["width"] * w["ss"] * w["height"] * w["ss"] * 64 / 1e6,
+                w["width"] * w["ss"] * w["height"] * w["ss"] * 112 / 1e6)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="room", choices=sorted(WORKLOADS))
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--ref-step-seconds", type=float, default=5.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    w = WORKLOADS[args.workload]
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args, w)
+        return
+
+    import numpy as np
+    import torch
+
+    from sh_baker_b200 import _capi as A
+    from sh_baker_b200 import api
+    from sh_baker_b200 import build as B
+
+    B.build()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    scene = make_scene(w)
+    ctx = api.Context(device=local, profiling=True)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ds = api.DeviceScene(ctx, scene)
+    rc = api.RasterConfig(w["width"], w["height"], w["ss"])
+    g = api.rasterize_to_device(ds, rc)
+    n = g.width * g.height
+    sh = torch.empty(n * 27, dtype=torch.float32, device="cuda")
+    env = torch.empty(n, dtype=torch.float32, device="cuda")
+    out = A.BakeOutput(sh.data_ptr(), env.data_ptr(), 1, 0)
+    lib = ctx.lib
+    import ctypes as C
+
+    def step(i):
+        A.check(lib.shb_scene_rebuild_bvh(ds.h))
+        cfg = api.BakeConfig(samples=w["spp"], bounces=w["bounces"], seed=1000 + 7919 * rank + i).c()
+        st = A.BakeStats()
+        A.check(lib.shb_bake(ds.h, g.h, C.byref(rc.c()), C.byref(cfg), C.byref(out), C.byref(st)))
+        return st
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = ctx.kernel_launches()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    stats = [step(args.warmup + i) for i in range(args.steps)]
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    launches = ctx.kernel_launches() - launches0
+    clk = clocks.stop()
+    ts = sum(s.texel_samples for s in stats)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+        tt = torch.tensor([float(ts)], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt)
+        ts = int(tt.item())
+    value = ts / (ms / 1e3)
+
+    # roofline of the dominant kernel (closest-hit or any-hit traversal)
+    ext_ms = sum(s.extend_kernel_ms for s in stats)
+    sh_ms = sum(s.shadow_kernel_ms for s in stats)
+    ext_rays = sum(s.extend_rays for s in stats)
+    sh_rays = sum(s.shadow_rays for s in stats)
+    bpr = bytes_per_ray(scene.triangle_count)
+    dom = "closest_hit" if ext_ms >= sh_ms else "any_hit"
+    k_ms, k_rays = (ext_ms, ext_rays) if dom == "closest_hit" else (sh_ms, sh_rays)
+    k_launch = sum((s.extend_launches if dom == "closest_hit" else s.shadow_launches) for s in stats)
+    achieved = k_rays * bpr / (k_ms / 1e3) / 1e9 if k_ms > 0 else 0.0
+    peak, peak_kind = measured_peak()
+    traffic = None
+    tp = ROOT / "profiles" / "traversal_traffic.json"
+    if tp.exists():
+        try:
+            tj = json.loads(tp.read_text())
+            per_ray = tj[dom]["dram_bytes_per_ray"]
+            traffic = per_ray * (k_rays / max(k_launch, 1))
+        except Exception:
+            traffic = None
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": dom, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+            "bytes_per_ray": bpr, "rays_per_launch": k_rays / max(k_launch, 1),
+            "launch_ms": k_ms / max(k_launch, 1),
+            "kernel_ms": {"closest_hit": ext_ms / args.steps, "any_hit": sh_ms / args.steps},
+            "rays_per_s": (ext_rays + sh_rays) / (ms / 1e3)}
+
+    # end to end through the public API from pinned host memory
+    e2e = None
+    if not args.no_e2e:
+        from sh_baker_b200.scene import pack_scene
+        H, W = w["height"], w["width"]
+        pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()  # noqa: E731
+        o_sh, o_env, o_mask = pin((H, W, 9, 3), torch.float32), pin((H, W), torch.float32), pin((H, W), torch.uint8)
+        pscene = pinned_scene(scene, pin)
+        desc, keep = pack_scene(pscene)
+        h2d = sum(a.nbytes for a in keep if isinstance(a, np.ndarray))
+        e_times, e_ts = [], 0
+        for i in range(args.warmup + args.steps):
+            ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ea.record(stream)
+            h = C.c_void_p()
+            A.check(lib.shb_scene_upload(ctx.h, C.byref(desc), C.byref(h)))
+            cfg = A.PipelineConfig(W, H, w["ss"], w["spp"], w["bounces"], w["dilation"], 1, 5000 + i)
+            st = A.BakeStats()
+            A.check(lib.shb_bake_pipeline(h, C.byref(cfg), o_sh.ctypes.data, o_env.ctypes.data, o_mask.ctypes.data,
+                                          C.byref(st)))
+            lib.shb_scene_destroy(h)
+            eb.record(stream)
+            torch.cuda.synchronize()
+            if i >= args.warmup:
+                e_times.append(ea.elapsed_time(eb))
+                e_ts += st.texel_samples
+        e_ms = sum(e_times)
+        if dist:
+            t = torch.tensor([e_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_ms = float(t.item())
+            tt = torch.tensor([float(e_ts)], device="cuda", dtype=torch.float64)
+            dist.all_reduce(tt)
+            e_ts = int(tt.item())
+        e2e = {"value": e_ts / (e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(o_sh.nbytes + o_env.nbytes + o_mask.nbytes),
+               "ms_per_step": e_ms / args.steps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        pts = g.download()
+        cpu = cpu_baseline(scene, pts, w, args.cpu_seconds, os.cpu_count() or 1)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_of(w, scene),
+                "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
+                "bvh": ds.bvh_info(), "valid_texels": int(stats[0].valid_texels),
+                "rays_per_texel_sample": (ext_rays + sh_rays) / max(ts, 1)}
+        print(json.dumps(line), flush=True)
+    del sh, env
+    g.close()
+    ds.close()
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

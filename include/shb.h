@@ -1,0 +1,316 @@
+/*
+ * shb.h - C ABI of the B200-native SH9 lightmap bake.
+ *
+ * This is the drop-in boundary for the bake hot path of sh-baker:
+ *   RasterizeScene        (src/rasterizer.h:27-28)   -> shb_rasterize
+ *   CreateValidityMask    (src/rasterizer.h:31-32)   -> shb_validity_mask
+ *   DownsampleValidityMask(src/rasterizer.h:37-39)   -> shb_downsample_validity_mask
+ *   BuildBVH / ReleaseBVH (src/scene.h:128-132)      -> shb_scene_upload / shb_scene_destroy
+ *   FindOcclusion         (src/occlusion.h:27)       -> shb_find_occlusion (batched)
+ *   BakeSHLightMap        (src/baker.h:25-28)        -> shb_bake
+ *   DownsampleSHTexture   (src/baker.h:31)           -> shb_downsample (channels = 27)
+ *   DownsampleEnvironmentVisibilityTexture
+ *                         (src/baker.h:35-36)        -> shb_downsample (channels = 1)
+ *   Dilate<T>             (src/dilation.h:14-16)     -> shb_dilate (kind = SH9 / F32 / U8)
+ *
+ * Plain C types only: host pointers are owned by the caller, device objects
+ * are owned by the opaque handles.  Every entry point returns a shb_status;
+ * shb_last_error() returns a thread-local message for the last failure.
+ * One context owns one CUDA stream; use one context per host thread.
+ *
+ * Memory layouts are binary compatible with the reference's Eigen structs:
+ *   shb_surface_point == sh_baker::SurfacePoint (64 bytes, Vector4f 16-byte
+ *   aligned), an SH texel is 27 floats == sh_baker::SHCoeffs (9 x RGB).
+ */
+#ifndef SHB_H_
+#define SHB_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(_WIN32)
+#define SHB_API __declspec(dllexport)
+#else
+#define SHB_API __attribute__((visibility("default")))
+#endif
+
+#define SHB_ABI_VERSION 1
+
+typedef enum shb_status {
+  SHB_OK = 0,
+  SHB_ERR_INVALID_ARG = 1,
+  SHB_ERR_OOM = 2,
+  SHB_ERR_CUDA = 3,
+  SHB_ERR_TIMEOUT = 4,
+  SHB_ERR_INTERNAL = 5,
+  SHB_ERR_NO_DEVICE = 6
+} shb_status;
+
+/* ---- scene description (mirrors src/scene.h:18-115) -------------------- */
+
+/* Light::Type order of src/scene.h:71. */
+typedef enum shb_light_type {
+  SHB_LIGHT_POINT = 0,
+  SHB_LIGHT_DIRECTIONAL = 1,
+  SHB_LIGHT_SPOT = 2,
+  SHB_LIGHT_AREA = 3
+} shb_light_type;
+
+/* One sh_baker::Geometry (src/scene.h:56-67), structure-of-arrays. */
+typedef struct shb_geometry_desc {
+  const float* vertices;     /* 3 * vertex_count, object space            */
+  const float* normals;      /* 3 * vertex_count or NULL                   */
+  const float* texture_uvs;  /* 2 * vertex_count or NULL                   */
+  const float* lightmap_uvs; /* 2 * vertex_count or NULL (raster needs it) */
+  const float* tangents;     /* 4 * vertex_count (xyz + sign) or NULL      */
+  uint32_t vertex_count;
+  const uint32_t* indices;   /* index_count, triangles                     */
+  uint32_t index_count;
+  int32_t material_id;       /* index into materials, -1 = none            */
+  float transform[12];       /* Affine3f as row-major 3x4 [L | t]          */
+} shb_geometry_desc;
+
+/* One sh_baker::Material (src/scene.h:43-53); only the albedo texture and
+ * the emission intensity are read by the bake (src/material.cpp:57-92). */
+typedef struct shb_material_desc {
+  const uint8_t* albedo_pixels; /* w*h*channels sRGB bytes or NULL        */
+  uint32_t albedo_width;
+  uint32_t albedo_height;
+  uint32_t albedo_channels;     /* 3 or 4 (4 = alpha in A)                */
+  float emission_intensity;
+} shb_material_desc;
+
+/* One sh_baker::Light (src/scene.h:70-87). */
+typedef struct shb_light_desc {
+  int32_t type; /* shb_light_type */
+  float position[3];
+  float direction[3];
+  float color[3];
+  float intensity;
+  float cos_inner_cone;
+  float cos_outer_cone;
+  float area;
+  int32_t material_index; /* area lights: Light::material            */
+  int32_t geometry_index; /* area lights: Light::geometry_index      */
+} shb_light_desc;
+
+typedef struct shb_scene_desc {
+  const shb_geometry_desc* geometries;
+  uint32_t geometry_count;
+  const shb_material_desc* materials;
+  uint32_t material_count;
+  const shb_light_desc* lights;
+  uint32_t light_count;
+} shb_scene_desc;
+
+/* ---- raster / bake types (src/rasterizer.h:12-23, src/baker.h:10-19) ---- */
+
+typedef struct shb_raster_config {
+  int32_t width;
+  int32_t height;
+  int32_t supersample_scale;
+} shb_raster_config;
+
+/* sh_baker::SurfacePoint, 64 bytes, same offsets as the Eigen layout. */
+typedef struct shb_surface_point {
+  float position[3];
+  float normal[3];
+  float _pad0[2];
+  float tangent[4];
+  int32_t material_id; /* invalid if < 0 */
+  int32_t _pad1[3];
+} shb_surface_point;
+
+typedef enum shb_rng_mode {
+  SHB_RNG_PHILOX = 0 /* counter-based Philox4x32-10 stream */
+} shb_rng_mode;
+
+typedef struct shb_bake_config {
+  int32_t samples;           /* BakeConfig::samples (default 128)          */
+  int32_t bounces;           /* BakeConfig::bounces (default 3)            */
+  int32_t num_light_samples; /* BakeConfig::num_light_samples (default 1)  */
+  uint32_t seed;             /* RNG stream id (reference: fixed 12345+idx) */
+  int32_t sample_offset;     /* first sample index (for split bakes)       */
+  int32_t rng_mode;          /* shb_rng_mode                               */
+  int32_t reserved[2];
+} shb_bake_config;
+
+/* Output of shb_bake.  Buffers are W*s x H*s texels (the supersampled size,
+ * as BakeSHLightMap returns, src/baker.cpp:198-216).  sh: 27 floats per
+ * texel (coeff-major RGB), env_visibility: 1 float per texel.  With
+ * device_ptrs != 0 both pointers are CUDA device pointers on the context's
+ * device, else host pointers. */
+typedef struct shb_bake_output {
+  float* sh;
+  float* env_visibility;
+  int32_t device_ptrs;
+  int32_t reserved;
+} shb_bake_output;
+
+/* Ray / hit of FindOcclusion (src/occlusion.h:11-23). */
+typedef struct shb_ray {
+  float origin[3];
+  float direction[3];
+  float tnear;
+  float tfar;
+} shb_ray;
+
+typedef struct shb_hit {
+  float position[3];
+  float uv[2];
+  float normal[3];
+  int32_t material_id;
+  int32_t hit;          /* 0 = miss (nullopt) */
+  float t;
+  uint32_t prim_id;     /* global triangle id (geometry-major order) */
+} shb_hit;
+
+/* Per-bake counters filled by shb_bake when stats != NULL. */
+typedef struct shb_bake_stats {
+  uint64_t texel_samples;  /* valid texels x samples                      */
+  uint64_t valid_texels;
+  uint64_t extend_rays;    /* closest-hit rays traced                     */
+  uint64_t shadow_rays;    /* any-hit rays traced                         */
+  uint64_t kernel_launches;
+  uint32_t error_flags;    /* device-side bounded-failure flags (0 = ok)  */
+  uint32_t waves;
+  double bvh_build_ms;     /* filled when profiling is on                 */
+  double trace_ms;
+  double extend_kernel_ms; /* sum of closest-hit kernel durations         */
+  double shadow_kernel_ms;
+  double shade_kernel_ms;
+  uint64_t extend_launches;
+  uint64_t shadow_launches;
+} shb_bake_stats;
+
+typedef enum shb_dilate_kind {
+  SHB_DILATE_SH9 = 0, /* 27 floats per texel (Dilate<SHCoeffs>) */
+  SHB_DILATE_F32 = 1, /* 1 float per texel    (Dilate<float>)    */
+  SHB_DILATE_U8 = 2   /* 1 byte per texel     (Dilate<uint8_t>)  */
+} shb_dilate_kind;
+
+typedef struct shb_options {
+  int32_t device;      /* CUDA device ordinal                          */
+  int32_t profiling;   /* 1: time kernel classes with CUDA events      */
+  int32_t reserved[6];
+} shb_options;
+
+typedef struct shb_context shb_context;
+typedef struct shb_scene shb_scene;
+typedef struct shb_gbuffer shb_gbuffer;
+
+/* ---- lifetime --------------------------------------------------------- */
+
+SHB_API int32_t shb_abi_version(void);
+SHB_API const char* shb_last_error(void);
+SHB_API shb_status shb_context_create(const shb_options* options,
+                                      shb_context** out);
+SHB_API shb_status shb_context_destroy(shb_context* ctx);
+/* Replaces the context's stream with a caller-owned cudaStream_t (or 0 for
+ * the context's own stream). */
+SHB_API shb_status shb_context_set_stream(shb_context* ctx, void* stream);
+SHB_API shb_status shb_context_synchronize(shb_context* ctx);
+/* Number of kernels this context has launched so far. */
+SHB_API uint64_t shb_context_kernel_launches(const shb_context* ctx);
+
+/* Uploads the scene and builds the GPU BVH (binned SAH, compressed 8-wide
+ * nodes).  Replaces BuildBVH (src/scene.cpp:209-262); the reference builds
+ * it inside every BakeSHLightMap call (src/baker.cpp:258-259). */
+SHB_API shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* desc,
+                                    shb_scene** out);
+SHB_API shb_status shb_scene_destroy(shb_scene* scene);
+/* Rebuilds the BVH of an uploaded scene (times the builder alone). */
+SHB_API shb_status shb_scene_rebuild_bvh(shb_scene* scene);
+SHB_API shb_status shb_scene_bvh_info(const shb_scene* scene, uint32_t* wide_nodes,
+                                      uint32_t* triangles, uint32_t* depth);
+
+/* ---- RasterizeScene (src/rasterizer.cpp:68-211) ----------------------- */
+
+/* Rasterises every triangle's lightmap UVs into a (W*s) x (H*s) texel
+ * G-buffer.  host_out (nullable) receives W*s*H*s surface points;
+ * out_gbuffer (nullable) receives the device-resident G-buffer handle. */
+SHB_API shb_status shb_rasterize(shb_scene* scene, const shb_raster_config* cfg,
+                                 shb_surface_point* host_out,
+                                 shb_gbuffer** out_gbuffer);
+/* Device G-buffer from caller surface points (BakeSHLightMap takes them as
+ * an argument, src/baker.h:25-28).  width/height are the texel dims. */
+SHB_API shb_status shb_gbuffer_upload(shb_context* ctx, const shb_surface_point* points,
+                                      int32_t width, int32_t height,
+                                      shb_gbuffer** out);
+SHB_API shb_status shb_gbuffer_download(const shb_gbuffer* g, shb_surface_point* points);
+SHB_API shb_status shb_gbuffer_dims(const shb_gbuffer* g, int32_t* width, int32_t* height);
+SHB_API shb_status shb_gbuffer_destroy(shb_gbuffer* g);
+
+/* ---- CreateValidityMask / DownsampleValidityMask ---------------------- */
+
+/* mask_out: width*height bytes (device pointer if device_ptr != 0). */
+SHB_API shb_status shb_validity_mask(shb_context* ctx, const shb_gbuffer* g,
+                                     uint8_t* mask_out, int32_t device_ptr);
+/* src/rasterizer.cpp:222-241: out[y*w+x] = any(in block).  in: (w*s)x(h*s). */
+SHB_API shb_status shb_downsample_validity_mask(shb_context* ctx, const uint8_t* in,
+                                                int32_t width, int32_t height,
+                                                int32_t scale, uint8_t* out,
+                                                int32_t device_ptrs);
+
+/* ---- BakeSHLightMap (src/baker.cpp:186-304) --------------------------- */
+
+/* raster_cfg gives the base size and supersample scale of the G-buffer, as
+ * in the reference; the G-buffer must be (W*s) x (H*s). */
+SHB_API shb_status shb_bake(shb_scene* scene, const shb_gbuffer* g,
+                            const shb_raster_config* raster_cfg,
+                            const shb_bake_config* cfg, shb_bake_output* out,
+                            shb_bake_stats* stats);
+
+/* ---- DownsampleTexture (src/baker.cpp:151-182) ------------------------ */
+
+/* Box average over scale x scale blocks including invalid texels; channels
+ * = 27 for SH, 1 for env visibility.  out: (in_w/scale) x (in_h/scale). */
+SHB_API shb_status shb_downsample(shb_context* ctx, const float* in, int32_t in_width,
+                                  int32_t in_height, int32_t channels, int32_t scale,
+                                  float* out, int32_t device_ptrs);
+
+/* ---- Dilate<T> (src/dilation.cpp:7-73) -------------------------------- */
+
+/* pixels and mask are updated in place, like the reference. */
+SHB_API shb_status shb_dilate(shb_context* ctx, int32_t kind, int32_t width,
+                              int32_t height, void* pixels, uint8_t* mask,
+                              int32_t passes, int32_t device_ptrs);
+
+/* ---- the CLI's bake sequence (src/main.cpp:91-163) -------------------- */
+
+typedef struct shb_pipeline_config {
+  int32_t width;             /* --width  */
+  int32_t height;            /* --height */
+  int32_t supersample_scale; /* --supersample_scale */
+  int32_t samples;           /* --samples */
+  int32_t bounces;           /* --bounces */
+  int32_t dilation;          /* --dilation (passes) */
+  int32_t num_light_samples;
+  uint32_t seed;
+} shb_pipeline_config;
+
+/* RasterizeScene -> BakeSHLightMap -> CreateValidityMask -> (s > 1)
+ * DownsampleSHTexture / DownsampleEnvironmentVisibilityTexture /
+ * DownsampleValidityMask -> (dilation > 0) Dilate(SH) then Dilate(env) with
+ * the mask the first Dilate already updated, all on the device.  Host
+ * outputs at width x height: sh (27 floats per texel), env_visibility,
+ * mask (nullable). */
+SHB_API shb_status shb_bake_pipeline(shb_scene* scene, const shb_pipeline_config* cfg,
+                                     float* sh_out, float* env_out, uint8_t* mask_out,
+                                     shb_bake_stats* stats);
+
+/* ---- FindOcclusion (src/occlusion.cpp:9-107), batched ----------------- */
+
+SHB_API shb_status shb_find_occlusion(shb_scene* scene, const shb_ray* rays,
+                                      int64_t count, shb_hit* hits,
+                                      int32_t device_ptrs);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* SHB_H_ */

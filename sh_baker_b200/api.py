@@ -1,0 +1,327 @@
+"""Host-side mirror of sh_baker's bake API over the C ABI.
+
+Names, argument meaning and return values follow the reference:
+RasterizeScene (src/rasterizer.h:27-28), CreateValidityMask /
+DownsampleValidityMask (src/rasterizer.h:31-39), BakeSHLightMap
+(src/baker.h:25-28), DownsampleSHTexture /
+DownsampleEnvironmentVisibilityTexture (src/baker.h:31-36), Dilate
+(src/dilation.h:14-16) and FindOcclusion (src/occlusion.h:27).  Where the
+reference aborts (CHECK) these raise ShbError.  All compute runs in
+libshb.so on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+from typing import Optional
+
+import numpy as np
+
+from . import _capi as A
+from .scene import SURFACE_POINT_DTYPE, Scene, pack_scene
+
+
+@dataclass
+class RasterConfig:
+    width: int = 1024
+    height: int = 1024
+    supersample_scale: int = 1
+
+    def c(self) -> A.RasterConfig:
+        return A.RasterConfig(self.width, self.height, self.supersample_scale)
+
+
+@dataclass
+class BakeConfig:
+    samples: int = 128
+    bounces: int = 3
+    num_light_samples: int = 1
+    seed: int = 12345
+    sample_offset: int = 0
+
+    def c(self) -> A.BakeConfig:
+        cfg = A.BakeConfig()
+        cfg.samples = self.samples
+        cfg.bounces = self.bounces
+        cfg.num_light_samples = self.num_light_samples
+        cfg.seed = self.seed & 0xFFFFFFFF
+        cfg.sample_offset = self.sample_offset
+        cfg.rng_mode = A.RNG_PHILOX
+        return cfg
+
+
+@dataclass
+class BakeResult:
+    """sh_texture: (H*s, W*s, 9, 3) float32; environment_visibility_texture:
+    (H*s, W*s) float32 (src/baker.h:16-19)."""
+    sh_texture: np.ndarray
+    environment_visibility_texture: np.ndarray
+    stats: Optional[A.BakeStats] = None
+
+
+class Context:
+    """One CUDA stream on one device (shb_context)."""
+
+    def __init__(self, device: int = 0, profiling: bool = False):
+        self.lib = A.load()
+        opts = A.Options()
+        opts.device = device
+        opts.profiling = int(profiling)
+        h = C.c_void_p()
+        A.check(self.lib.shb_context_create(C.byref(opts), C.byref(h)))
+        self.h = h
+
+    def kernel_launches(self) -> int:
+        return int(self.lib.shb_context_kernel_launches(self.h))
+
+    def set_stream(self, stream_ptr: int) -> None:
+        A.check(self.lib.shb_context_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    def synchronize(self) -> None:
+        A.check(self.lib.shb_context_synchronize(self.h))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.shb_context_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DeviceScene:
+    """An uploaded scene with its GPU BVH (shb_scene)."""
+
+    def __init__(self, ctx: Context, scene: Scene):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        desc, keep = pack_scene(scene)
+        h = C.c_void_p()
+        A.check(self.lib.shb_scene_upload(ctx.h, C.byref(desc), C.byref(h)))
+        self.h = h
+
+    def bvh_info(self):
+        n, t, d = C.c_uint32(), C.c_uint32(), C.c_uint32()
+        A.check(self.lib.shb_scene_bvh_info(self.h, C.byref(n), C.byref(t), C.byref(d)))
+        return {"wide_nodes": n.value, "triangles": t.value, "depth": d.value}
+
+    def rebuild_bvh(self) -> None:
+        A.check(self.lib.shb_scene_rebuild_bvh(self.h))
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.shb_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class GBuffer:
+    """Device-resident texel G-buffer (shb_gbuffer)."""
+
+    def __init__(self, ctx: Context, handle: C.c_void_p):
+        self.ctx = ctx
+        self.lib = ctx.lib
+        self.h = handle
+        w, hh = C.c_int32(), C.c_int32()
+        A.check(self.lib.shb_gbuffer_dims(handle, C.byref(w), C.byref(hh)))
+        self.width, self.height = w.value, hh.value
+
+    @staticmethod
+    def from_points(ctx: Context, points: np.ndarray, width: int, height: int) -> "GBuffer":
+        pts = np.ascontiguousarray(points, dtype=SURFACE_POINT_DTYPE)
+        if pts.size != width * height:
+            raise ValueError("points size must be width*height")
+        h = C.c_void_p()
+        A.check(ctx.lib.shb_gbuffer_upload(ctx.h, pts.ctypes.data, width, height, C.byref(h)))
+        return GBuffer(ctx, h)
+
+    def download(self) -> np.ndarray:
+        out = np.empty(self.width * self.height, dtype=SURFACE_POINT_DTYPE)
+        A.check(self.lib.shb_gbuffer_download(self.h, out.ctypes.data))
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.shb_gbuffer_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default: Optional[Context] = None
+
+
+def default_context() -> Context:
+    global _default
+    if _default is None:
+        _default = Context()
+    return _default
+
+
+def _scene_handle(scene, ctx: Context) -> DeviceScene:
+    return scene if isinstance(scene, DeviceScene) else DeviceScene(ctx, scene)
+
+
+# ------------------------------------------------------ reference-named API --
+
+def RasterizeScene(scene, config: RasterConfig, ctx: Optional[Context] = None) -> np.ndarray:
+    """src/rasterizer.cpp:68-211.  Returns (W*s)*(H*s) surface points."""
+    ctx = ctx or default_context()
+    ds = _scene_handle(scene, ctx)
+    n = config.width * config.supersample_scale * config.height * config.supersample_scale
+    out = np.empty(n, dtype=SURFACE_POINT_DTYPE)
+    A.check(ctx.lib.shb_rasterize(ds.h, C.byref(config.c()), out.ctypes.data, None))
+    return out
+
+
+def rasterize_to_device(ds: DeviceScene, config: RasterConfig) -> GBuffer:
+    h = C.c_void_p()
+    A.check(ds.lib.shb_rasterize(ds.h, C.byref(config.c()), None, C.byref(h)))
+    return GBuffer(ds.ctx, h)
+
+
+def CreateValidityMask(points: np.ndarray, ctx: Optional[Context] = None) -> np.ndarray:
+    """src/rasterizer.cpp:213-220."""
+    ctx = ctx or default_context()
+    g = GBuffer.from_points(ctx, points, len(points), 1)
+    out = np.empty(len(points), np.uint8)
+    A.check(ctx.lib.shb_validity_mask(ctx.h, g.h, out.ctypes.data, 0))
+    return out
+
+
+def DownsampleValidityMask(high_res_mask: np.ndarray, width: int, height: int, scale: int,
+                           ctx: Optional[Context] = None) -> np.ndarray:
+    """src/rasterizer.cpp:222-241."""
+    ctx = ctx or default_context()
+    m = np.ascontiguousarray(high_res_mask, dtype=np.uint8).reshape(-1)
+    if m.size != width * height * scale * scale:
+        raise A.ShbError(1, "high_res_mask size != width*height*scale*scale")
+    out = np.empty(width * height, np.uint8)
+    A.check(ctx.lib.shb_downsample_validity_mask(ctx.h, m.ctypes.data, width, height, scale, out.ctypes.data, 0))
+    return out
+
+
+def BakeSHLightMap(scene, surface_points, raster_config: RasterConfig, config: BakeConfig,
+                   ctx: Optional[Context] = None, with_stats: bool = False) -> BakeResult:
+    """src/baker.cpp:186-304 on the GPU.  surface_points: numpy array of
+    SURFACE_POINT_DTYPE or a GBuffer."""
+    ctx = ctx or default_context()
+    ds = _scene_handle(scene, ctx)
+    W = raster_config.width * raster_config.supersample_scale
+    H = raster_config.height * raster_config.supersample_scale
+    g = surface_points if isinstance(surface_points, GBuffer) else GBuffer.from_points(ctx, surface_points, W, H)
+    sh = np.empty((H, W, 9, 3), np.float32)
+    env = np.empty((H, W), np.float32)
+    out = A.BakeOutput(sh.ctypes.data, env.ctypes.data, 0, 0)
+    st = A.BakeStats()
+    A.check(ctx.lib.shb_bake(ds.h, g.h, C.byref(raster_config.c()), C.byref(config.c()), C.byref(out), C.byref(st)))
+    return BakeResult(sh, env, st if with_stats else None)
+
+
+def _downsample(x: np.ndarray, w: int, h: int, ch: int, scale: int, ctx: Context) -> np.ndarray:
+    x = np.ascontiguousarray(x, np.float32)
+    ow, oh = (w, h) if scale <= 1 else (w // scale, h // scale)
+    out = np.empty(ow * oh * ch, np.float32)
+    A.check(ctx.lib.shb_downsample(ctx.h, x.ctypes.data, w, h, ch, scale, out.ctypes.data, 0))
+    return out
+
+
+def DownsampleSHTexture(sh_texture: np.ndarray, scale: int, ctx: Optional[Context] = None) -> np.ndarray:
+    """src/baker.cpp:306-313: (H, W, 9, 3) -> (H/s, W/s, 9, 3)."""
+    ctx = ctx or default_context()
+    h, w = sh_texture.shape[:2]
+    out = _downsample(sh_texture, w, h, 27, scale, ctx)
+    return out.reshape((h if scale <= 1 else h // scale), (w if scale <= 1 else w // scale), 9, 3)
+
+
+def DownsampleEnvironmentVisibilityTexture(env: np.ndarray, scale: int, ctx: Optional[Context] = None) -> np.ndarray:
+    """src/baker.cpp:315-323."""
+    ctx = ctx or default_context()
+    h, w = env.shape[:2]
+    out = _downsample(env, w, h, 1, scale, ctx)
+    return out.reshape((h if scale <= 1 else h // scale), (w if scale <= 1 else w // scale))
+
+
+def Dilate(width: int, height: int, pixels: np.ndarray, mask: np.ndarray, passes: int = 1,
+           ctx: Optional[Context] = None) -> None:
+    """src/dilation.cpp:7-73; pixels and mask are updated in place.  The
+    element type follows the reference's instantiations: 27 floats per texel
+    (SHCoeffs), float32, or uint8."""
+    ctx = ctx or default_context()
+    if pixels.size == 0 or mask.size == 0:
+        return
+    n = width * height
+    if mask.dtype != np.uint8 or not mask.flags.c_contiguous or not pixels.flags.c_contiguous:
+        raise TypeError("pixels and mask must be C-contiguous; mask uint8")
+    if pixels.dtype == np.uint8:
+        kind = A.DILATE_U8
+    elif pixels.dtype == np.float32 and pixels.size == 27 * n:
+        kind = A.DILATE_SH9
+    elif pixels.dtype == np.float32 and pixels.size == n:
+        kind = A.DILATE_F32
+    else:
+        raise TypeError("unsupported pixel layout")
+    if mask.size != n or (kind == A.DILATE_U8 and pixels.size != n):
+        return  # the reference returns when sizes disagree
+    A.check(ctx.lib.shb_dilate(ctx.h, kind, width, height, pixels.ctypes.data, mask.ctypes.data, passes, 0))
+
+
+@dataclass
+class LightmapResult:
+    """Final lightmap at width x height: sh (H, W, 9, 3), env (H, W), mask."""
+    sh: np.ndarray
+    env: np.ndarray
+    mask: np.ndarray
+    stats: A.BakeStats
+
+
+def bake_lightmap(scene, width: int, height: int, samples: int = 128, bounces: int = 3, supersample_scale: int = 1,
+                  dilation: int = 16, seed: int = 12345, num_light_samples: int = 1,
+                  ctx: Optional[Context] = None, out: Optional[tuple] = None) -> LightmapResult:
+    """The sh_baker CLI's sequence (src/main.cpp:91-163) in one device
+    pipeline: raster, bake, validity mask, downsample, dilation.  `out` may
+    supply (sh, env, mask) host arrays (for example pinned memory)."""
+    ctx = ctx or default_context()
+    ds = _scene_handle(scene, ctx)
+    cfg = A.PipelineConfig(width, height, supersample_scale, samples, bounces, dilation, num_light_samples,
+                           seed & 0xFFFFFFFF)
+    if out is None:
+        out = (np.empty((height, width, 9, 3), np.float32), np.empty((height, width), np.float32),
+               np.empty((height, width), np.uint8))
+    sh, env, mask = out
+    st = A.BakeStats()
+    A.check(ctx.lib.shb_bake_pipeline(ds.h, C.byref(cfg), sh.ctypes.data, env.ctypes.data, mask.ctypes.data,
+                                      C.byref(st)))
+    return LightmapResult(sh, env, mask, st)
+
+
+def FindOcclusion(scene, rays: np.ndarray, ctx: Optional[Context] = None):
+    """Batched src/occlusion.cpp:9-107.  rays: (N, 8) float32 rows of
+    origin(3), direction(3), tnear, tfar.  Returns a structured hit array."""
+    ctx = ctx or default_context()
+    ds = _scene_handle(scene, ctx)
+    r = np.ascontiguousarray(rays, np.float32).reshape(-1, 8)
+    hits = (A.Hit * max(1, len(r)))()
+    A.check(ctx.lib.shb_find_occlusion(ds.h, r.ctypes.data, len(r), C.addressof(hits), 0))
+    return hits_to_numpy(hits, len(r))
+
+
+HIT_DTYPE = np.dtype([("position", "<f4", 3), ("uv", "<f4", 2), ("normal", "<f4", 3), ("material_id", "<i4"),
+                      ("hit", "<i4"), ("t", "<f4"), ("prim_id", "<u4")])
+
+
+def hits_to_numpy(hits, n: int) -> np.ndarray:
+    buf = (C.c_char * (C.sizeof(A.Hit) * n)).from_address(C.addressof(hits))
+    return np.frombuffer(bytes(buf), dtype=HIT_DTYPE, count=n).copy()

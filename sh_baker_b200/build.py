@@ -1,0 +1,66 @@
+"""Builds libshb.so (the CUDA bake library) in-tree with nvcc for sm_100a.
+
+Files whose arithmetic must round exactly like the CPU restatement of the
+reference are compiled with -fmad=false; the traversal and BVH builder keep
+FMA contraction (their exact steps use explicit rounding intrinsics).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+CSRC = PKG / "csrc"
+BUILD = PKG / "_build"
+LIB = PKG / "libshb.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+          "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr", "-Xptxas", "-warn-spills"]
+SOURCES = {
+    "shb_capi.cu": ["-fmad=false"],
+    "raster.cu": ["-fmad=false"],
+    "shade.cu": ["-fmad=false"],
+    "traverse.cu": ["-fmad=true"],
+    "bvh_build.cu": ["-fmad=true"],
+}
+HEADERS = ["shb_internal.h", "shb_math.cuh", "wavefront.h"]
+
+
+def nvcc() -> str:
+    cand = os.environ.get("NVCC") or "/usr/local/cuda/bin/nvcc"
+    return cand if Path(cand).exists() else "nvcc"
+
+
+def _newer(out: Path, deps) -> bool:
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def build(verbose: bool = False, force: bool = False) -> Path:
+    BUILD.mkdir(exist_ok=True)
+    headers = [CSRC / h for h in HEADERS] + [PKG.parent / "include" / "shb.h"]
+    objs = []
+    for src, flags in SOURCES.items():
+        s = CSRC / src
+        o = BUILD / (src + ".o")
+        objs.append(o)
+        if force or _newer(o, [s, *headers, Path(__file__)]):
+            cmd = [nvcc(), *ARCH, *COMMON, *flags, "-c", str(s), "-o", str(o)]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
+    if force or _newer(LIB, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-Xlinker", "--no-undefined"]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True, force="--force" in sys.argv)

@@ -1,0 +1,790 @@
+// shade.cu - wavefront stages of BakeSHLightMap (src/baker.cpp:186-304):
+//   generate  one path per (texel, sample): uniform-hemisphere primary ray
+//             and texel-level next-event estimation (src/light.cpp:191-293)
+//   shade     per closest hit: alpha, emission, NEE with BRDF
+//             (src/light.cpp:82-189), cosine BSDF sample (material.cpp:113-162)
+//   resolve   one warp per texel: SH9 projection of every sample in
+//             registers, warp-shuffle reduction, one coalesced store
+// plus the host loop that drives the waves.  Compiled with -fmad=false so
+// the arithmetic rounds like the CPU restatement.
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
+
+#include <chrono>
+
+#include "shb_math.cuh"
+#include "wavefront.h"
+
+namespace shb {
+
+__constant__ float c_srgb[256];
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr double kTwoPiD = 6.283185307179586;
+
+struct MatInfo {
+  f3 albedo_over_pi;
+  float alpha;
+  f3 emission;
+};
+
+__device__ __forceinline__ DMat load_mat(const SceneView& sc, int id) {
+  if (id < 0 || (uint32_t)id >= sc.mat_count) {
+    DMat d;
+    d.pix_offset = 0;
+    d.w = d.h = d.c = 0;
+    d.emission = 0.f;
+    d.use_override = 0;
+    d.override_rgb[0] = d.override_rgb[1] = d.override_rgb[2] = 0.f;
+    d.pad = 0.f;
+    return d;
+  }
+  return sc.mats[id];
+}
+
+__device__ __forceinline__ int tex_index(const DMat& m, f2 uv) {
+  int tx = min(max(cvt_trunc(uv.x * (float)m.w), 0), (int)m.w - 1);
+  int ty = min(max(cvt_trunc(uv.y * (float)m.h), 0), (int)m.h - 1);
+  return (ty * (int)m.w + tx) * (int)m.c;
+}
+
+// src/material.cpp:69-85
+__device__ __forceinline__ f3 get_albedo(const SceneView& sc, const DMat& m, f2 uv) {
+  if (m.use_override) return {m.override_rgb[0], m.override_rgb[1], m.override_rgb[2]};
+  if (m.c == 0) return {0.8f, 0.8f, 0.8f};
+  const uint8_t* px = sc.pixels + m.pix_offset + tex_index(m, uv);
+  return {c_srgb[px[0]], c_srgb[px[1]], c_srgb[px[2]]};
+}
+// src/material.cpp:57-67
+__device__ __forceinline__ float get_alpha(const SceneView& sc, const DMat& m, f2 uv) {
+  if (m.c < 4) return 1.0f;
+  const uint8_t* px = sc.pixels + m.pix_offset + tex_index(m, uv);
+  return (float)px[3] / 255.0f;
+}
+// src/material.cpp:87-92
+__device__ __forceinline__ f3 get_emission(const SceneView& sc, const DMat& m, f2 uv) {
+  if (m.emission > 0.0f) return get_albedo(sc, m, uv) * m.emission;
+  return {0.f, 0.f, 0.f};
+}
+
+// std::max(a.x, std::max(a.y, a.z)) with std::max(a, b) = a < b ? b : a.
+__device__ __forceinline__ float max_coeff_std(f3 a) {
+  float m = a.y < a.z ? a.z : a.y;
+  return a.x < m ? m : a.x;
+}
+
+// src/light.cpp:16-78; uniforms ubase (triangle), ubase+1, ubase+2.
+__device__ void sample_area(const SceneView& sc, const DLight& L, Event& ev, int ubase, f3& point, f3& rad,
+                            float& pdf) {
+  point = {0.f, 0.f, 0.f};
+  rad = {0.f, 0.f, 0.f};
+  pdf = 0.f;
+  if (L.geom < 0 || L.mat < 0) return;
+  DGeom g = sc.geoms[L.geom];
+  uint32_t n = g.tri_count;
+  if (n == 0) return;
+  uint32_t tri = ev.tri(ubase, n);
+  uint32_t p = g.prim_base + tri;
+  uint32_t i0 = sc.tri_vidx[3 * p], i1 = sc.tri_vidx[3 * p + 1], i2 = sc.tri_vidx[3 * p + 2];
+  float u1 = ev.u(ubase + 1);
+  float u2 = ev.u(ubase + 2);
+  if (u1 + u2 > 1.0f) {
+    u1 = 1.0f - u1;
+    u2 = 1.0f - u2;
+  }
+  float w = 1.0f - u1 - u2;
+  f3 v0 = ld3(sc.obj_v, i0), v1 = ld3(sc.obj_v, i1), v2 = ld3(sc.obj_v, i2);
+  point = w * v0 + u1 * v1 + u2 * v2;
+  f2 uv = {0.f, 0.f};
+  if (g.flags & GEOM_HAS_TEXUV) uv = w * ld2(sc.tex_uv, i0) + u1 * ld2(sc.tex_uv, i1) + u2 * ld2(sc.tex_uv, i2);
+  rad = get_emission(sc, load_mat(sc, L.mat), uv);
+  float area = sqrtf(sqnorm(cross(v0 - v1, v0 - v2))) / 2.f;
+  float x = 1.f / (float)n * 1.f / area;
+  pdf = 1e-6f < x ? x : 1e-6f;
+}
+
+struct LightEval {
+  f3 rad;
+  f3 ray_d;
+  float tfar;
+  float apdf;
+  float w;
+};
+
+// Incoming radiance without visibility (src/light.h:34-49,72-95,117-144,
+// 166-188); with HIT, times cos x BRDF (src/light.h:51-203).
+template <bool HIT>
+__device__ LightEval eval_light(const SceneView& sc, uint32_t li, f3 P, f3 N, Event& ev, f3 wo, f3 aop) {
+  DLight L = sc.lights[li];
+  LightEval e;
+  e.apdf = 1.0f;
+  f3 color = {L.cr, L.cg, L.cb};
+  float cos_n;
+  f3 incident;
+  if (L.type == SHB_LIGHT_DIRECTIONAL) {
+    f3 dir = {L.dx, L.dy, L.dz};
+    e.ray_d = -dir;
+    e.tfar = 1.0e10f;
+    cos_n = dot(N, -dir);
+    incident = -dir;
+    e.rad = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : L.intensity * color;
+  } else if (L.type == SHB_LIGHT_POINT || L.type == SHB_LIGHT_SPOT || L.type == SHB_LIGHT_AREA) {
+    f3 target, arad = {0.f, 0.f, 0.f};
+    if (L.type == SHB_LIGHT_AREA) sample_area(sc, L, ev, 3 * L.area_ord, target, arad, e.apdf);
+    else target = {L.px, L.py, L.pz};
+    f3 Lv = target - P;
+    float dist_sq = sqnorm(Lv);
+    float dist = sqrtf(dist_sq);
+    e.ray_d = target - P;
+    e.tfar = dist - 0.001f;
+    Lv = Lv / dist;
+    incident = Lv;
+    cos_n = dot(N, Lv);
+    if (L.type == SHB_LIGHT_POINT) {
+      e.rad = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : L.intensity * color / (dist * dist);
+    } else if (L.type == SHB_LIGHT_SPOT) {
+      float cos_l = dot(f3{L.dx, L.dy, L.dz}, -Lv);
+      float falloff = (cos_l - L.cos_outer) / (L.cos_inner - L.cos_outer);
+      falloff = fminf(fmaxf(falloff, 0.0f), 1.0f);
+      e.rad = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : L.intensity * color / (dist * dist) * falloff;
+    } else {
+      e.rad = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : arad / (dist * dist);
+    }
+  } else {
+    e.rad = {0.f, 0.f, 0.f};
+    e.ray_d = {0.f, 0.f, 1.f};
+    e.tfar = 0.f;
+    cos_n = -1.f;
+    incident = {0.f, 0.f, 1.f};
+  }
+  if (HIT) {
+    if (cos_n < 0.f) {
+      e.rad = {0.f, 0.f, 0.f};
+    } else {
+      bool zero = dot(N, wo) <= 0.0f || dot(N, incident) <= 0.0f;
+      f3 brdf = zero ? f3{0.f, 0.f, 0.f} : aop;
+      e.rad = cmul(e.rad, cos_n * brdf);
+    }
+  }
+  e.w = max_coeff_std(e.rad);
+  return e;
+}
+
+// One light pick of the discrete distribution over weights (the counter
+// stream's uniform `u` against the running float sum; zero-weight lights
+// are never picked).
+template <bool HIT>
+__device__ bool pick_light(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3 aop, float sum, float u,
+                           LightEval& out) {
+  float target = u * sum;
+  float cum = 0.f;
+  int last = -1;
+  for (uint32_t i = 0; i < sc.light_count; ++i) {
+    LightEval e = eval_light<HIT>(sc, i, P, N, ev, wo, aop);
+    cum += e.w;
+    if (e.w > 0.f) last = (int)i;
+    if (target < cum) {
+      out = e;
+      return true;
+    }
+  }
+  if (last < 0) return false;
+  out = eval_light<HIT>(sc, (uint32_t)last, P, N, ev, wo, aop);
+  return true;
+}
+
+template <bool HIT>
+__device__ float light_weight_sum(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3 aop) {
+  float sum = 0.0f;
+  for (uint32_t i = 0; i < sc.light_count; ++i) sum += eval_light<HIT>(sc, i, P, N, ev, wo, aop).w;
+  return sum;
+}
+
+// Warp-aggregated queue slot: every lane of the warp must call this.
+__device__ __forceinline__ int warp_push(int* counter, bool pred) {
+  unsigned b = __ballot_sync(0xFFFFFFFFu, pred);
+  if (b == 0) return -1;
+  int lane = threadIdx.x & 31;
+  int leader = __ffs(b) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(counter, __popc(b));
+  base = __shfl_sync(0xFFFFFFFFu, base, leader);
+  return pred ? base + __popc(b & ((1u << lane) - 1u)) : -1;
+}
+
+struct SP {
+  f3 pos, nrm, tan;
+  float tw;
+  int mat;
+};
+__device__ __forceinline__ SP load_sp(const shb_surface_point* pts, uint32_t texel) {
+  const float4* q = reinterpret_cast<const float4*>(pts + texel);
+  float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+  SP s;
+  s.pos = {a.x, a.y, a.z};
+  s.nrm = {a.w, b.x, b.y};
+  s.tan = {c.x, c.y, c.z};
+  s.tw = c.w;
+  s.mat = __float_as_int(d.x);
+  return s;
+}
+
+// src/baker.cpp:38-46,266-271
+__device__ __forceinline__ f3 primary_dir(const SP& sp, uint32_t seed, uint32_t texel, uint32_t sample) {
+  Event e;
+  e.init(seed, texel, sample, 0, EV_HEMI);
+  float u1 = e.u(0), u2 = e.u(1);
+  float r = sqrtf(1.0f - u1 * u1);
+  float phi = (float)(kTwoPiD * (double)u2);
+  f3 dl = {r * cosf(phi), r * sinf(phi), u1};
+  f3 bit = cross(sp.nrm, sp.tan) * sp.tw;
+  return sp.tan * dl.x + bit * dl.y + sp.nrm * dl.z;
+}
+
+struct WaveArgs {
+  SceneView sc;
+  const shb_surface_point* pts;
+  const uint32_t* valid;
+  uint32_t t0;       // first valid-texel slot of the wave
+  uint32_t n_tex;    // texels in the wave
+  uint32_t spp;
+  uint32_t seed;
+  uint32_t sample_offset;
+  int nls;
+  int bounces;
+  ExtQueue ext[2];
+  float4* hits;
+  ShadowQueue sh;
+  float4* path_L;
+  float4* nee_li;
+  float4* nee_dir;
+  int* cnt;
+  float* sh_out;
+  float* env_out;
+};
+
+// ------------------------------------------------------------- generate --
+__global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
+  const int64_t P = (int64_t)a.n_tex * a.spp;
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t warp_id = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = warp_id * 32; base < P; base += warps * 32) {
+    int64_t p = base + lane;
+    bool active = p < P;
+    f3 o = {0.f, 0.f, 0.f}, dw = {0.f, 0.f, 1.f}, P0 = o, N = o;
+    uint32_t texel = 0, sample = 0;
+    if (active) {
+      uint32_t slot = (uint32_t)(p / a.spp);
+      sample = (uint32_t)(p % a.spp) + a.sample_offset;
+      texel = a.valid[a.t0 + slot];
+      SP sp = load_sp(a.pts, texel);
+      P0 = sp.pos;
+      N = sp.nrm;
+      dw = primary_dir(sp, a.seed, texel, sample);
+      o = sp.pos + sp.nrm * 0.001f;
+      a.path_L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    // texel-level NEE (src/light.cpp:191-293), origin without offset
+    Event ev;
+    ev.init(a.seed, texel, sample, 0, EV_NEE);
+    const f3 zero3 = {0.f, 0.f, 0.f};
+    float sum = active ? light_weight_sum<false>(a.sc, P0, N, ev, zero3, zero3) : 0.f;
+    bool any_light = active && !(sum < 1e-6f);
+    for (int j = 0; j < a.nls; ++j) {
+      LightEval e;
+      bool ok = false;
+      if (any_light) {
+        ok = pick_light<false>(a.sc, P0, N, ev, zero3, zero3, sum, ev.u(3 * (int)a.sc.area_light_count + j), e);
+        if (ok) {
+          float pdf = e.w / sum;
+          float joint = pdf * e.apdf;
+          ok = !(joint < 1e-3f);
+          if (ok) {
+            f3 Li = e.rad / (joint * (float)a.nls);
+            a.nee_li[p * a.nls + j] = make_float4(Li.x, Li.y, Li.z, 0.f);
+            a.nee_dir[p * a.nls + j] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, 0.f);
+          }
+        }
+      }
+      if (active && !ok) a.nee_li[p * a.nls + j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      int slot = warp_push(a.cnt + CNT_SHADOW, ok);
+      if (ok) {
+        a.sh.o[slot] = make_float4(P0.x, P0.y, P0.z, e.tfar);
+        a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float((uint32_t)(p * a.nls + j)));
+        a.sh.c[slot] = make_float4(0.f, 0.f, 0.f, __uint_as_float(1u));
+      }
+    }
+    int slot = warp_push(a.cnt + CNT_EXT0, active);
+    if (active) {
+      a.ext[0].o[slot] = make_float4(o.x, o.y, o.z, __uint_as_float((uint32_t)p));
+      a.ext[0].d[slot] = make_float4(dw.x, dw.y, dw.z, __uint_as_float(1u));
+      a.ext[0].beta[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
+    }
+  }
+}
+
+// --------------------------------------------------------------- shade ---
+// One path vertex of Trace (src/baker.cpp:70-149) in throughput form.
+__global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int depth, int can_extend) {
+  const int n = a.cnt[cur];
+  const int nxt = cur ^ 1;
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const ExtQueue q = a.ext[cur];
+  const ExtQueue qn = a.ext[nxt];
+  for (int base = warp_id * 32; base < n; base += warps * 32) {
+    int i = base + lane;
+    bool active = i < n;
+    bool hit = false;
+    uint32_t path = 0, vertex = 0, texel = 0, sample = 0;
+    f3 d = {0.f, 0.f, 1.f}, beta = {0.f, 0.f, 0.f}, pos = {0.f, 0.f, 0.f}, N = {0.f, 0.f, 1.f};
+    f2 uv = {0.f, 0.f};
+    float alpha = 1.f;
+    DMat mat;
+    if (active) {
+      float4 qo = q.o[i], qd = q.d[i], qb = q.beta[i], h = a.hits[i];
+      path = __float_as_uint(qo.w);
+      vertex = __float_as_uint(qd.w);
+      d = {qd.x, qd.y, qd.z};
+      beta = {qb.x, qb.y, qb.z};
+      uint32_t prim = __float_as_uint(h.w);
+      if (prim == kMissPrim) {
+        if (depth == 0) a.path_L[path].w += 1.0f;
+      } else {
+        hit = true;
+        uint32_t slot = path / a.spp;
+        texel = a.valid[a.t0 + slot];
+        sample = path % a.spp + a.sample_offset;
+        f3 o = {qo.x, qo.y, qo.z};
+        pos = o + d * h.x;
+        float u = h.y, v = h.z;
+        float w = 1.0f - u - v;
+        uint32_t g = a.sc.tri_geom[prim];
+        DGeom G = a.sc.geoms[g];
+        uint32_t i0 = a.sc.tri_vidx[3 * prim], i1 = a.sc.tri_vidx[3 * prim + 1], i2 = a.sc.tri_vidx[3 * prim + 2];
+        if (G.flags & GEOM_HAS_NORMALS) {
+          N = normalized(w * ld3(a.sc.obj_n, i0) + u * ld3(a.sc.obj_n, i1) + v * ld3(a.sc.obj_n, i2));
+        } else {
+          f3 v0 = ld3(a.sc.world_v, i0), v1 = ld3(a.sc.world_v, i1), v2 = ld3(a.sc.world_v, i2);
+          N = normalized(cross(v1 - v0, v2 - v0));
+        }
+        if (G.flags & GEOM_HAS_TEXUV)
+          uv = w * ld2(a.sc.tex_uv, i0) + u * ld2(a.sc.tex_uv, i1) + v * ld2(a.sc.tex_uv, i2);
+        mat = load_mat(a.sc, G.material_id);
+        alpha = get_alpha(a.sc, mat, uv);
+      }
+    }
+    // transmission (src/baker.cpp:99-105)
+    if (a.sc.has_alpha) {
+      bool tr = hit && alpha < 1.0f && can_extend;
+      int slot = warp_push(a.cnt + nxt, tr);
+      if (tr) {
+        f3 hp = pos + d * 0.001f;
+        f3 bt = beta * (1.0f - alpha);
+        qn.o[slot] = make_float4(hp.x, hp.y, hp.z, __uint_as_float(path));
+        qn.d[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(2u * vertex + 1u));
+        qn.beta[slot] = make_float4(bt.x, bt.y, bt.z, 0.f);
+      }
+    }
+    bool opaque_hit = hit && alpha != 0.0f;
+    f3 hit_pos = pos, aop = {0.f, 0.f, 0.f};
+    if (opaque_hit) {
+      f3 alb = get_albedo(a.sc, mat, uv);
+      aop = alb / 3.14159265358979323846f;
+      if (depth == 0) {
+        f3 em = mat.emission > 0.0f ? alb * mat.emission : f3{0.f, 0.f, 0.f};
+        if (!is_zero_eigen(em)) {
+          f3 c = cmul(beta, alpha * em);
+          float4 L = a.path_L[path];
+          a.path_L[path] = make_float4(L.x + c.x, L.y + c.y, L.z + c.z, L.w);
+        }
+      }
+      hit_pos = pos + N * 0.001f;
+    }
+    // NEE at the hit (src/light.cpp:82-189)
+    f3 wo = -d;
+    Event ev;
+    ev.init(a.seed, texel, sample, vertex, EV_NEE);
+    float sum = opaque_hit ? light_weight_sum<true>(a.sc, hit_pos, N, ev, wo, aop) : 0.f;
+    bool any_light = opaque_hit && !(sum < 1e-6f);
+    for (int j = 0; j < a.nls; ++j) {
+      LightEval e;
+      bool ok = false;
+      f3 c = {0.f, 0.f, 0.f};
+      if (any_light) {
+        ok = pick_light<true>(a.sc, hit_pos, N, ev, wo, aop, sum, ev.u(3 * (int)a.sc.area_light_count + j), e);
+        if (ok) {
+          float pdf = e.w / sum;
+          float joint = pdf * e.apdf;
+          ok = !(joint < 1e-3f);
+          if (ok) c = cmul(beta, alpha * ((e.rad / joint) / (float)a.nls));
+        }
+      }
+      int slot = warp_push(a.cnt + CNT_SHADOW, ok);
+      if (ok) {
+        a.sh.o[slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, e.tfar);
+        a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float(path));
+        a.sh.c[slot] = make_float4(c.x, c.y, c.z, __uint_as_float(0u));
+      }
+    }
+    // indirect (src/material.cpp:113-162, src/baker.cpp:131-148)
+    bool ext = false;
+    f3 nd = {0.f, 0.f, 1.f}, nb = {0.f, 0.f, 0.f};
+    if (opaque_hit && can_extend) {
+      Event eb;
+      eb.init(a.seed, texel, sample, vertex, EV_BSDF);
+      f3 t = fabsf(N.x) > fabsf(N.z) ? f3{-N.y, N.x, 0.0f} : f3{0.0f, -N.z, N.y};
+      t = normalized(t);
+      f3 b = cross(N, t);
+      float r1 = eb.u(0), r2 = eb.u(1);
+      float phi = (float)(kTwoPiD * (double)r1);
+      float theta = acosf(sqrtf(r2));
+      float sin_theta = sinf(theta);
+      f3 local = {cosf(phi) * sin_theta, sinf(phi) * sin_theta, cosf(theta)};
+      nd = normalized(t * local.x + b * local.y + N * local.z);
+      float pdf = (float)((double)local.z / 3.14159265358979323846);
+      if (!(pdf < 1e-3f)) {
+        bool zero = dot(N, nd) <= 0.0f || dot(N, wo) <= 0.0f;
+        f3 brdf = zero ? f3{0.f, 0.f, 0.f} : aop;
+        float cos_term = dot(N, nd);
+        nb = cmul(beta, alpha * (brdf * (cos_term / pdf)));
+        ext = !(nb.x == 0.f && nb.y == 0.f && nb.z == 0.f);
+      }
+    }
+    int slot = warp_push(a.cnt + nxt, ext);
+    if (ext) {
+      qn.o[slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, __uint_as_float(path));
+      qn.d[slot] = make_float4(nd.x, nd.y, nd.z, __uint_as_float(2u * vertex));
+      qn.beta[slot] = make_float4(nb.x, nb.y, nb.z, 0.f);
+    }
+  }
+}
+
+// ------------------------------------------------------------- resolve ---
+__device__ __forceinline__ void sh_accumulate(f3 L, f3 d, float acc[27]) {
+  const float x = d.x, y = d.y, z = d.z;
+  float sh[9];
+  sh[0] = 0.282095f;
+  sh[1] = 0.488603f * y;
+  sh[2] = 0.488603f * z;
+  sh[3] = 0.488603f * x;
+  sh[4] = 1.092548f * x * y;
+  sh[5] = 1.092548f * y * z;
+  sh[6] = 0.315392f * (3.0f * z * z - 1.0f);
+  sh[7] = 1.092548f * x * z;
+  sh[8] = 0.546274f * (x * x - y * y);
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    acc[3 * i] += L.x * sh[i];
+    acc[3 * i + 1] += L.y * sh[i];
+    acc[3 * i + 2] += L.z * sh[i];
+  }
+}
+
+// One warp per texel: each lane projects its samples into SH9 in registers
+// (src/sh_coeffs.cpp:50-78), the warp reduces with shuffles, and lanes
+// 0..27 store the 27 coefficients and the environment visibility.
+__global__ void __launch_bounds__(kThreads) k_resolve(WaveArgs a) {
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const float two_pi = (float)kTwoPiD;
+  for (uint32_t slot = warp_id; slot < a.n_tex; slot += warps) {
+    uint32_t texel = a.valid[a.t0 + slot];
+    SP sp = load_sp(a.pts, texel);
+    float acc[27];
+#pragma unroll
+    for (int k = 0; k < 27; ++k) acc[k] = 0.f;
+    float env = 0.f;
+    for (uint32_t s = lane; s < a.spp; s += 32) {
+      int64_t p = (int64_t)slot * a.spp + s;
+      for (int j = 0; j < a.nls; ++j) {
+        float4 li = a.nee_li[p * a.nls + j];
+        if (li.x != 0.f || li.y != 0.f || li.z != 0.f) {
+          float4 nd = a.nee_dir[p * a.nls + j];
+          sh_accumulate(f3{li.x, li.y, li.z}, f3{nd.x, nd.y, nd.z}, acc);
+        }
+      }
+      float4 L = a.path_L[p];
+      f3 dw = primary_dir(sp, a.seed, texel, s + a.sample_offset);
+      sh_accumulate(f3{L.x, L.y, L.z} * two_pi, dw, acc);
+      env += L.w;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+      for (int k = 0; k < 27; ++k) acc[k] += __shfl_xor_sync(0xFFFFFFFFu, acc[k], off);
+      env += __shfl_xor_sync(0xFFFFFFFFu, env, off);
+    }
+    const float inv = 1.0f / (float)a.spp;
+    float mine = 0.f;
+#pragma unroll
+    for (int k = 0; k < 27; ++k)
+      if (lane == k) mine = acc[k];
+    if (lane < 27) a.sh_out[(int64_t)texel * 27 + lane] = mine * inv;
+    else if (lane == 27) a.env_out[texel] = env * inv;
+  }
+}
+
+// Hit attributes of FindOcclusion (src/occlusion.cpp:70-133).
+__global__ void k_occ_attrs(SceneView sc, const shb_ray* __restrict__ rays, const float4* __restrict__ hits, int64_t n,
+                            shb_hit* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    float4 h = hits[i];
+    uint32_t prim = __float_as_uint(h.w);
+    shb_hit r;
+    r.position[0] = r.position[1] = r.position[2] = 0.f;
+    r.uv[0] = r.uv[1] = 0.f;
+    r.normal[0] = r.normal[1] = r.normal[2] = 0.f;
+    r.material_id = 0;
+    r.hit = 0;
+    r.t = 0.f;
+    r.prim_id = 0;
+    if (prim != kMissPrim) {
+      const shb_ray& ray = rays[i];
+      f3 o = {ray.origin[0], ray.origin[1], ray.origin[2]};
+      f3 d = {ray.direction[0], ray.direction[1], ray.direction[2]};
+      f3 pos = o + d * h.x;
+      float u = h.y, v = h.z, w = 1.0f - u - v;
+      DGeom G = sc.geoms[sc.tri_geom[prim]];
+      uint32_t i0 = sc.tri_vidx[3 * prim], i1 = sc.tri_vidx[3 * prim + 1], i2 = sc.tri_vidx[3 * prim + 2];
+      f3 N;
+      if (G.flags & GEOM_HAS_NORMALS) {
+        N = normalized(w * ld3(sc.obj_n, i0) + u * ld3(sc.obj_n, i1) + v * ld3(sc.obj_n, i2));
+      } else {
+        f3 v0 = ld3(sc.world_v, i0), v1 = ld3(sc.world_v, i1), v2 = ld3(sc.world_v, i2);
+        N = normalized(cross(v1 - v0, v2 - v0));
+      }
+      f2 uv = {0.f, 0.f};
+      if (G.flags & GEOM_HAS_TEXUV) uv = w * ld2(sc.tex_uv, i0) + u * ld2(sc.tex_uv, i1) + v * ld2(sc.tex_uv, i2);
+      r.position[0] = pos.x;
+      r.position[1] = pos.y;
+      r.position[2] = pos.z;
+      r.uv[0] = uv.x;
+      r.uv[1] = uv.y;
+      r.normal[0] = N.x;
+      r.normal[1] = N.y;
+      r.normal[2] = N.z;
+      r.material_id = G.material_id;
+      r.hit = 1;
+      r.t = h.x;
+      r.prim_id = prim;
+    }
+    out[i] = r;
+  }
+}
+
+struct ValidPred {
+  const shb_surface_point* pts;
+  __device__ __forceinline__ bool operator()(uint32_t i) const { return pts[i].material_id >= 0; }
+};
+
+inline int grid_for(int64_t n) {
+  int64_t g = (n + kThreads - 1) / kThreads;
+  if (g > 148 * 8) g = 148 * 8;
+  return (int)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+void srgb_upload(const float table[256]) { cudaMemcpyToSymbol(c_srgb, table, sizeof(float) * 256); }
+
+shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n, shb_hit* d_hits) {
+  shb_context* c = s->ctx;
+  if (n <= 0) return SHB_OK;
+  SHB_TRY(c->scratch[9].reserve(sizeof(float4) * (size_t)n));
+  SHB_TRY(c->counters.reserve(sizeof(int) * CNT_COUNT + sizeof(Counters64)));
+  int* cnt = c->counters.as<int>();
+  SHB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * CNT_COUNT, c->stream));
+  float4* hits = c->scratch[9].as<float4>();
+  launch_closest_rays(c->stream, s->bvh(), d_rays, n, hits, cnt + CNT_ERROR);
+  k_occ_attrs<<<grid_for(n), kThreads, 0, c->stream>>>(s->view(), d_rays, hits, n, d_hits);
+  count_launch(c, 2);
+  SHB_CUDA(cudaGetLastError());
+  int err = 0;
+  SHB_CUDA(cudaMemcpyAsync(&err, cnt + CNT_ERROR, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  SHB_CUDA(cudaStreamSynchronize(c->stream));
+  if (err) {
+    set_error("traversal stack overflow");
+    return SHB_ERR_INTERNAL;
+  }
+  return SHB_OK;
+}
+
+// BakeSHLightMap on a device G-buffer: waves of (texels x samples) paths.
+shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int H, const shb_bake_config* cfg,
+                       float* d_sh, float* d_env, shb_bake_stats* stats) {
+  shb_context* c = s->ctx;
+  cudaStream_t st = c->stream;
+  const int64_t total = (int64_t)W * H;
+  const int spp = cfg->samples, B = cfg->bounces;
+  const int nls = cfg->num_light_samples;
+  SHB_CUDA(cudaMemsetAsync(d_sh, 0, sizeof(float) * 27 * (size_t)total, st));
+  SHB_CUDA(cudaMemsetAsync(d_env, 0, sizeof(float) * (size_t)total, st));
+  // compact valid texels (material_id >= 0), stable order
+  SHB_TRY(c->scratch[10].reserve(sizeof(uint32_t) * (size_t)(total + 1)));
+  SHB_TRY(c->counters.reserve(sizeof(int) * CNT_COUNT + sizeof(Counters64)));
+  uint32_t* valid = c->scratch[10].as<uint32_t>();
+  int* cnt = c->counters.as<int>();
+  Counters64* c64 = reinterpret_cast<Counters64*>(cnt + CNT_COUNT);
+  SHB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * CNT_COUNT + sizeof(Counters64), st));
+  thrust::counting_iterator<uint32_t> it(0);
+  size_t tb = 0;
+  int* nsel = cnt + CNT_COUNT - 1;
+  cub::DeviceSelect::If(nullptr, tb, it, valid, nsel, (int)total, ValidPred{d_pts}, st);
+  SHB_TRY(c->scratch[11].reserve(tb));
+  SHB_CUDA(cub::DeviceSelect::If(c->scratch[11].ptr, tb, it, valid, nsel, (int)total, ValidPred{d_pts}, st));
+  count_launch(c, 1);
+  int n_valid = 0;
+  SHB_CUDA(cudaMemcpyAsync(&n_valid, nsel, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SHB_CUDA(cudaStreamSynchronize(st));
+
+  // wave sizing: paths per wave, queue capacity per depth
+  const int64_t kPathsPerWave = 1 << 22;
+  int64_t tex_per_wave = kPathsPerWave / spp;
+  if (tex_per_wave < 1) tex_per_wave = 1;
+  int64_t mult = 1;
+  if (s->has_alpha) {
+    int sh = B < 4 ? B : 4;
+    mult = (int64_t)1 << sh;
+    tex_per_wave = tex_per_wave / mult > 0 ? tex_per_wave / mult : 1;
+  }
+  if (tex_per_wave > n_valid && n_valid > 0) tex_per_wave = n_valid;
+  const int64_t P = tex_per_wave * spp;
+  const int64_t ext_cap = P * mult;
+  const int64_t sh_cap = (P + ext_cap) * nls;
+  SHB_TRY(c->scratch[12].reserve(sizeof(float4) * 3 * (size_t)ext_cap));
+  SHB_TRY(c->scratch[13].reserve(sizeof(float4) * 3 * (size_t)ext_cap));
+  SHB_TRY(c->scratch[14].reserve(sizeof(float4) * (size_t)ext_cap));
+  SHB_TRY(c->scratch[15].reserve(sizeof(float4) * 3 * (size_t)sh_cap));
+  SHB_TRY(c->scratch[16].reserve(sizeof(float4) * (size_t)P));
+  SHB_TRY(c->scratch[17].reserve(sizeof(float4) * 2 * (size_t)P * nls));
+  WaveArgs a;
+  a.sc = s->view();
+  a.pts = d_pts;
+  a.valid = valid;
+  a.spp = (uint32_t)spp;
+  a.seed = cfg->seed;
+  a.sample_offset = (uint32_t)cfg->sample_offset;
+  a.nls = nls;
+  a.bounces = B;
+  for (int k = 0; k < 2; ++k) {
+    float4* base = c->scratch[12 + k].as<float4>();
+    a.ext[k] = ExtQueue{base, base + ext_cap, base + 2 * ext_cap};
+  }
+  a.hits = c->scratch[14].as<float4>();
+  {
+    float4* base = c->scratch[15].as<float4>();
+    a.sh = ShadowQueue{base, base + sh_cap, base + 2 * sh_cap};
+  }
+  a.path_L = c->scratch[16].as<float4>();
+  a.nee_li = c->scratch[17].as<float4>();
+  a.nee_dir = a.nee_li + P * nls;
+  a.cnt = cnt;
+  a.sh_out = d_sh;
+  a.env_out = d_env;
+
+  const BvhView bvh = s->bvh();
+  const int tgrid = traversal_grid(c->device);
+  const int sgrid = 148 * 8;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  double ext_ms = 0.0, sh_ms = 0.0;
+  uint64_t ext_launches = 0, sh_launches = 0;
+  std::vector<cudaEvent_t> evs;
+  if (c->profiling) {
+    cudaEventCreate(&ev[0]);
+    cudaEventCreate(&ev[1]);
+    cudaEventRecord(ev[0], st);
+  }
+  int waves = 0;
+  struct Pair { cudaEvent_t a, b; int kind; };
+  std::vector<Pair> timed;
+  for (int64_t t0 = 0; t0 < n_valid; t0 += tex_per_wave) {
+    a.t0 = (uint32_t)t0;
+    a.n_tex = (uint32_t)((n_valid - t0) < tex_per_wave ? (n_valid - t0) : tex_per_wave);
+    SHB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * CNT_FETCH_SHADOW + sizeof(int), st));
+    k_generate<<<grid_for((int64_t)a.n_tex * spp), kThreads, 0, st>>>(a);
+    count_launch(c);
+    for (int k = 0; k <= B; ++k) {
+      int cur = k & 1, nxt = cur ^ 1;
+      SHB_CUDA(cudaMemsetAsync(cnt + nxt, 0, sizeof(int), st));
+      SHB_CUDA(cudaMemsetAsync(cnt + CNT_FETCH_EXT, 0, sizeof(int) * 2, st));
+      Pair pe{nullptr, nullptr, 0};
+      if (c->profiling) {
+        cudaEventCreate(&pe.a);
+        cudaEventCreate(&pe.b);
+        cudaEventRecord(pe.a, st);
+      }
+      launch_extend(st, tgrid, bvh, a.ext[cur], cnt + cur, a.hits, cnt + CNT_FETCH_EXT, cnt + CNT_ERROR, c64);
+      if (c->profiling) {
+        cudaEventRecord(pe.b, st);
+        timed.push_back(pe);
+      }
+      k_shade<<<sgrid, kThreads, 0, st>>>(a, cur, k, k < B ? 1 : 0);
+      Pair ps{nullptr, nullptr, 1};
+      if (c->profiling) {
+        cudaEventCreate(&ps.a);
+        cudaEventCreate(&ps.b);
+        cudaEventRecord(ps.a, st);
+      }
+      launch_shadow(st, tgrid, bvh, a.sh, cnt + CNT_SHADOW, a.path_L, a.nee_li, cnt + CNT_FETCH_SHADOW,
+                    cnt + CNT_ERROR, c64);
+      if (c->profiling) {
+        cudaEventRecord(ps.b, st);
+        timed.push_back(ps);
+      }
+      SHB_CUDA(cudaMemsetAsync(cnt + CNT_SHADOW, 0, sizeof(int), st));
+      count_launch(c, 3);
+      ext_launches++;
+      sh_launches++;
+    }
+    k_resolve<<<grid_for((int64_t)a.n_tex * 32), kThreads, 0, st>>>(a);
+    count_launch(c);
+    SHB_CUDA(cudaGetLastError());
+    waves++;
+  }
+  int err = 0;
+  Counters64 h64{0, 0};
+  SHB_CUDA(cudaMemcpyAsync(&err, cnt + CNT_ERROR, sizeof(int), cudaMemcpyDeviceToHost, st));
+  SHB_CUDA(cudaMemcpyAsync(&h64, c64, sizeof(Counters64), cudaMemcpyDeviceToHost, st));
+  if (c->profiling) cudaEventRecord(ev[1], st);
+  SHB_CUDA(cudaStreamSynchronize(st));
+  float total_ms = 0.f;
+  if (c->profiling) {
+    cudaEventElapsedTime(&total_ms, ev[0], ev[1]);
+    for (auto& pr : timed) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, pr.a, pr.b);
+      if (pr.kind == 0) ext_ms += ms;
+      else sh_ms += ms;
+      cudaEventDestroy(pr.a);
+      cudaEventDestroy(pr.b);
+    }
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+  }
+  if (stats) {
+    stats->texel_samples = (uint64_t)n_valid * (uint64_t)spp;
+    stats->valid_texels = (uint64_t)n_valid;
+    stats->extend_rays = h64.extend_rays;
+    stats->shadow_rays = h64.shadow_rays;
+    stats->error_flags = (uint32_t)err;
+    stats->waves = (uint32_t)waves;
+    stats->trace_ms = total_ms;
+    stats->extend_kernel_ms = ext_ms;
+    stats->shadow_kernel_ms = sh_ms;
+    stats->extend_launches = ext_launches;
+    stats->shadow_launches = sh_launches;
+  }
+  if (err) {
+    set_error(err & ERR_STACK ? "traversal stack overflow" : "ray queue overflow");
+    return SHB_ERR_INTERNAL;
+  }
+  return SHB_OK;
+}
+
+}  // namespace shb

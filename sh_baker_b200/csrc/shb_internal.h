@@ -1,0 +1,189 @@
+// shb_internal.h - host/device data structures shared by the CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/shb.h"
+
+#define SHB_HD __host__ __device__ __forceinline__
+
+namespace shb {
+
+// ------------------------------------------------------------ errors ------
+
+void set_error(const std::string& msg);
+shb_status cuda_fail(cudaError_t e, const char* what);
+
+#define SHB_CUDA(call)                                             \
+  do {                                                             \
+    cudaError_t _e = (call);                                       \
+    if (_e != cudaSuccess) return ::shb::cuda_fail(_e, #call);     \
+  } while (0)
+
+#define SHB_TRY(call)                      \
+  do {                                     \
+    shb_status _s = (call);                \
+    if (_s != SHB_OK) return _s;           \
+  } while (0)
+
+// --------------------------------------------------------- device buffer --
+
+// Owning device allocation (cudaMalloc), grown on demand, never shrunk.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  ~DevBuf() { release(); }
+  void release() {
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+  }
+  shb_status reserve(size_t n);  // keeps no contents
+  template <class T>
+  T* as() const { return reinterpret_cast<T*>(ptr); }
+};
+
+// -------------------------------------------------------------- scene -----
+
+struct DGeom {
+  uint32_t vbase;      // first vertex in the global vertex arrays
+  uint32_t prim_base;  // first triangle in global (geometry-major) order
+  uint32_t tri_count;
+  int32_t material_id;
+  uint32_t flags;      // GEOM_* bits
+  uint32_t pad[3];
+};
+enum : uint32_t { GEOM_HAS_NORMALS = 1, GEOM_HAS_TEXUV = 2, GEOM_HAS_TANGENTS = 4, GEOM_HAS_LMUV = 8 };
+
+struct DMat {
+  uint32_t pix_offset;
+  uint32_t w, h, c;    // c == 0: no albedo texture (default 0.8 grey)
+  float emission;
+  int32_t use_override;  // 1: albedo := override (linear), adjoint parameter
+  float override_rgb[3];
+  float pad;
+};
+
+struct DLight {
+  int32_t type;
+  float px, py, pz;
+  float dx, dy, dz;
+  float cr, cg, cb;
+  float intensity;
+  float cos_inner, cos_outer;
+  int32_t geom;      // area: geometry index
+  int32_t mat;       // area: material index
+  int32_t area_ord;  // area: ordinal among area lights (RNG slots)
+};
+
+// Compressed 8-wide BVH node (80 bytes).  Children boxes are quantised on
+// a per-node power-of-two grid anchored at p; slot s holds the child whose
+// centroid lies in octant s of the parent (bit a set = positive side of
+// axis a), so a ray visits slots in order i ^ octant(ray).
+struct alignas(16) WideNode {
+  float px, py, pz;
+  uint32_t e_imask;   // ex | ey<<8 | ez<<16 | imask<<24
+  uint32_t child_base;
+  uint32_t tri_base;
+  uint32_t meta_lo;   // meta of slots 0..3 (byte each)
+  uint32_t meta_hi;   // meta of slots 4..7
+  uint32_t qlo[6];    // qlo_x[8], qlo_y[8], qlo_z[8]
+  uint32_t qhi[6];    // qhi_x[8], qhi_y[8], qhi_z[8]
+};
+static_assert(sizeof(WideNode) == 80, "WideNode must be 80 bytes");
+// meta byte: 0 = empty slot; internal child: 1; leaf: count<<5 | offset.
+
+struct BvhView {
+  const WideNode* nodes;
+  const float4* tris;   // 3 float4 per triangle in leaf order, v0.w = prim id
+  uint32_t node_count;
+  uint32_t tri_count;
+};
+
+struct SceneView {
+  // per vertex (global)
+  const float* obj_v;    // 3 per vertex
+  const float* obj_n;    // 3 per vertex
+  const float* tex_uv;   // 2 per vertex
+  const float* world_v;  // 3 per vertex
+  // per triangle (global order)
+  const uint32_t* tri_vidx;  // 3 per triangle (global vertex ids)
+  const uint32_t* tri_geom;  // geometry of each triangle
+  const DGeom* geoms;
+  const DMat* mats;
+  const uint8_t* pixels;
+  const DLight* lights;
+  uint32_t geom_count, mat_count, light_count, area_light_count;
+  uint32_t prim_count, vertex_count;
+  int32_t has_alpha;     // any material with 4-channel albedo
+};
+
+}  // namespace shb
+
+// Opaque handles of the C ABI.
+struct shb_context {
+  int device = 0;
+  int profiling = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  uint64_t launches = 0;
+  // scratch reused across calls
+  shb::DevBuf scratch[24];
+  shb::DevBuf counters;
+  void* host_pinned = nullptr;
+  size_t host_pinned_bytes = 0;
+};
+
+struct shb_scene {
+  shb_context* ctx = nullptr;
+  // uploaded per-vertex arrays
+  shb::DevBuf obj_v, obj_n, tex_uv, lm_uv, obj_t, world_v, world_n, world_t;
+  shb::DevBuf tri_vidx, tri_geom, geoms, mats, pixels, lights, rot, lin, vgeom;
+  uint32_t vertex_count = 0, prim_count = 0, geom_count = 0, mat_count = 0, light_count = 0;
+  uint32_t area_light_count = 0;
+  int32_t has_alpha = 0;
+  bool raster_ready = true;  // every geometry has normals, tangents, lightmap uvs
+  std::string raster_error;
+  std::vector<shb::DGeom> h_geoms;
+  // BVH
+  shb::DevBuf bvh_nodes, bvh_tris;
+  uint32_t bvh_node_count = 0, bvh_tri_count = 0, bvh_depth = 0;
+  double bvh_build_ms = 0.0;
+  shb::SceneView view() const;
+  shb::BvhView bvh() const;
+};
+
+struct shb_gbuffer {
+  shb_context* ctx = nullptr;
+  shb::DevBuf points;  // shb_surface_point per texel
+  int32_t width = 0, height = 0;
+};
+
+namespace shb {
+
+// launch bookkeeping
+inline void count_launch(shb_context* c, uint64_t n = 1) { c->launches += n; }
+
+// kernels implemented in the .cu files
+shb_status transform_vertices(shb_scene* s);
+shb_status build_bvh(shb_scene* s);
+shb_status rasterize_device(shb_scene* s, int W, int H, shb_surface_point* d_out);
+shb_status validity_mask_device(shb_context* c, const shb_surface_point* pts, int64_t n, uint8_t* out);
+shb_status downsample_mask_device(shb_context* c, const uint8_t* in, int w, int h, int s, uint8_t* out);
+shb_status downsample_device(shb_context* c, const float* in, int w, int h, int ch, int s, float* out);
+shb_status dilate_device(shb_context* c, int kind, int w, int h, void* pixels, uint8_t* mask, int passes);
+shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int H,
+                       const shb_bake_config* cfg, float* d_sh, float* d_env, shb_bake_stats* stats);
+shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n, shb_hit* d_hits);
+
+// sRGB -> linear table (computed on the host with powf, colorspace.h:10-14)
+void srgb_table(float out[256]);
+
+}  // namespace shb

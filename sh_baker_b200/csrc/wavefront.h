@@ -1,0 +1,58 @@
+// wavefront.h - ray queues and per-path state of the wavefront path tracer.
+#pragma once
+
+#include "shb_internal.h"
+
+namespace shb {
+
+constexpr uint32_t kMissPrim = 0xFFFFFFFFu;
+
+// Extend (closest-hit) queue entry, structure of arrays:
+//   o    = (origin.xyz, path index bits)
+//   d    = (direction.xyz, path-vertex id bits)
+//   beta = (throughput.xyz, unused)
+struct ExtQueue {
+  float4* o;
+  float4* d;
+  float4* beta;
+};
+
+// Shadow (any-hit) queue entry: tnear is 0.001 for every shadow ray
+// (src/light.h:40,83,128,177).
+//   o = (origin.xyz, tfar), d = (direction.xyz, target bits),
+//   c = (contribution.xyz, kind bits): kind 0 adds c to the path radiance
+//   of `target` when unoccluded; kind 1 clears texel-NEE slot `target`
+//   when occluded.
+struct ShadowQueue {
+  float4* o;
+  float4* d;
+  float4* c;
+};
+
+// Device counters of one bake.
+enum CounterSlot {
+  CNT_EXT0 = 0,
+  CNT_EXT1 = 1,
+  CNT_SHADOW = 2,
+  CNT_FETCH_EXT = 3,
+  CNT_FETCH_SHADOW = 4,
+  CNT_ERROR = 5,
+  CNT_COUNT = 8
+};
+enum ErrorBits : int { ERR_STACK = 1, ERR_QUEUE = 2 };
+
+struct Counters64 {
+  unsigned long long extend_rays;
+  unsigned long long shadow_rays;
+};
+
+// Launch helpers for the persistent traversal kernels (traverse.cu).
+void launch_extend(cudaStream_t st, int grid, const BvhView& bvh, ExtQueue q, const int* n, float4* hits,
+                   int* fetch, int* err, Counters64* stats);
+void launch_shadow(cudaStream_t st, int grid, const BvhView& bvh, ShadowQueue q, const int* n, float4* path_L,
+                   float4* nee_li, int* fetch, int* err, Counters64* stats);
+void launch_closest_rays(cudaStream_t st, const BvhView& bvh, const shb_ray* rays, int64_t n, float4* hits,
+                         int* err);
+int traversal_grid(int device);
+
+}  // namespace shb

@@ -1,0 +1,235 @@
+"""Seeded synthetic scenes with the shapes and sizes of the bake workloads.
+
+Every generator is deterministic in its seed.  Lightmap UVs come from this
+module's own chart packer (one chart per planar patch or unwrapped
+cylinder, shelf-packed with a texel padding); the reference's xatlas
+unwrapper (src/atlas.cpp) is not used.  Emissive geometries become area
+lights the way the reference's loader does it (src/loader.cpp:391-411).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+from typing import List, Tuple
+
+import numpy as np
+
+from .scene import AREA, DIRECTIONAL, POINT, Geometry, Light, Material, Scene, Texture
+
+
+def linear_to_srgb_byte(x: float) -> int:
+    """src/colorspace.h:16-21."""
+    if x <= 0.0031308:
+        return int(np.rint(x * 12.92 * 255.0))
+    return int(np.rint((1.055 * math.pow(x, 1.0 / 2.4) - 0.055) * 255.0))
+
+
+def solid_material(rgb, emission: float = 0.0, name: str = "") -> Material:
+    px = np.array([linear_to_srgb_byte(float(c)) for c in rgb], dtype=np.uint8)
+    return Material(name=name, albedo=Texture(1, 1, 3, px), emission_intensity=float(emission))
+
+
+def _normalize(v):
+    v = np.asarray(v, dtype=np.float64)
+    return v / np.linalg.norm(v)
+
+
+# ------------------------------------------------------------------ patches --
+
+@dataclass
+class Patch:
+    """A chart: a planar grid (corner, eu, ev) or a cylinder side."""
+    geom: int
+    kind: str  # "quad" | "cyl"
+    corner: np.ndarray
+    eu: np.ndarray
+    ev: np.ndarray
+    nu: int = 1
+    nv: int = 1
+    radius: float = 0.0
+    height: float = 0.0
+    inward: bool = False
+
+    def world_size(self) -> Tuple[float, float]:
+        if self.kind == "quad":
+            return float(np.linalg.norm(self.eu)), float(np.linalg.norm(self.ev))
+        return 2.0 * math.pi * self.radius, self.height
+
+
+def shelf_pack(sizes: List[Tuple[float, float]], res: int, padding: int):
+    """Packs world-size charts into a res x res atlas at one texel density.
+    Returns (texel_size, [(x0, y0, cw, ch)]) in texels."""
+    total = sum(w * h for w, h in sizes)
+    s = math.sqrt(total / (res * res * 0.55)) if total > 0 else 1.0
+    order = sorted(range(len(sizes)), key=lambda i: -sizes[i][1])
+    for _ in range(200):
+        rects = [None] * len(sizes)
+        x = y = shelf_h = 0
+        ok = True
+        for i in order:
+            cw = max(1, int(math.ceil(sizes[i][0] / s)))
+            ch = max(1, int(math.ceil(sizes[i][1] / s)))
+            ow, oh = cw + padding, ch + padding
+            if ow > res:
+                ok = False
+                break
+            if x + ow > res:
+                x = 0
+                y += shelf_h
+                shelf_h = 0
+            if y + oh > res:
+                ok = False
+                break
+            rects[i] = (x + padding // 2, y + padding // 2, cw, ch)
+            x += ow
+            shelf_h = max(shelf_h, oh)
+        if ok:
+            return s, rects
+        s *= 1.04
+    raise RuntimeError("chart packing failed")
+
+
+class MeshBuilder:
+    def __init__(self, n_geoms: int):
+        self.v = [[] for _ in range(n_geoms)]
+        self.n = [[] for _ in range(n_geoms)]
+        self.t = [[] for _ in range(n_geoms)]
+        self.tuv = [[] for _ in range(n_geoms)]
+        self.luv = [[] for _ in range(n_geoms)]
+        self.idx = [[] for _ in range(n_geoms)]
+
+    def add_patch(self, p: Patch, rect, res: int):
+        g = p.geom
+        x0, y0, cw, ch = rect
+        base = sum(len(a) for a in self.v[g])
+        nu, nv = p.nu, p.nv
+        a = np.linspace(0.0, 1.0, nu + 1)
+        b = np.linspace(0.0, 1.0, nv + 1)
+        A, B = np.meshgrid(a, b)  # (nv+1, nu+1)
+        A = A.reshape(-1)
+        B = B.reshape(-1)
+        if p.kind == "quad":
+            pos = p.corner[None, :] + A[:, None] * p.eu[None, :] + B[:, None] * p.ev[None, :]
+            nrm = np.repeat(_normalize(np.cross(p.eu, p.ev))[None, :], len(A), 0)
+            tan = np.repeat(_normalize(p.eu)[None, :], len(A), 0)
+        else:
+            ang = A * 2.0 * math.pi
+            radial = np.stack([np.cos(ang), np.zeros_like(ang), np.sin(ang)], 1)
+            pos = p.corner[None, :] + p.radius * radial + (B * p.height)[:, None] * np.array([0.0, 1.0, 0.0])[None, :]
+            nrm = -radial if p.inward else radial
+            tan = np.stack([-np.sin(ang), np.zeros_like(ang), np.cos(ang)], 1)
+        luv = np.stack([(x0 + A * cw) / res, (y0 + B * ch) / res], 1)
+        self.v[g].append(pos.astype(np.float32))
+        self.n[g].append(nrm.astype(np.float32))
+        self.t[g].append(np.hstack([tan, np.ones((len(A), 1))]).astype(np.float32))
+        self.tuv[g].append(np.stack([A, B], 1).astype(np.float32))
+        self.luv[g].append(luv.astype(np.float32))
+        ii = []
+        for j in range(nv):
+            for i in range(nu):
+                q0 = j * (nu + 1) + i
+                q1, q2, q3 = q0 + 1, q0 + nu + 2, q0 + nu + 1
+                if p.kind == "cyl" and not p.inward:
+                    ii += [q0, q2, q1, q0, q3, q2]
+                else:
+                    ii += [q0, q1, q2, q0, q2, q3]
+        self.idx[g].append(np.asarray(ii, dtype=np.uint32) + base)
+
+    def geometries(self, material_ids: List[int]) -> List[Geometry]:
+        out = []
+        for g in range(len(self.v)):
+            if not self.v[g]:
+                continue
+            out.append(Geometry(
+                vertices=np.vstack(self.v[g]), indices=np.concatenate(self.idx[g]), normals=np.vstack(self.n[g]),
+                texture_uvs=np.vstack(self.tuv[g]), lightmap_uvs=np.vstack(self.luv[g]),
+                tangents=np.vstack(self.t[g]), material_id=material_ids[g]))
+        return out
+
+
+def build_from_patches(patches: List[Patch], material_ids: List[int], res: int, padding: int) -> List[Geometry]:
+    sizes = [p.world_size() for p in patches]
+    _, rects = shelf_pack(sizes, res, padding)
+    mb = MeshBuilder(len(material_ids))
+    for p, r in zip(patches, rects):
+        mb.add_patch(p, r, res)
+    return mb.geometries(material_ids)
+
+
+def box_patches(geom: int, lo, hi, inward: bool, subdiv: int = 1) -> List[Patch]:
+    lo = np.asarray(lo, np.float64)
+    hi = np.asarray(hi, np.float64)
+    d = hi - lo
+    X, Y, Z = np.array([d[0], 0, 0]), np.array([0, d[1], 0]), np.array([0, 0, d[2]])
+    # (corner, eu, ev) with eu x ev pointing outward
+    faces = [
+        (lo, Z, Y),                # -x
+        (lo + X, Y, Z),            # +x
+        (lo, X, Z),                # -y
+        (lo + Y, Z, X),            # +y
+        (lo, Y, X),                # -z
+        (lo + Z, X, Y),            # +z
+    ]
+    out = []
+    for c, eu, ev in faces:
+        if inward:
+            eu, ev = ev, eu
+        out.append(Patch(geom, "quad", np.asarray(c, np.float64), np.asarray(eu, np.float64),
+                         np.asarray(ev, np.float64), subdiv, subdiv))
+    return out
+
+
+def mark_area_lights(scene: Scene) -> None:
+    """Every geometry with an emissive material becomes an area light
+    (src/loader.cpp:391-411)."""
+    for gi, g in enumerate(scene.geometries):
+        m = scene.materials[g.material_id]
+        if m.emission_intensity > 0.0:
+            v = np.asarray(g.vertices, np.float64)
+            i = np.asarray(g.indices).reshape(-1, 3)
+            area = 0.5 * np.linalg.norm(np.cross(v[i[:, 1]] - v[i[:, 0]], v[i[:, 2]] - v[i[:, 0]]), axis=1).sum()
+            scene.lights.append(Light(type=AREA, material_index=g.material_id, geometry_index=gi,
+                                      area=float(area), intensity=m.emission_intensity))
+
+
+# ---------------------------------------------------------------- configs --
+
+def unit_quad() -> Scene:
+    """Unit quad [-0.5,0.5]^2 in the XZ plane at y=0, normal +Y, tangent +X,
+    UV = lightmap UV = [0,1]^2, default albedo 0.8; directional light
+    (0.3,-1,0.2)/|.| radiance 3 and a point light at (0,1,0) intensity 10."""
+    v = np.array([[-0.5, 0, -0.5], [0.5, 0, -0.5], [0.5, 0, 0.5], [-0.5, 0, 0.5]], np.float32)
+    uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
+    g = Geometry(vertices=v, indices=np.array([0, 2, 1, 0, 3, 2], np.uint32),
+                 normals=np.tile([0, 1, 0], (4, 1)).astype(np.float32), texture_uvs=uv, lightmap_uvs=uv,
+                 tangents=np.tile([1, 0, 0, 1], (4, 1)).astype(np.float32), material_id=0)
+    d = np.array([0.3, -1.0, 0.2], np.float32)
+    d = d / np.linalg.norm(d)
+    lights = [Light(type=DIRECTIONAL, direction=tuple(float(x) for x in d), intensity=3.0),
+              Light(type=POINT, position=(0.0, 1.0, 0.0), intensity=10.0)]
+    return Scene([g], [Material(name="grey")], lights)
+
+
+def procedural_room(seed: int = 2, n_boxes: int = 200, res: int = 1024, padding: int = 2,
+                    n_materials: int = 8, n_point_lights: int = 4, box_subdiv: int = 1) -> Scene:
+    """Closed 10x3x10 room (12 inward triangles) plus `n_boxes` axis-aligned
+    boxes with uniform positions inside and edges U[0.1, 1.0]; one chart per
+    face; 8 Lambertian materials with albedo U[0.1, 0.9]; one directional and
+    `n_point_lights` point lights with intensity U[5, 50]."""
+    rng = np.random.default_rng(seed)
+    mats = [solid_material(rng.uniform(0.1, 0.9, 3), name=f"m{i}") for i in range(n_materials)]
+    room_lo, room_hi = np.array([-5.0, 0.0, -5.0]), np.array([5.0, 3.0, 5.0])
+    patches = box_patches(0, room_lo, room_hi, inward=True)
+    mat_ids = [0]
+    for b in range(n_boxes):
+        size = rng.uniform(0.1, 1.0, 3)
+        lo = rng.uniform(room_lo, room_hi - size)
+        patches += box_patches(b + 1, lo, lo + size, inward=False, subdiv=box_subdiv)
+        mat_ids.append(int(rng.integers(0, n_materials)))
+    geoms = build_from_patches(patches, mat_ids, res, padding)
+    d = _normalize([rng.uniform(-0.5, 0.5), -1.0, rng.uniform(-0.5, 0.5)])
+    lights = [Light(type=DIRECTIONAL, direction=tuple(float(x) for x in d), intensity=3.0)]
+    for _ in range(n_point_lights):
+        pos = (rng.uniform(-4, 4), rng.uniform(1.5, 2.8), rng.uniform(-4, 4))
+        lights.append(Light(type=POINT, position=tuple(float(x) for x in pos), intensity=float(rng.uniform(5, 50))))
+    return Scene(geoms, mats, lights)
