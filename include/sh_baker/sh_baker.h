@@ -1,0 +1,369 @@
+// sh_baker/sh_baker.h - C++ mirror of sh-baker's bake API over the C ABI
+// (shb.h).  Header-only; link against libshb.so.
+//
+// Same names, structs, field order and argument meaning as the reference:
+//   Texture, Texture32F, Material, Geometry, Light, Scene   (src/scene.h:18-115)
+//   RasterConfig, SurfacePoint                              (src/rasterizer.h:12-23)
+//   BakeConfig, BakeResult                                  (src/baker.h:10-19)
+//   SHCoeffs, SHTexture                                     (src/sh_coeffs.h:10-23, src/saver.h:12-16)
+//   RasterizeScene, CreateValidityMask, DownsampleValidityMask (src/rasterizer.h:27-39)
+//   BakeSHLightMap, DownsampleSHTexture,
+//   DownsampleEnvironmentVisibilityTexture                  (src/baker.h:25-36)
+//   Dilate<T> for SHCoeffs, float, uint8_t                  (src/dilation.h:14-16)
+// Where the reference CHECK-fails these throw sh_baker::Error.  With Eigen
+// available the vector types are Eigen's; otherwise small POD stand-ins with
+// the same memory layout and accessors are used.
+#ifndef SH_BAKER_B200_SH_BAKER_H_
+#define SH_BAKER_B200_SH_BAKER_H_
+
+#include <cstdint>
+#include <cstdlib>
+#include <cstring>
+#include <filesystem>
+#include <type_traits>
+#include <optional>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../shb.h"
+
+#if __has_include(<Eigen/Dense>)
+#include <Eigen/Dense>
+#define SH_BAKER_HAS_EIGEN 1
+#endif
+
+namespace sh_baker {
+
+#ifdef SH_BAKER_HAS_EIGEN
+using Vector2f = Eigen::Vector2f;
+using Vector3f = Eigen::Vector3f;
+using Vector4f = Eigen::Vector4f;
+using Affine3f = Eigen::Affine3f;
+inline void affine_rows(const Affine3f& a, float out[12]) {
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 4; ++c) out[r * 4 + c] = a.matrix()(r, c);
+}
+#else
+template <int N>
+struct VecN {
+  float v[N];
+  VecN() { for (int i = 0; i < N; ++i) v[i] = 0.f; }
+  template <class... T>
+  VecN(T... xs) : v{static_cast<float>(xs)...} {}
+  float& operator[](int i) { return v[i]; }
+  float operator[](int i) const { return v[i]; }
+  float& x() { return v[0]; }
+  float& y() { return v[1]; }
+  float x() const { return v[0]; }
+  float y() const { return v[1]; }
+  template <int M = N, class = std::enable_if_t<(M > 2)>>
+  float z() const { return v[2]; }
+  template <int M = N, class = std::enable_if_t<(M > 3)>>
+  float w() const { return v[3]; }
+  static VecN Zero() { return VecN(); }
+};
+using Vector2f = VecN<2>;
+using Vector3f = VecN<3>;
+struct alignas(16) Vector4f : VecN<4> {
+  using VecN<4>::VecN;
+};
+struct Affine3f {
+  float m[12] = {1, 0, 0, 0, 0, 1, 0, 0, 0, 0, 1, 0};  // row-major [L | t]
+  static Affine3f Identity() { return Affine3f(); }
+};
+inline void affine_rows(const Affine3f& a, float out[12]) { std::memcpy(out, a.m, sizeof(a.m)); }
+#endif
+
+struct Error : std::runtime_error {
+  shb_status status;
+  Error(shb_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+inline void check(shb_status s) {
+  if (s != SHB_OK) throw Error(s, std::string("shb: ") + shb_last_error());
+}
+
+// ---- src/scene.h:18-115 ----------------------------------------------------
+
+struct Texture {
+  std::optional<std::filesystem::path> file_path;
+  uint32_t width = 0;
+  uint32_t height = 0;
+  uint32_t channels = 0;
+  std::vector<uint8_t> pixel_data;
+};
+
+struct Texture32F {
+  std::optional<std::filesystem::path> file_path;
+  uint32_t width = 0;
+  uint32_t height = 0;
+  uint32_t channels = 0;
+  std::vector<float> pixel_data;
+};
+
+struct Material {
+  std::string name;
+  Texture albedo;
+  Texture normal_texture;
+  Texture metallic_roughness_texture;
+  float emission_intensity = 0.0f;
+};
+
+struct Geometry {
+  std::vector<Vector3f> vertices;
+  std::vector<Vector3f> normals;
+  std::vector<Vector2f> texture_uvs;
+  std::vector<Vector2f> lightmap_uvs;
+  std::vector<Vector4f> tangents;
+  std::vector<uint32_t> indices;
+  int material_id = -1;
+  Affine3f transform = Affine3f::Identity();
+};
+
+struct Light {
+  enum class Type { Point, Directional, Spot, Area };
+  Type type = Type::Point;
+  Vector3f position = Vector3f(0.f, 0.f, 0.f);
+  Vector3f direction = Vector3f(0.f, 0.f, -1.f);
+  Vector3f color = Vector3f(1.f, 1.f, 1.f);
+  float intensity = 1.0f;
+  float cos_inner_cone = 1.0f;
+  float cos_outer_cone = 0.70710678118654752440f;
+  float area = 0.0f;
+  const Material* material = nullptr;
+  const Geometry* geometry = nullptr;
+  int geometry_index = -1;
+};
+
+struct Scene {
+  std::vector<Geometry> geometries;
+  std::vector<Material> materials;
+  std::vector<Light> lights;
+};
+
+// ---- src/rasterizer.h:12-23, src/baker.h:10-19, src/sh_coeffs.h ------------
+
+struct RasterConfig {
+  int width = 1024;
+  int height = 1024;
+  int supersample_scale = 1;
+};
+
+struct SurfacePoint {
+  Vector3f position = Vector3f(0.f, 0.f, 0.f);
+  Vector3f normal = Vector3f(0.f, 0.f, 0.f);
+  Vector4f tangent = Vector4f(0.f, 0.f, 0.f, 0.f);
+  int32_t material_id = -1;
+};
+static_assert(sizeof(SurfacePoint) == sizeof(shb_surface_point), "SurfacePoint layout");
+
+struct SHCoeffs {
+  Vector3f coeffs[9];
+};
+static_assert(sizeof(SHCoeffs) == 27 * sizeof(float), "SHCoeffs layout");
+
+struct SHTexture {
+  int width = 0;
+  int height = 0;
+  std::vector<SHCoeffs> pixels;
+};
+
+struct BakeConfig {
+  int samples = 128;
+  int bounces = 3;
+  int num_light_samples = 1;
+};
+
+struct BakeResult {
+  SHTexture sh_texture;
+  Texture32F environment_visibility_texture;
+};
+
+// ---- device plumbing ---------------------------------------------------------
+
+namespace detail {
+
+// One context per host thread, on device 0 (SHB_DEVICE overrides).
+inline shb_context* context() {
+  struct Holder {
+    shb_context* ctx = nullptr;
+    ~Holder() {
+      if (ctx) shb_context_destroy(ctx);
+    }
+  };
+  static thread_local Holder h;
+  if (!h.ctx) {
+    shb_options o{};
+    const char* d = std::getenv("SHB_DEVICE");
+    o.device = d ? std::atoi(d) : 0;
+    check(shb_context_create(&o, &h.ctx));
+  }
+  return h.ctx;
+}
+
+struct SceneHandle {
+  shb_scene* s = nullptr;
+  ~SceneHandle() { shb_scene_destroy(s); }
+};
+
+inline void upload(const Scene& scene, SceneHandle* out) {
+  std::vector<shb_geometry_desc> g(scene.geometries.size());
+  for (size_t i = 0; i < g.size(); ++i) {
+    const Geometry& G = scene.geometries[i];
+    shb_geometry_desc& d = g[i];
+    std::memset(&d, 0, sizeof(d));
+    d.vertices = G.vertices.empty() ? nullptr : reinterpret_cast<const float*>(G.vertices.data());
+    d.normals = G.normals.empty() ? nullptr : reinterpret_cast<const float*>(G.normals.data());
+    d.texture_uvs = G.texture_uvs.empty() ? nullptr : reinterpret_cast<const float*>(G.texture_uvs.data());
+    d.lightmap_uvs = G.lightmap_uvs.empty() ? nullptr : reinterpret_cast<const float*>(G.lightmap_uvs.data());
+    d.tangents = G.tangents.empty() ? nullptr : reinterpret_cast<const float*>(G.tangents.data());
+    d.vertex_count = (uint32_t)G.vertices.size();
+    d.indices = G.indices.data();
+    d.index_count = (uint32_t)G.indices.size();
+    d.material_id = G.material_id;
+    affine_rows(G.transform, d.transform);
+  }
+  std::vector<shb_material_desc> m(scene.materials.size());
+  for (size_t i = 0; i < m.size(); ++i) {
+    const Material& M = scene.materials[i];
+    m[i].albedo_pixels = M.albedo.pixel_data.empty() ? nullptr : M.albedo.pixel_data.data();
+    m[i].albedo_width = M.albedo.width;
+    m[i].albedo_height = M.albedo.height;
+    m[i].albedo_channels = M.albedo.channels;
+    m[i].emission_intensity = M.emission_intensity;
+  }
+  std::vector<shb_light_desc> l(scene.lights.size());
+  for (size_t i = 0; i < l.size(); ++i) {
+    const Light& L = scene.lights[i];
+    shb_light_desc& d = l[i];
+    d.type = (int32_t)L.type;
+    for (int k = 0; k < 3; ++k) {
+      d.position[k] = L.position[k];
+      d.direction[k] = L.direction[k];
+      d.color[k] = L.color[k];
+    }
+    d.intensity = L.intensity;
+    d.cos_inner_cone = L.cos_inner_cone;
+    d.cos_outer_cone = L.cos_outer_cone;
+    d.area = L.area;
+    d.geometry_index = L.geometry_index;
+    if (d.geometry_index < 0 && L.geometry) d.geometry_index = (int32_t)(L.geometry - scene.geometries.data());
+    d.material_index = L.material ? (int32_t)(L.material - scene.materials.data()) : -1;
+  }
+  shb_scene_desc desc{g.data(), (uint32_t)g.size(), m.data(), (uint32_t)m.size(), l.data(), (uint32_t)l.size()};
+  check(shb_scene_upload(context(), &desc, &out->s));
+}
+
+}  // namespace detail
+
+// ---- src/rasterizer.h:27-39 ------------------------------------------------
+
+inline std::vector<SurfacePoint> RasterizeScene(const Scene& scene, const RasterConfig& config) {
+  detail::SceneHandle s;
+  detail::upload(scene, &s);
+  std::vector<SurfacePoint> out((size_t)config.width * config.supersample_scale * config.height *
+                                config.supersample_scale);
+  shb_raster_config rc{config.width, config.height, config.supersample_scale};
+  check(shb_rasterize(s.s, &rc, reinterpret_cast<shb_surface_point*>(out.data()), nullptr));
+  return out;
+}
+
+inline std::vector<uint8_t> CreateValidityMask(const std::vector<SurfacePoint>& points) {
+  std::vector<uint8_t> mask(points.size());
+  if (points.empty()) return mask;
+  shb_gbuffer* g = nullptr;
+  check(shb_gbuffer_upload(detail::context(), reinterpret_cast<const shb_surface_point*>(points.data()),
+                           (int32_t)points.size(), 1, &g));
+  shb_status st = shb_validity_mask(detail::context(), g, mask.data(), 0);
+  shb_gbuffer_destroy(g);
+  check(st);
+  return mask;
+}
+
+inline std::vector<uint8_t> DownsampleValidityMask(const std::vector<uint8_t>& high_res_mask, int width,
+                                                   int height, int scale) {
+  if (high_res_mask.size() != (size_t)width * height * scale * scale)
+    throw Error(SHB_ERR_INVALID_ARG, "DownsampleValidityMask: size mismatch (CHECK_EQ in the reference)");
+  std::vector<uint8_t> mask((size_t)width * height, 0);
+  check(shb_downsample_validity_mask(detail::context(), high_res_mask.data(), width, height, scale, mask.data(), 0));
+  return mask;
+}
+
+// ---- src/baker.h:25-36 -----------------------------------------------------
+
+inline BakeResult BakeSHLightMap(const Scene& scene, const std::vector<SurfacePoint>& surface_points,
+                                 const RasterConfig& raster_config, const BakeConfig& config,
+                                 uint32_t seed = 12345) {
+  detail::SceneHandle s;
+  detail::upload(scene, &s);
+  const int W = raster_config.width * raster_config.supersample_scale;
+  const int H = raster_config.height * raster_config.supersample_scale;
+  BakeResult r;
+  r.sh_texture.width = W;
+  r.sh_texture.height = H;
+  r.sh_texture.pixels.resize((size_t)W * H);
+  r.environment_visibility_texture.width = W;
+  r.environment_visibility_texture.height = H;
+  r.environment_visibility_texture.pixel_data.resize((size_t)W * H);
+  shb_gbuffer* g = nullptr;
+  check(shb_gbuffer_upload(detail::context(), reinterpret_cast<const shb_surface_point*>(surface_points.data()), W,
+                           H, &g));
+  shb_raster_config rc{raster_config.width, raster_config.height, raster_config.supersample_scale};
+  shb_bake_config bc{};
+  bc.samples = config.samples;
+  bc.bounces = config.bounces;
+  bc.num_light_samples = config.num_light_samples;
+  bc.seed = seed;
+  bc.rng_mode = SHB_RNG_PHILOX;
+  shb_bake_output out{reinterpret_cast<float*>(r.sh_texture.pixels.data()),
+                      r.environment_visibility_texture.pixel_data.data(), 0, 0};
+  shb_status st = shb_bake(s.s, g, &rc, &bc, &out, nullptr);
+  shb_gbuffer_destroy(g);
+  check(st);
+  return r;
+}
+
+inline SHTexture DownsampleSHTexture(const SHTexture& input, int scale) {
+  SHTexture out;
+  out.width = input.width / scale;
+  out.height = input.height / scale;
+  if (scale <= 1) {
+    out.width = input.width;
+    out.height = input.height;
+  }
+  out.pixels.resize((size_t)out.width * out.height);
+  if (input.pixels.empty() || out.pixels.empty()) return out;
+  check(shb_downsample(detail::context(), reinterpret_cast<const float*>(input.pixels.data()), input.width,
+                       input.height, 27, scale, reinterpret_cast<float*>(out.pixels.data()), 0));
+  return out;
+}
+
+inline Texture32F DownsampleEnvironmentVisibilityTexture(const Texture32F& input, int scale) {
+  Texture32F out;
+  out.width = scale <= 1 ? input.width : input.width / scale;
+  out.height = scale <= 1 ? input.height : input.height / scale;
+  out.pixel_data.resize((size_t)out.width * out.height);
+  if (input.pixel_data.empty() || out.pixel_data.empty()) return out;
+  check(shb_downsample(detail::context(), input.pixel_data.data(), (int)input.width, (int)input.height, 1, scale,
+                       out.pixel_data.data(), 0));
+  return out;
+}
+
+// ---- src/dilation.h:14-16 --------------------------------------------------
+
+template <typename T>
+inline void Dilate(int width, int height, std::vector<T>& pixels, std::vector<uint8_t>& mask, int passes = 1) {
+  static_assert(std::is_same<T, SHCoeffs>::value || std::is_same<T, float>::value ||
+                    std::is_same<T, uint8_t>::value,
+                "Dilate is instantiated for SHCoeffs, float and uint8_t");
+  if (pixels.empty() || mask.empty() || pixels.size() != mask.size()) return;
+  int kind = std::is_same<T, SHCoeffs>::value ? SHB_DILATE_SH9
+             : std::is_same<T, float>::value  ? SHB_DILATE_F32
+                                              : SHB_DILATE_U8;
+  check(shb_dilate(detail::context(), kind, width, height, pixels.data(), mask.data(), passes, 0));
+}
+
+}  // namespace sh_baker
+
+#endif  // SH_BAKER_B200_SH_BAKER_H_

@@ -263,7 +263,16 @@ struct WaveArgs {
   int* cnt;
   float* sh_out;
   float* env_out;
+  int ext_cap;  // capacity of each extend queue
+  int sh_cap;   // capacity of the shadow queue
 };
+
+// Queue slot within capacity, else the error flag is raised and the ray dropped.
+__device__ __forceinline__ bool slot_ok(const WaveArgs& a, int slot, int cap) {
+  if (slot < cap) return true;
+  atomicOr(a.cnt + CNT_ERROR, ERR_QUEUE);
+  return false;
+}
 
 // ------------------------------------------------------------- generate --
 __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
@@ -311,14 +320,14 @@ __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
       }
       if (active && !ok) a.nee_li[p * a.nls + j] = make_float4(0.f, 0.f, 0.f, 0.f);
       int slot = warp_push(a.cnt + CNT_SHADOW, ok);
-      if (ok) {
+      if (ok && slot_ok(a, slot, a.sh_cap)) {
         a.sh.o[slot] = make_float4(P0.x, P0.y, P0.z, e.tfar);
         a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float((uint32_t)(p * a.nls + j)));
         a.sh.c[slot] = make_float4(0.f, 0.f, 0.f, __uint_as_float(1u));
       }
     }
     int slot = warp_push(a.cnt + CNT_EXT0, active);
-    if (active) {
+    if (active && slot_ok(a, slot, a.ext_cap)) {
       a.ext[0].o[slot] = make_float4(o.x, o.y, o.z, __uint_as_float((uint32_t)p));
       a.ext[0].d[slot] = make_float4(dw.x, dw.y, dw.z, __uint_as_float(1u));
       a.ext[0].beta[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
@@ -329,7 +338,7 @@ __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
 // --------------------------------------------------------------- shade ---
 // One path vertex of Trace (src/baker.cpp:70-149) in throughput form.
 __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int depth, int can_extend) {
-  const int n = a.cnt[cur];
+  const int n = min(a.cnt[cur], a.ext_cap);
   const int nxt = cur ^ 1;
   const int warps = gridDim.x * (blockDim.x >> 5);
   const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -382,7 +391,7 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
     if (a.sc.has_alpha) {
       bool tr = hit && alpha < 1.0f && can_extend;
       int slot = warp_push(a.cnt + nxt, tr);
-      if (tr) {
+      if (tr && slot_ok(a, slot, a.ext_cap)) {
         f3 hp = pos + d * 0.001f;
         f3 bt = beta * (1.0f - alpha);
         qn.o[slot] = make_float4(hp.x, hp.y, hp.z, __uint_as_float(path));
@@ -425,7 +434,7 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
         }
       }
       int slot = warp_push(a.cnt + CNT_SHADOW, ok);
-      if (ok) {
+      if (ok && slot_ok(a, slot, a.sh_cap)) {
         a.sh.o[slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, e.tfar);
         a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float(path));
         a.sh.c[slot] = make_float4(c.x, c.y, c.z, __uint_as_float(0u));
@@ -456,7 +465,7 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
       }
     }
     int slot = warp_push(a.cnt + nxt, ext);
-    if (ext) {
+    if (ext && slot_ok(a, slot, a.ext_cap)) {
       qn.o[slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, __uint_as_float(path));
       qn.d[slot] = make_float4(nd.x, nd.y, nd.z, __uint_as_float(2u * vertex));
       qn.beta[slot] = make_float4(nb.x, nb.y, nb.z, 0.f);
@@ -687,6 +696,8 @@ shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int 
   a.cnt = cnt;
   a.sh_out = d_sh;
   a.env_out = d_env;
+  a.ext_cap = (int)ext_cap;
+  a.sh_cap = (int)sh_cap;
 
   const BvhView bvh = s->bvh();
   const int tgrid = traversal_grid(c->device);
@@ -719,7 +730,7 @@ shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int 
         cudaEventCreate(&pe.b);
         cudaEventRecord(pe.a, st);
       }
-      launch_extend(st, tgrid, bvh, a.ext[cur], cnt + cur, a.hits, cnt + CNT_FETCH_EXT, cnt + CNT_ERROR, c64);
+      launch_extend(st, tgrid, bvh, a.ext[cur], cnt + cur, a.ext_cap, a.hits, cnt + CNT_FETCH_EXT, cnt + CNT_ERROR, c64);
       if (c->profiling) {
         cudaEventRecord(pe.b, st);
         timed.push_back(pe);
@@ -731,7 +742,7 @@ shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int 
         cudaEventCreate(&ps.b);
         cudaEventRecord(ps.a, st);
       }
-      launch_shadow(st, tgrid, bvh, a.sh, cnt + CNT_SHADOW, a.path_L, a.nee_li, cnt + CNT_FETCH_SHADOW,
+      launch_shadow(st, tgrid, bvh, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, cnt + CNT_FETCH_SHADOW,
                     cnt + CNT_ERROR, c64);
       if (c->profiling) {
         cudaEventRecord(ps.b, st);
@@ -781,7 +792,7 @@ shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int 
     stats->shadow_launches = sh_launches;
   }
   if (err) {
-    set_error(err & ERR_STACK ? "traversal stack overflow" : "ray queue overflow");
+    set_error(std::string("bounded device failure:") + (err & ERR_STACK ? " traversal stack overflow" : "") + (err & ERR_QUEUE ? " ray queue overflow" : "") + (err & ERR_ITER ? " traversal iteration limit" : ""));
     return SHB_ERR_INTERNAL;
   }
   return SHB_OK;

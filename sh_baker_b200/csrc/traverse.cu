@@ -113,7 +113,14 @@ __device__ bool traverse(const BvhView& bvh, const TravRay& r, float tnear, floa
   float tmax = tfar;
   bool hit = false;
   const uint4* nodes = reinterpret_cast<const uint4*>(bvh.nodes);
+  // Every child index is larger than its parent's, so the walk ends; the
+  // bound only turns a corrupted tree into an error flag.
+  uint32_t iters = 0;
   while (true) {
+    if (++iters > (1u << 22)) {
+      atomicOr(err, ERR_ITER);
+      break;
+    }
     while (tg_hits) {
       int k = __ffs(tg_hits) - 1;
       tg_hits &= tg_hits - 1;
@@ -206,10 +213,10 @@ __device__ __forceinline__ void load_ray(TravRay& r, float4 o, float4 d) {
   prepare(r);
 }
 
-__global__ void __launch_bounds__(kTravThreads) k_extend(BvhView bvh, ExtQueue q, const int* __restrict__ n_ptr,
+__global__ void __launch_bounds__(kTravThreads) k_extend(BvhView bvh, ExtQueue q, const int* __restrict__ n_ptr, int cap,
                                                         float4* __restrict__ hits, int* fetch, int* err,
                                                         Counters64* stats) {
-  const int n = *n_ptr;
+  const int n = min(*n_ptr, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&stats->extend_rays, (unsigned long long)n);
   const int lane = threadIdx.x & 31;
   while (true) {
@@ -229,10 +236,10 @@ __global__ void __launch_bounds__(kTravThreads) k_extend(BvhView bvh, ExtQueue q
   }
 }
 
-__global__ void __launch_bounds__(kTravThreads) k_shadow(BvhView bvh, ShadowQueue q, const int* __restrict__ n_ptr,
+__global__ void __launch_bounds__(kTravThreads) k_shadow(BvhView bvh, ShadowQueue q, const int* __restrict__ n_ptr, int cap,
                                                         float4* __restrict__ path_L, float4* __restrict__ nee_li,
                                                         int* fetch, int* err, Counters64* stats) {
-  const int n = *n_ptr;
+  const int n = min(*n_ptr, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&stats->shadow_rays, (unsigned long long)n);
   const int lane = threadIdx.x & 31;
   while (true) {
@@ -294,14 +301,14 @@ int traversal_grid(int device) {
   return sms * per_sm;
 }
 
-void launch_extend(cudaStream_t st, int grid, const BvhView& bvh, ExtQueue q, const int* n, float4* hits, int* fetch,
+void launch_extend(cudaStream_t st, int grid, const BvhView& bvh, ExtQueue q, const int* n, int cap, float4* hits, int* fetch,
                    int* err, Counters64* stats) {
-  k_extend<<<grid, kTravThreads, 0, st>>>(bvh, q, n, hits, fetch, err, stats);
+  k_extend<<<grid, kTravThreads, 0, st>>>(bvh, q, n, cap, hits, fetch, err, stats);
 }
 
-void launch_shadow(cudaStream_t st, int grid, const BvhView& bvh, ShadowQueue q, const int* n, float4* path_L,
+void launch_shadow(cudaStream_t st, int grid, const BvhView& bvh, ShadowQueue q, const int* n, int cap, float4* path_L,
                    float4* nee_li, int* fetch, int* err, Counters64* stats) {
-  k_shadow<<<grid, kTravThreads, 0, st>>>(bvh, q, n, path_L, nee_li, fetch, err, stats);
+  k_shadow<<<grid, kTravThreads, 0, st>>>(bvh, q, n, cap, path_L, nee_li, fetch, err, stats);
 }
 
 void launch_closest_rays(cudaStream_t st, const BvhView& bvh, const shb_ray* rays, int64_t n, float4* hits, int* err) {

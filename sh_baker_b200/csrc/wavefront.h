@@ -39,7 +39,7 @@ enum CounterSlot {
   CNT_ERROR = 5,
   CNT_COUNT = 8
 };
-enum ErrorBits : int { ERR_STACK = 1, ERR_QUEUE = 2 };
+enum ErrorBits : int { ERR_STACK = 1, ERR_QUEUE = 2, ERR_ITER = 4 };
 
 struct Counters64 {
   unsigned long long extend_rays;
@@ -47,9 +47,9 @@ struct Counters64 {
 };
 
 // Launch helpers for the persistent traversal kernels (traverse.cu).
-void launch_extend(cudaStream_t st, int grid, const BvhView& bvh, ExtQueue q, const int* n, float4* hits,
+void launch_extend(cudaStream_t st, int grid, const BvhView& bvh, ExtQueue q, const int* n, int cap, float4* hits,
                    int* fetch, int* err, Counters64* stats);
-void launch_shadow(cudaStream_t st, int grid, const BvhView& bvh, ShadowQueue q, const int* n, float4* path_L,
+void launch_shadow(cudaStream_t st, int grid, const BvhView& bvh, ShadowQueue q, const int* n, int cap, float4* path_L,
                    float4* nee_li, int* fetch, int* err, Counters64* stats);
 void launch_closest_rays(cudaStream_t st, const BvhView& bvh, const shb_ray* rays, int64_t n, float4* hits,
                          int* err);

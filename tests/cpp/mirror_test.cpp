@@ -1,0 +1,144 @@
+// The reference's own unit tests, restated against the C++ mirror
+// (include/sh_baker/sh_baker.h) so they run on the CUDA library:
+//   src/rasterizer_test.cpp:7-126, src/dilation_test.cpp:11-58,
+//   src/baker_test.cpp:10-88.
+// Exit status 0 when every check passes.
+#include <cmath>
+#include <cstdio>
+
+#include "sh_baker/sh_baker.h"
+
+using namespace sh_baker;
+
+static int failures = 0;
+#define EXPECT(cond)                                                  \
+  do {                                                                \
+    if (!(cond)) {                                                    \
+      std::printf("FAILED %s:%d: %s\n", __FILE__, __LINE__, #cond);   \
+      ++failures;                                                     \
+    }                                                                 \
+  } while (0)
+
+static Geometry Quad() {
+  Geometry quad;
+  quad.material_id = 0;
+  quad.vertices = {Vector3f(-1, -1, 0), Vector3f(1, -1, 0), Vector3f(1, 1, 0), Vector3f(-1, 1, 0)};
+  quad.normals = {Vector3f(0, 0, 1), Vector3f(0, 0, 1), Vector3f(0, 0, 1), Vector3f(0, 0, 1)};
+  quad.texture_uvs = {Vector2f(0, 0), Vector2f(1, 0), Vector2f(1, 1), Vector2f(0, 1)};
+  quad.lightmap_uvs = quad.texture_uvs;
+  quad.tangents = {Vector4f(1, 0, 0, 1), Vector4f(1, 0, 0, 1), Vector4f(1, 0, 0, 1), Vector4f(1, 0, 0, 1)};
+  quad.indices = {0, 1, 2, 0, 2, 3};
+  return quad;
+}
+
+static void RasterizeQuad() {
+  Scene scene;
+  scene.geometries.push_back(Quad());
+  scene.materials.push_back(Material{});
+  RasterConfig config;
+  config.width = 4;
+  config.height = 4;
+  std::vector<SurfacePoint> result = RasterizeScene(scene, config);
+  EXPECT(result.size() == 16);
+  for (int i = 0; i < 16; ++i) EXPECT(result[i].material_id >= 0);
+  EXPECT(std::fabs(result[5].position[0] + 0.25f) < 0.001f);
+  EXPECT(std::fabs(result[5].position[1] + 0.25f) < 0.001f);
+  EXPECT(std::fabs(result[5].normal[2] - 1.0f) < 0.001f);
+  config.supersample_scale = 2;
+  result = RasterizeScene(scene, config);
+  EXPECT(result.size() == 64);
+  for (int i = 0; i < 64; ++i) EXPECT(result[i].material_id >= 0);
+}
+
+static void Masks() {
+  std::vector<SurfacePoint> points(3);
+  points[0].material_id = 0;
+  points[1].material_id = -1;
+  points[2].material_id = 0;
+  std::vector<uint8_t> mask = CreateValidityMask(points);
+  EXPECT(mask.size() == 3 && mask[0] == 1 && mask[1] == 0 && mask[2] == 1);
+  std::vector<uint8_t> hi(16, 0);
+  hi[2] = hi[8] = hi[9] = hi[12] = hi[13] = hi[15] = 1;
+  std::vector<uint8_t> lo = DownsampleValidityMask(hi, 2, 2, 2);
+  EXPECT(lo.size() == 4 && lo[0] == 0 && lo[1] == 1 && lo[2] == 1 && lo[3] == 1);
+}
+
+static void Dilation() {
+  std::vector<SHCoeffs> pixels(9);
+  std::vector<uint8_t> mask(9, 0);
+  mask[4] = 1;
+  pixels[4].coeffs[0] = Vector3f(1.0f, 0.0f, 0.0f);
+  Dilate(3, 3, pixels, mask, 1);
+  EXPECT(mask[1] == 1 && std::fabs(pixels[1].coeffs[0][0] - 1.0f) < 0.001f);
+  EXPECT(mask[0] == 1 && std::fabs(pixels[0].coeffs[0][0] - 1.0f) < 0.001f);
+  std::vector<SHCoeffs> p2(9);
+  std::vector<uint8_t> m2(9, 0);
+  m2[3] = m2[5] = 1;
+  p2[3].coeffs[0] = Vector3f(1.0f, 0.0f, 0.0f);
+  p2[5].coeffs[0] = Vector3f(0.0f, 0.0f, 1.0f);
+  Dilate(3, 3, p2, m2, 1);
+  EXPECT(m2[4] == 1 && std::fabs(p2[4].coeffs[0][0] - 0.5f) < 0.001f && std::fabs(p2[4].coeffs[0][2] - 0.5f) < 0.001f);
+  std::vector<float> f(9, 0.f);
+  std::vector<uint8_t> m3(9, 0);
+  m3[4] = 1;
+  f[4] = 2.0f;
+  Dilate(3, 3, f, m3, 1);
+  EXPECT(m3[0] == 1 && f[0] == 2.0f);
+}
+
+static void BakeSimpleQuad() {
+  Scene scene;
+  Geometry quad = Quad();
+  quad.tangents.clear();
+  scene.geometries.push_back(quad);
+  Material mat;
+  mat.name = "white";
+  mat.albedo.pixel_data = {255, 255, 255, 255};
+  mat.albedo.width = 1;
+  mat.albedo.height = 1;
+  mat.albedo.channels = 4;
+  scene.materials.push_back(mat);
+  Light light;
+  light.type = Light::Type::Directional;
+  light.direction = Vector3f(0, 0, -1);
+  light.color = Vector3f(1, 1, 1);
+  light.intensity = 1.0f;
+  scene.lights.push_back(light);
+  std::vector<SurfacePoint> surface_points(16);
+  RasterConfig raster_config;
+  raster_config.width = 4;
+  raster_config.height = 4;
+  surface_points[5].material_id = 0;
+  surface_points[5].position = Vector3f(-0.25f, -0.25f, 0.0f);
+  surface_points[5].normal = Vector3f(0.0f, 0.0f, 1.0f);
+  surface_points[5].tangent = Vector4f(1.0f, 0.0f, 0.0f, 1.0f);
+  BakeConfig config;
+  config.samples = 64;
+  config.bounces = 0;
+  BakeResult output = BakeSHLightMap(scene, surface_points, raster_config, config);
+  EXPECT(output.sh_texture.pixels[5].coeffs[0][0] > 0.1f);
+
+  SHTexture input;
+  input.width = 2;
+  input.height = 2;
+  input.pixels.resize(4);
+  for (auto& p : input.pixels)
+    for (auto& c : p.coeffs) c = Vector3f(1.0f, 1.0f, 1.0f);
+  SHTexture ds = DownsampleSHTexture(input, 2);
+  EXPECT(ds.width == 1 && ds.height == 1 && ds.pixels.size() == 1);
+  for (int c = 0; c < 9; ++c) EXPECT(ds.pixels[0].coeffs[c][0] == 1.0f);
+}
+
+int main() {
+  try {
+    RasterizeQuad();
+    Masks();
+    Dilation();
+    BakeSimpleQuad();
+  } catch (const std::exception& e) {
+    std::printf("exception: %s\n", e.what());
+    return 2;
+  }
+  std::printf("%s (%d failures)\n", failures ? "FAILED" : "OK", failures);
+  return failures ? 1 : 0;
+}

@@ -126,7 +126,8 @@ def test_unit_quad_gpu_equals_oracle_philox(gpu_ctx):
 
 
 def small_room(res=32, seed=2):
-    return scenes.procedural_room(seed=seed, res=res)
+    # few boxes so that one chart per face fits a small atlas
+    return scenes.procedural_room(seed=seed, n_boxes=max(2, res // 5), res=res)
 
 
 def test_room_gpu_matches_oracle_philox(gpu_ctx):
@@ -204,16 +205,18 @@ def test_all_light_types_and_alpha_match_oracle(gpu_ctx):
 
 
 def test_bake_rejects_bad_arguments(gpu_ctx):
-    sc = small_room(16)
+    sc = small_room(32)
     pts = O.OracleScene(sc).rasterize(16, 16, 1)
     with pytest.raises(Exception, match="INVALID_ARG"):
         api.BakeSHLightMap(sc, pts, api.RasterConfig(16, 16, 1), api.BakeConfig(samples=0), ctx=gpu_ctx)
+    # a 16x16 G-buffer baked with a raster config of 32x16 texels
+    g = api.GBuffer.from_points(gpu_ctx, pts, 16, 16)
     with pytest.raises(Exception, match="INVALID_ARG"):
-        api.BakeSHLightMap(sc, pts[: 16 * 8], api.RasterConfig(16, 8, 2), api.BakeConfig(samples=4), ctx=gpu_ctx)
+        api.BakeSHLightMap(sc, g, api.RasterConfig(16, 8, 2), api.BakeConfig(samples=4), ctx=gpu_ctx)
 
 
 def test_bake_all_invalid_texels(gpu_ctx):
-    sc = small_room(16)
+    sc = small_room(32)
     from sh_baker_b200.scene import surface_points_empty
     pts = surface_points_empty(16 * 16)
     out = api.BakeSHLightMap(sc, pts, api.RasterConfig(16, 16, 1), api.BakeConfig(samples=4), ctx=gpu_ctx)

@@ -91,7 +91,7 @@ def test_rasterize_rejects_missing_tangents(gpu_ctx):
 
 
 def test_validity_mask_and_downsample(gpu_ctx):
-    sc = scenes.procedural_room(seed=2, res=64)
+    sc = scenes.procedural_room(seed=2, n_boxes=40, res=64)
     pts = O.OracleScene(sc).rasterize(64, 64, 3)
     m = api.CreateValidityMask(pts, ctx=gpu_ctx)
     np.testing.assert_array_equal(m, O.validity_mask(pts))
