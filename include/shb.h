@@ -280,6 +280,24 @@ SHB_API shb_status shb_dilate(shb_context* ctx, int32_t kind, int32_t width,
                               int32_t height, void* pixels, uint8_t* mask,
                               int32_t passes, int32_t device_ptrs);
 
+/* Dilation that allocates nothing.  No counterpart in the reference: it
+ * exists for callers that cannot allocate device memory while they run (a
+ * host application that owns and pre-reserves the GPU's memory, or a path
+ * with a deadline where cudaMalloc's implicit synchronisation is not
+ * acceptable).  Same passes and results as shb_dilate on device pointers
+ * (pixels and mask on the context's device, updated in place).  The
+ * ping-pong scratch lives in one fixed 16 MiB array inside the library,
+ * which every GPU that loads the library holds until the process exits.  At
+ * most about 153,000 texels of SH9, 3.3 million of float or 8.3 million of
+ * uint8, and at most 4096 passes; larger requests return
+ * SHB_ERR_INVALID_ARG.  The first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  All
+ * calls share the array, so calls that overlap on the GPU (other host
+ * threads or streams) race and must be serialised by the caller. */
+SHB_API shb_status shb_dilate_noalloc(shb_context* ctx, int32_t kind, int32_t width,
+                                      int32_t height, void* pixels, uint8_t* mask,
+                                      int32_t passes);
+
 /* ---- the CLI's bake sequence (src/main.cpp:91-163) -------------------- */
 
 typedef struct shb_pipeline_config {

@@ -139,6 +139,7 @@ SIGNATURES = {
     "shb_dilate": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_int32, C.c_int32]),
     "shb_find_occlusion": (C.c_int, [vp, vp, C.c_int64, vp, C.c_int32]),
     "shb_bake_pipeline": (C.c_int, [vp, C.POINTER(PipelineConfig), vp, vp, vp, C.POINTER(BakeStats)]),
+    "shb_dilate_noalloc": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_int32]),
 }
 
 _lib = None

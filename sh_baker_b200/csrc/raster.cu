@@ -4,6 +4,8 @@
 // and src/dilation.cpp.
 #include <cub/cub.cuh>
 
+#include <mutex>
+
 #include "shb_internal.h"
 #include "shb_math.cuh"
 
@@ -455,3 +457,112 @@ shb_status dilate_device(shb_context* c, int kind, int w, int h, void* pixels, u
 }
 
 }  // namespace shb
+
+// ============================================= allocation-free dilation ====
+//
+// Some callers cannot allocate device memory while they run: a host
+// application that owns the GPU's memory budget and reserves all of it up
+// front (an editor or content tool baking lightmaps beside its renderer),
+// and callers on a deadline path, where cudaMalloc's implicit device-wide
+// synchronisation and unpredictable latency are not acceptable.  For them
+// shb_dilate_noalloc runs the same dilation passes as shb_dilate, but the
+// ping-pong copy of the pixels and mask and the per-pass change flags live
+// in the fixed array below.  The library holds that array on every GPU that
+// loads it until the process exits.
+
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(16) << 20;  // 16 MiB
+constexpr int kNoAllocMaxPasses = 4096;
+constexpr size_t kNoAllocFlagBytes = sizeof(int) * kNoAllocMaxPasses;  // 16 KiB
+constexpr int kNoAllocMaxDevices = 64;
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+std::mutex g_noalloc_mutex;
+void* g_noalloc_device_addr[kNoAllocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on `device` (current).  The name is
+// only a host-side stand-in for the symbol, so the address comes from
+// cudaGetSymbolAddress once per device and is cached.
+shb_status noalloc_scratch(int device, unsigned char** out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) {
+    shb::set_error("shb_dilate_noalloc: device ordinal out of range");
+    return SHB_ERR_INVALID_ARG;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_device_addr[device]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return shb::cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+    g_noalloc_device_addr[device] = p;
+  }
+  *out = static_cast<unsigned char*>(g_noalloc_device_addr[device]);
+  return SHB_OK;
+}
+
+}  // namespace
+
+extern "C" SHB_API shb_status shb_dilate_noalloc(shb_context* ctx, int32_t kind, int32_t width, int32_t height,
+                                                 void* pixels, uint8_t* mask, int32_t passes) {
+  using namespace shb;
+  if (!ctx) {
+    set_error("ctx is NULL");
+    return SHB_ERR_INVALID_ARG;
+  }
+  if (kind < SHB_DILATE_SH9 || kind > SHB_DILATE_U8) {
+    set_error("bad dilate kind");
+    return SHB_ERR_INVALID_ARG;
+  }
+  if (width <= 0 || height <= 0 || passes <= 0) return SHB_OK;  // nothing to do, as Dilate<T>
+  if (!pixels || !mask) {
+    set_error("NULL argument");
+    return SHB_ERR_INVALID_ARG;
+  }
+  const int64_t n = (int64_t)width * height;
+  const int ch = kind == SHB_DILATE_SH9 ? 27 : 1;
+  const size_t esz = kind == SHB_DILATE_U8 ? 1 : 4;
+  const size_t pbytes = esz * (size_t)n * ch;
+  const size_t pbytes_aligned = (pbytes + 255) & ~size_t(255);
+  const size_t need = kNoAllocFlagBytes + pbytes_aligned + (size_t)n;
+  if (passes > kNoAllocMaxPasses) {
+    set_error("shb_dilate_noalloc: at most " + std::to_string(kNoAllocMaxPasses) + " passes");
+    return SHB_ERR_INVALID_ARG;
+  }
+  if (need > kNoAllocScratchBytes) {
+    set_error("shb_dilate_noalloc: " + std::to_string(width) + "x" + std::to_string(height) + " texels need " +
+              std::to_string(need) + " bytes of scratch; the fixed array holds " +
+              std::to_string(kNoAllocScratchBytes) + " (about 153,000 texels of SH9, 3.3 M of float, 8.3 M of uint8)");
+    return SHB_ERR_INVALID_ARG;
+  }
+  SHB_CUDA(cudaSetDevice(ctx->device));
+  unsigned char* base = nullptr;
+  SHB_TRY(noalloc_scratch(ctx->device, &base));
+  int* changed = reinterpret_cast<int*>(base);
+  void* pbuf = base + kNoAllocFlagBytes;
+  uint8_t* mbuf = base + kNoAllocFlagBytes + pbytes_aligned;
+  cudaStream_t st = ctx->stream;
+  // the array keeps the previous call's contents: the change flags must start at zero
+  SHB_CUDA(cudaMemsetAsync(changed, 0, sizeof(int) * (size_t)passes, st));
+  void* bufs[2] = {pixels, pbuf};
+  uint8_t* masks[2] = {mask, mbuf};
+  const int64_t work = n * ch;
+  for (int p = 0; p < passes; ++p) {
+    int src = p & 1, dst = src ^ 1;
+    if (kind == SHB_DILATE_U8)
+      k_dilate<uint8_t><<<grid_for(work), kThreads, 0, st>>>((const uint8_t*)bufs[src], masks[src],
+                                                             (uint8_t*)bufs[dst], masks[dst], width, height, ch,
+                                                             changed, p);
+    else
+      k_dilate<float><<<grid_for(work), kThreads, 0, st>>>((const float*)bufs[src], masks[src], (float*)bufs[dst],
+                                                           masks[dst], width, height, ch, changed, p);
+    count_launch(ctx);
+  }
+  if (passes & 1) {
+    SHB_CUDA(cudaMemcpyAsync(pixels, bufs[1], pbytes, cudaMemcpyDeviceToDevice, st));
+    SHB_CUDA(cudaMemcpyAsync(mask, masks[1], (size_t)n, cudaMemcpyDeviceToDevice, st));
+  }
+  SHB_CUDA(cudaGetLastError());
+  SHB_CUDA(cudaStreamSynchronize(st));
+  return SHB_OK;
+}
