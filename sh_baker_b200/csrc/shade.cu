@@ -653,7 +653,7 @@ shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int 
   SHB_CUDA(cudaStreamSynchronize(st));
 
   // wave sizing: paths per wave, queue capacity per depth
-  const int64_t kPathsPerWave = 1 << 22;
+  const int64_t kPathsPerWave = 1 << 23;
   int64_t tex_per_wave = kPathsPerWave / spp;
   if (tex_per_wave < 1) tex_per_wave = 1;
   int64_t mult = 1;

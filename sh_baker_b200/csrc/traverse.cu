@@ -2,13 +2,15 @@
 // BVH; replaces rtcIntersect1 (src/occlusion.cpp:37) for path rays and for
 // shadow rays (src/light.cpp:173,275).
 //
-// Persistent kernels: a grid sized to fill every SM once; each warp takes
-// 32 queue entries at a time from an atomic counter until the queue (whose
-// length lives in device memory) is drained.  Children are visited in the
-// ray-octant order of their slots; the watertight triangle test (Woop,
-// Benthin, Wald 2013) is written with explicit round-to-nearest intrinsics
-// so it rounds exactly like the CPU restatement even though this file is
-// compiled with FMA contraction enabled for the box tests.
+// Persistent kernels with per-lane ray replacement: the grid fills every SM
+// once; a lane whose ray finishes takes the next queue entry (one atomic per
+// warp for all lanes that refill), so lanes do not wait for the slowest ray
+// of a batch.  Within a ray, children are visited in the ray-octant order of
+// their slots; triangle groups are postponed on the stack while too few
+// lanes of the warp want to test triangles (Ylitie, Karras, Laine 2017).
+// The watertight triangle test (Woop, Benthin, Wald 2013) uses explicit
+// round-to-nearest intrinsics so it rounds exactly like the CPU restatement
+// even though this file is compiled with FMA contraction for the box tests.
 #include "wavefront.h"
 
 namespace shb {
@@ -17,6 +19,9 @@ namespace {
 
 constexpr int kStack = 64;
 constexpr int kTravThreads = 128;
+constexpr int kPostpone = 6;        // fewer lanes than this on triangles: postpone them
+constexpr uint32_t kNodeGroup = 0x80000000u;
+constexpr uint32_t kMaxIters = 1u << 22;
 
 struct TravRay {
   float ox, oy, oz, dx, dy, dz;
@@ -100,107 +105,133 @@ __device__ __forceinline__ float byte_f(uint32_t w, int k) {
   return __uint_as_float(0x4B000000u | ((w >> (8 * k)) & 0xFFu)) - 8388608.0f;
 }
 
-// Returns true on a hit; for ANY the first hit ends the walk.
-template <bool ANY>
-__device__ bool traverse(const BvhView& bvh, const TravRay& r, float tnear, float tfar, float& t_out, float& u_out,
-                         float& v_out, uint32_t& prim_out, int* err) {
-  if (bvh.node_count == 0) return false;
-  uint2 stack[kStack];
-  int sp = 0;
+// Traversal state of one ray.  Groups are (base, bits): a node group has
+// kNodeGroup set, the internal-child mask in bits 8..15 and the remaining
+// hit slots (in ray-octant order) in bits 0..7; a triangle group has the
+// remaining triangle bits 0..23.
+struct Walk {
+  TravRay r;
+  float tnear, tmax;
+  uint2 G, T;
+  int sp;
+  uint32_t iters;
+  bool hit;
+  float u, v;
+  uint32_t prim;
+};
+
+__device__ __forceinline__ void walk_init(Walk& w, const BvhView& bvh, float tnear, float tfar) {
+  w.tnear = tnear;
+  w.tmax = tfar;
+  w.G = bvh.node_count ? make_uint2(0u, kNodeGroup | (1u << 8) | (1u << w.r.oct)) : make_uint2(0u, 0u);
+  w.T = make_uint2(0u, 0u);
+  w.sp = 0;
+  w.iters = 0;
+  w.hit = false;
+  w.u = w.v = 0.f;
+  w.prim = kMissPrim;
+}
+
+// Tests the 8 children of `node`; returns the internal children as a node
+// group and the hit leaf triangles as a triangle group.
+__device__ __forceinline__ void intersect_node(const BvhView& bvh, const Walk& w, uint32_t node, uint2& Gn,
+                                               uint2& Tn) {
+  const TravRay& r = w.r;
+  const uint4* np = reinterpret_cast<const uint4*>(bvh.nodes) + 5 * (size_t)node;
+  uint4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
+  uint32_t eim = n0.w;
+  float sx = __uint_as_float((eim & 0xFFu) << 23) * r.ix;
+  float sy = __uint_as_float(((eim >> 8) & 0xFFu) << 23) * r.iy;
+  float sz = __uint_as_float(((eim >> 16) & 0xFFu) << 23) * r.iz;
+  float ax = (__uint_as_float(n0.x) - r.ox) * r.ix;
+  float ay = (__uint_as_float(n0.y) - r.oy) * r.iy;
+  float az = (__uint_as_float(n0.z) - r.oz) * r.iz;
+  uint32_t imask = eim >> 24;
   const uint32_t oct = r.oct;
-  uint32_t ng_base = 0, ng_hits = 1u << oct, ng_imask = 1u;
-  uint32_t tg_base = 0, tg_hits = 0;
-  float tmax = tfar;
-  bool hit = false;
-  const uint4* nodes = reinterpret_cast<const uint4*>(bvh.nodes);
-  // Every child index is larger than its parent's, so the walk ends; the
-  // bound only turns a corrupted tree into an error flag.
-  uint32_t iters = 0;
-  while (true) {
-    if (++iters > (1u << 22)) {
-      atomicOr(err, ERR_ITER);
-      break;
-    }
-    while (tg_hits) {
-      int k = __ffs(tg_hits) - 1;
-      tg_hits &= tg_hits - 1;
-      const float4* tp = bvh.tris + 3 * (size_t)(tg_base + k);
-      float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-      float t, u, v;
-      if (tri_test(r, a, b, c, tnear, tmax, t, u, v)) {
-        hit = true;
-        tmax = t;
-        t_out = t;
-        u_out = u;
-        v_out = v;
-        prim_out = __float_as_uint(a.w);
-        if (ANY) return true;
-      }
-    }
-    if (ng_hits == 0) {
-      if (sp == 0) break;
-      --sp;
-      ng_base = stack[sp].x;
-      ng_hits = stack[sp].y & 0xFFu;
-      ng_imask = stack[sp].y >> 8;
-    }
-    int bpos = __ffs(ng_hits) - 1;
-    ng_hits &= ng_hits - 1;
-    uint32_t slot = (uint32_t)bpos ^ oct;
-    uint32_t node = ng_base + __popc(ng_imask & ((1u << slot) - 1u));
-    if (ng_hits) {
-      if (sp < kStack) {
-        stack[sp++] = make_uint2(ng_base, ng_hits | (ng_imask << 8));
-      } else {
-        atomicOr(err, ERR_STACK);
-      }
-    }
-    const uint4* np = nodes + 5 * (size_t)node;
-    uint4 n0 = __ldg(np), n1 = __ldg(np + 1), n2 = __ldg(np + 2), n3 = __ldg(np + 3), n4 = __ldg(np + 4);
-    float px = __uint_as_float(n0.x), py = __uint_as_float(n0.y), pz = __uint_as_float(n0.z);
-    uint32_t eim = n0.w;
-    float sx = __uint_as_float((eim & 0xFFu) << 23) * r.ix;
-    float sy = __uint_as_float(((eim >> 8) & 0xFFu) << 23) * r.iy;
-    float sz = __uint_as_float(((eim >> 16) & 0xFFu) << 23) * r.iz;
-    float ax = (px - r.ox) * r.ix, ay = (py - r.oy) * r.iy, az = (pz - r.oz) * r.iz;
-    uint32_t imask = eim >> 24;
-    // near / far quantised planes per axis (octant select)
-    uint32_t lx0 = n2.x, lx1 = n2.y, ly0 = n2.z, ly1 = n2.w, lz0 = n3.x, lz1 = n3.y;
-    uint32_t hx0 = n3.z, hx1 = n3.w, hy0 = n4.x, hy1 = n4.y, hz0 = n4.z, hz1 = n4.w;
-    if (oct & 1u) { uint32_t t0 = lx0, t1 = lx1; lx0 = hx0; lx1 = hx1; hx0 = t0; hx1 = t1; }
-    if (oct & 2u) { uint32_t t0 = ly0, t1 = ly1; ly0 = hy0; ly1 = hy1; hy0 = t0; hy1 = t1; }
-    if (oct & 4u) { uint32_t t0 = lz0, t1 = lz1; lz0 = hz0; lz1 = hz1; hz0 = t0; hz1 = t1; }
-    uint32_t hits_int = 0, hits_tri = 0;
-    const float tlim = tmax * 1.0000004f;
+  uint32_t lx0 = n2.x, lx1 = n2.y, ly0 = n2.z, ly1 = n2.w, lz0 = n3.x, lz1 = n3.y;
+  uint32_t hx0 = n3.z, hx1 = n3.w, hy0 = n4.x, hy1 = n4.y, hz0 = n4.z, hz1 = n4.w;
+  if (oct & 1u) { uint32_t t0 = lx0, t1 = lx1; lx0 = hx0; lx1 = hx1; hx0 = t0; hx1 = t1; }
+  if (oct & 2u) { uint32_t t0 = ly0, t1 = ly1; ly0 = hy0; ly1 = hy1; hy0 = t0; hy1 = t1; }
+  if (oct & 4u) { uint32_t t0 = lz0, t1 = lz1; lz0 = hz0; lz1 = hz1; hz0 = t0; hz1 = t1; }
+  uint32_t hits_int = 0, hits_tri = 0;
+  const float tlim = w.tmax * 1.0000004f;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      uint32_t meta = ((j < 4 ? n1.z : n1.w) >> (8 * (j & 3))) & 0xFFu;
-      int k = j & 3;
-      float nx = byte_f(j < 4 ? lx0 : lx1, k), fx = byte_f(j < 4 ? hx0 : hx1, k);
-      float ny = byte_f(j < 4 ? ly0 : ly1, k), fy = byte_f(j < 4 ? hy0 : hy1, k);
-      float nz = byte_f(j < 4 ? lz0 : lz1, k), fz = byte_f(j < 4 ? hz0 : hz1, k);
-      float t0x = fmaf(nx, sx, ax), t1x = fmaf(fx, sx, ax);
-      float t0y = fmaf(ny, sy, ay), t1y = fmaf(fy, sy, ay);
-      float t0z = fmaf(nz, sz, az), t1z = fmaf(fz, sz, az);
-      float tmin_c = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, tnear));
-      float tmax_c = fminf(fminf(t1x, t1y), fminf(t1z, tlim));
-      bool h = meta != 0u && tmin_c <= tmax_c;
-      if (h) {
-        if (imask & (1u << j)) {
-          hits_int |= 1u << ((uint32_t)j ^ oct);
-        } else {
-          uint32_t cnt = meta >> 5, off = meta & 31u;
-          hits_tri |= ((1u << cnt) - 1u) << off;
-        }
+  for (int j = 0; j < 8; ++j) {
+    uint32_t meta = ((j < 4 ? n1.z : n1.w) >> (8 * (j & 3))) & 0xFFu;
+    int k = j & 3;
+    float t0x = fmaf(byte_f(j < 4 ? lx0 : lx1, k), sx, ax), t1x = fmaf(byte_f(j < 4 ? hx0 : hx1, k), sx, ax);
+    float t0y = fmaf(byte_f(j < 4 ? ly0 : ly1, k), sy, ay), t1y = fmaf(byte_f(j < 4 ? hy0 : hy1, k), sy, ay);
+    float t0z = fmaf(byte_f(j < 4 ? lz0 : lz1, k), sz, az), t1z = fmaf(byte_f(j < 4 ? hz0 : hz1, k), sz, az);
+    float tmin_c = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, w.tnear));
+    float tmax_c = fminf(fminf(t1x, t1y), fminf(t1z, tlim));
+    if (meta != 0u && tmin_c <= tmax_c) {
+      if (imask & (1u << j)) hits_int |= 1u << ((uint32_t)j ^ oct);
+      else hits_tri |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+    }
+  }
+  Gn = make_uint2(n1.x, kNodeGroup | (imask << 8) | hits_int);
+  Tn = make_uint2(n1.y, hits_tri);
+}
+
+// One step: visit one node (or take a popped triangle group) and test the
+// current triangle group.  Returns true when the ray is finished.
+template <bool ANY>
+__device__ __forceinline__ bool walk_step(const BvhView& bvh, Walk& w, uint2* stack, int* err) {
+  if (++w.iters > kMaxIters) {
+    atomicOr(err, ERR_ITER);
+    return true;
+  }
+  bool descended = false;
+  if ((w.G.y & kNodeGroup) && (w.G.y & 0xFFu)) {
+    uint32_t hits = w.G.y & 0xFFu;
+    uint32_t imask = (w.G.y >> 8) & 0xFFu;
+    int bpos = __ffs(hits) - 1;
+    hits &= hits - 1;
+    uint32_t slot = (uint32_t)bpos ^ w.r.oct;
+    uint32_t node = w.G.x + __popc(imask & ((1u << slot) - 1u));
+    if (hits) {
+      if (w.sp < kStack) stack[w.sp++] = make_uint2(w.G.x, kNodeGroup | (imask << 8) | hits);
+      else atomicOr(err, ERR_STACK);
+    }
+    uint2 Tn;
+    intersect_node(bvh, w, node, w.G, Tn);
+    w.T = Tn;
+    descended = true;
+  } else if (!(w.G.y & kNodeGroup)) {
+    w.T = w.G;  // a popped triangle group
+    w.G = make_uint2(0u, 0u);
+  } else {
+    w.G = make_uint2(0u, 0u);
+  }
+  while (w.T.y) {
+    // postpone when few lanes test triangles and this ray still has nodes to visit
+    if (descended && (w.G.y & 0xFFu) && __popc(__activemask()) < kPostpone) {
+      if (w.sp < kStack) {
+        stack[w.sp++] = w.T;
+        w.T.y = 0;
+        break;
       }
     }
-    ng_base = n1.x;
-    ng_hits = hits_int;
-    ng_imask = imask;
-    tg_base = n1.y;
-    tg_hits = hits_tri;
+    int k = __ffs(w.T.y) - 1;
+    w.T.y &= w.T.y - 1;
+    const float4* tp = bvh.tris + 3 * (size_t)(w.T.x + k);
+    float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+    float t, u, v;
+    if (tri_test(w.r, a, b, c, w.tnear, w.tmax, t, u, v)) {
+      w.hit = true;
+      w.tmax = t;
+      w.u = u;
+      w.v = v;
+      w.prim = __float_as_uint(a.w);
+      if (ANY) return true;
+    }
   }
-  return hit;
+  bool g_empty = !((w.G.y & kNodeGroup) ? (w.G.y & 0xFFu) : w.G.y);
+  if (g_empty) {
+    if (w.sp == 0) return true;
+    w.G = stack[--w.sp];
+  }
+  return false;
 }
 
 __device__ __forceinline__ void load_ray(TravRay& r, float4 o, float4 d) {
@@ -213,27 +244,54 @@ __device__ __forceinline__ void load_ray(TravRay& r, float4 o, float4 d) {
   prepare(r);
 }
 
+// Persistent queue consumer: lanes refill from the queue as their rays end.
+template <bool SHADOW, class Q, class Fin>
+__device__ __forceinline__ void consume(const BvhView& bvh, const Q& q, int n, int* fetch, int* err, Fin&& finish) {
+  const int lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  uint2 stack[kStack];
+  Walk w;
+  int ray = -1;
+  bool exhausted = false;
+  while (true) {
+    bool need = ray < 0 && !exhausted;
+    unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
+    if (needm) {
+      int leader = __ffs(needm) - 1;
+      int base = 0;
+      if (lane == leader) base = atomicAdd(fetch, __popc(needm));
+      base = __shfl_sync(0xFFFFFFFFu, base, leader);
+      if (need) {
+        int r = base + __popc(needm & lt);
+        if (r < n) {
+          ray = r;
+          float4 o = q.o[r], d = q.d[r];
+          load_ray(w.r, o, d);
+          walk_init(w, bvh, 0.001f, SHADOW ? o.w : INFINITY);
+        } else {
+          exhausted = true;
+        }
+      }
+    }
+    if (!__any_sync(0xFFFFFFFFu, ray >= 0)) break;
+    if (ray >= 0) {
+      if (walk_step<SHADOW>(bvh, w, stack, err)) {
+        finish(ray, w);
+        ray = -1;
+      }
+    }
+  }
+}
+
 __global__ void __launch_bounds__(kTravThreads) k_extend(BvhView bvh, ExtQueue q, const int* __restrict__ n_ptr, int cap,
                                                         float4* __restrict__ hits, int* fetch, int* err,
                                                         Counters64* stats) {
   const int n = min(*n_ptr, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&stats->extend_rays, (unsigned long long)n);
-  const int lane = threadIdx.x & 31;
-  while (true) {
-    int base = 0;
-    if (lane == 0) base = atomicAdd(fetch, 32);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= n) break;
-    int i = base + lane;
-    if (i < n) {
-      TravRay r;
-      load_ray(r, q.o[i], q.d[i]);
-      float t = 0.f, u = 0.f, v = 0.f;
-      uint32_t prim = kMissPrim;
-      bool h = traverse<false>(bvh, r, 0.001f, INFINITY, t, u, v, prim, err);
-      hits[i] = h ? make_float4(t, u, v, __uint_as_float(prim)) : make_float4(0.f, 0.f, 0.f, __uint_as_float(kMissPrim));
-    }
-  }
+  consume<false>(bvh, q, n, fetch, err, [&](int i, const Walk& w) {
+    hits[i] = w.hit ? make_float4(w.tmax, w.u, w.v, __uint_as_float(w.prim))
+                    : make_float4(0.f, 0.f, 0.f, __uint_as_float(kMissPrim));
+  });
 }
 
 __global__ void __launch_bounds__(kTravThreads) k_shadow(BvhView bvh, ShadowQueue q, const int* __restrict__ n_ptr, int cap,
@@ -241,52 +299,40 @@ __global__ void __launch_bounds__(kTravThreads) k_shadow(BvhView bvh, ShadowQueu
                                                         int* fetch, int* err, Counters64* stats) {
   const int n = min(*n_ptr, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&stats->shadow_rays, (unsigned long long)n);
-  const int lane = threadIdx.x & 31;
-  while (true) {
-    int base = 0;
-    if (lane == 0) base = atomicAdd(fetch, 32);
-    base = __shfl_sync(0xFFFFFFFFu, base, 0);
-    if (base >= n) break;
-    int i = base + lane;
-    if (i < n) {
-      float4 o = q.o[i], d = q.d[i];
-      TravRay r;
-      load_ray(r, o, d);
-      float t, u, v;
-      uint32_t prim;
-      bool occ = traverse<true>(bvh, r, 0.001f, o.w, t, u, v, prim, err);
-      float4 c = q.c[i];
-      uint32_t target = __float_as_uint(d.w);
-      if (__float_as_uint(c.w) == 0u) {
-        if (!occ) {
-          float4* L = path_L + target;
-          atomicAdd(&L->x, c.x);
-          atomicAdd(&L->y, c.y);
-          atomicAdd(&L->z, c.z);
-        }
-      } else if (occ) {
-        nee_li[target] = make_float4(0.f, 0.f, 0.f, 0.f);
+  consume<true>(bvh, q, n, fetch, err, [&](int i, const Walk& w) {
+    float4 c = q.c[i];
+    uint32_t target = __float_as_uint(q.d[i].w);
+    if (__float_as_uint(c.w) == 0u) {
+      if (!w.hit) {
+        float4* L = path_L + target;
+        atomicAdd(&L->x, c.x);
+        atomicAdd(&L->y, c.y);
+        atomicAdd(&L->z, c.z);
       }
+    } else if (w.hit) {
+      nee_li[target] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
-  }
+  });
 }
 
 __global__ void k_closest_rays(BvhView bvh, const shb_ray* __restrict__ rays, int64_t n, float4* __restrict__ hits,
                                int* err) {
+  uint2 stack[kStack];
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const shb_ray& sr = rays[i];
-    TravRay r;
-    r.ox = sr.origin[0];
-    r.oy = sr.origin[1];
-    r.oz = sr.origin[2];
-    r.dx = sr.direction[0];
-    r.dy = sr.direction[1];
-    r.dz = sr.direction[2];
-    prepare(r);
-    float t = 0.f, u = 0.f, v = 0.f;
-    uint32_t prim = kMissPrim;
-    bool h = traverse<false>(bvh, r, sr.tnear, sr.tfar, t, u, v, prim, err);
-    hits[i] = h ? make_float4(t, u, v, __uint_as_float(prim)) : make_float4(0.f, 0.f, 0.f, __uint_as_float(kMissPrim));
+    Walk w;
+    w.r.ox = sr.origin[0];
+    w.r.oy = sr.origin[1];
+    w.r.oz = sr.origin[2];
+    w.r.dx = sr.direction[0];
+    w.r.dy = sr.direction[1];
+    w.r.dz = sr.direction[2];
+    prepare(w.r);
+    walk_init(w, bvh, sr.tnear, sr.tfar);
+    while (!walk_step<false>(bvh, w, stack, err)) {
+    }
+    hits[i] = w.hit ? make_float4(w.tmax, w.u, w.v, __uint_as_float(w.prim))
+                    : make_float4(0.f, 0.f, 0.f, __uint_as_float(kMissPrim));
   }
 }
 
@@ -301,8 +347,8 @@ int traversal_grid(int device) {
   return sms * per_sm;
 }
 
-void launch_extend(cudaStream_t st, int grid, const BvhView& bvh, ExtQueue q, const int* n, int cap, float4* hits, int* fetch,
-                   int* err, Counters64* stats) {
+void launch_extend(cudaStream_t st, int grid, const BvhView& bvh, ExtQueue q, const int* n, int cap, float4* hits,
+                   int* fetch, int* err, Counters64* stats) {
   k_extend<<<grid, kTravThreads, 0, st>>>(bvh, q, n, cap, hits, fetch, err, stats);
 }
 
