@@ -35,6 +35,10 @@ WORKLOADS = {
     "room": dict(kind="room", width=1024, height=1024, ss=3, spp=128, bounces=3, dilation=2, seed=2),
     "room_small": dict(kind="room", width=256, height=256, ss=2, spp=32, bounces=3, dilation=2, seed=2),
     "unit_quad": dict(kind="unit_quad", width=256, height=256, ss=1, spp=64, bounces=3, dilation=0, seed=1),
+    # two-storey colonnaded courtyard (~262k triangles), lightmap 2048^2,
+    # supersample 3, 256 spp, 4 bounces, dilation 4
+    "atrium": dict(kind="atrium", width=2048, height=2048, ss=3, spp=256, bounces=4, dilation=4, seed=3),
+    "atrium_small": dict(kind="atrium", width=512, height=512, ss=1, spp=32, bounces=4, dilation=4, seed=3),
 }
 
 
@@ -42,6 +46,8 @@ def make_scene(w):
     from sh_baker_b200 import scenes
     if w["kind"] == "room":
         return scenes.procedural_room(seed=w["seed"], res=w["width"])
+    if w["kind"] == "atrium":
+        return scenes.atrium(seed=w["seed"], res=w["width"])
     if w["kind"] == "unit_quad":
         return scenes.unit_quad()
     raise ValueError(w["kind"])

@@ -175,18 +175,31 @@ __device__ LightEval eval_light(const SceneView& sc, uint32_t li, f3 P, f3 N, Ev
 // One light pick of the discrete distribution over weights (the counter
 // stream's uniform `u` against the running float sum; zero-weight lights
 // are never picked).
+// Weights of up to kWeightCache lights are kept from the summing pass, so
+// the pick only re-evaluates the chosen light; beyond that every light is
+// re-evaluated (same values either way: evaluation is deterministic).
+constexpr uint32_t kWeightCache = 32;
+
 template <bool HIT>
 __device__ bool pick_light(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3 aop, float sum, float u,
-                           LightEval& out) {
+                           const float* wcache, LightEval& out) {
   float target = u * sum;
   float cum = 0.f;
   int last = -1;
+  const bool cached = sc.light_count <= kWeightCache;
   for (uint32_t i = 0; i < sc.light_count; ++i) {
-    LightEval e = eval_light<HIT>(sc, i, P, N, ev, wo, aop);
-    cum += e.w;
-    if (e.w > 0.f) last = (int)i;
+    float w;
+    LightEval e;
+    if (cached) {
+      w = wcache[i];
+    } else {
+      e = eval_light<HIT>(sc, i, P, N, ev, wo, aop);
+      w = e.w;
+    }
+    cum += w;
+    if (w > 0.f) last = (int)i;
     if (target < cum) {
-      out = e;
+      out = cached ? eval_light<HIT>(sc, i, P, N, ev, wo, aop) : e;
       return true;
     }
   }
@@ -196,9 +209,14 @@ __device__ bool pick_light(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3
 }
 
 template <bool HIT>
-__device__ float light_weight_sum(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3 aop) {
+__device__ float light_weight_sum(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3 aop, float* wcache) {
   float sum = 0.0f;
-  for (uint32_t i = 0; i < sc.light_count; ++i) sum += eval_light<HIT>(sc, i, P, N, ev, wo, aop).w;
+  const bool cached = sc.light_count <= kWeightCache;
+  for (uint32_t i = 0; i < sc.light_count; ++i) {
+    float w = eval_light<HIT>(sc, i, P, N, ev, wo, aop).w;
+    if (cached) wcache[i] = w;
+    sum += w;
+  }
   return sum;
 }
 
@@ -300,13 +318,15 @@ __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
     Event ev;
     ev.init(a.seed, texel, sample, 0, EV_NEE);
     const f3 zero3 = {0.f, 0.f, 0.f};
-    float sum = active ? light_weight_sum<false>(a.sc, P0, N, ev, zero3, zero3) : 0.f;
+    float wcache[kWeightCache];
+    float sum = active ? light_weight_sum<false>(a.sc, P0, N, ev, zero3, zero3, wcache) : 0.f;
     bool any_light = active && !(sum < 1e-6f);
     for (int j = 0; j < a.nls; ++j) {
       LightEval e;
       bool ok = false;
       if (any_light) {
-        ok = pick_light<false>(a.sc, P0, N, ev, zero3, zero3, sum, ev.u(3 * (int)a.sc.area_light_count + j), e);
+        ok = pick_light<false>(a.sc, P0, N, ev, zero3, zero3, sum, ev.u(3 * (int)a.sc.area_light_count + j), wcache,
+                               e);
         if (ok) {
           float pdf = e.w / sum;
           float joint = pdf * e.apdf;
@@ -418,14 +438,16 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
     f3 wo = -d;
     Event ev;
     ev.init(a.seed, texel, sample, vertex, EV_NEE);
-    float sum = opaque_hit ? light_weight_sum<true>(a.sc, hit_pos, N, ev, wo, aop) : 0.f;
+    float wcache[kWeightCache];
+    float sum = opaque_hit ? light_weight_sum<true>(a.sc, hit_pos, N, ev, wo, aop, wcache) : 0.f;
     bool any_light = opaque_hit && !(sum < 1e-6f);
     for (int j = 0; j < a.nls; ++j) {
       LightEval e;
       bool ok = false;
       f3 c = {0.f, 0.f, 0.f};
       if (any_light) {
-        ok = pick_light<true>(a.sc, hit_pos, N, ev, wo, aop, sum, ev.u(3 * (int)a.sc.area_light_count + j), e);
+        ok = pick_light<true>(a.sc, hit_pos, N, ev, wo, aop, sum, ev.u(3 * (int)a.sc.area_light_count + j), wcache,
+                              e);
         if (ok) {
           float pdf = e.w / sum;
           float joint = pdf * e.apdf;

@@ -50,9 +50,14 @@ class Patch:
     height: float = 0.0
     inward: bool = False
 
+    # "arch": half barrel vault; corner = centre of the springing line,
+    # eu = half-span vector (radius), ev = depth vector; "cloth": quad with a
+    # sinusoidal sag of amplitude `radius` along its normal.
     def world_size(self) -> Tuple[float, float]:
-        if self.kind == "quad":
+        if self.kind in ("quad", "cloth"):
             return float(np.linalg.norm(self.eu)), float(np.linalg.norm(self.ev))
+        if self.kind == "arch":
+            return math.pi * float(np.linalg.norm(self.eu)), float(np.linalg.norm(self.ev))
         return 2.0 * math.pi * self.radius, self.height
 
 
@@ -112,6 +117,26 @@ class MeshBuilder:
             pos = p.corner[None, :] + A[:, None] * p.eu[None, :] + B[:, None] * p.ev[None, :]
             nrm = np.repeat(_normalize(np.cross(p.eu, p.ev))[None, :], len(A), 0)
             tan = np.repeat(_normalize(p.eu)[None, :], len(A), 0)
+        elif p.kind == "cloth":
+            n0 = _normalize(np.cross(p.eu, p.ev))
+            sag = p.radius * np.sin(math.pi * A) * np.sin(math.pi * B)
+            pos = (p.corner[None, :] + A[:, None] * p.eu[None, :] + B[:, None] * p.ev[None, :]
+                   + sag[:, None] * n0[None, :])
+            # analytic normal of the sagging sheet
+            du = p.eu[None, :] + (p.radius * math.pi * np.cos(math.pi * A) * np.sin(math.pi * B))[:, None] * n0[None, :]
+            dv = p.ev[None, :] + (p.radius * math.pi * np.sin(math.pi * A) * np.cos(math.pi * B))[:, None] * n0[None, :]
+            nrm = np.cross(du, dv)
+            nrm /= np.linalg.norm(nrm, axis=1, keepdims=True)
+            tan = du / np.linalg.norm(du, axis=1, keepdims=True)
+        elif p.kind == "arch":
+            r = float(np.linalg.norm(p.eu))
+            span = p.eu / r
+            up = np.array([0.0, 1.0, 0.0])
+            ang = A * math.pi
+            radial = np.cos(ang)[:, None] * span[None, :] + np.sin(ang)[:, None] * up[None, :]
+            pos = p.corner[None, :] + r * radial + B[:, None] * p.ev[None, :]
+            nrm = -radial  # the intrados faces the axis
+            tan = -np.sin(ang)[:, None] * span[None, :] + np.cos(ang)[:, None] * up[None, :]
         else:
             ang = A * 2.0 * math.pi
             radial = np.stack([np.cos(ang), np.zeros_like(ang), np.sin(ang)], 1)
@@ -129,7 +154,7 @@ class MeshBuilder:
             for i in range(nu):
                 q0 = j * (nu + 1) + i
                 q1, q2, q3 = q0 + 1, q0 + nu + 2, q0 + nu + 1
-                if p.kind == "cyl" and not p.inward:
+                if (p.kind == "cyl" and not p.inward) or (p.kind == "arch" and not p.inward):
                     ii += [q0, q2, q1, q0, q3, q2]
                 else:
                     ii += [q0, q1, q2, q0, q2, q3]
@@ -233,3 +258,121 @@ def procedural_room(seed: int = 2, n_boxes: int = 200, res: int = 1024, padding:
         pos = (rng.uniform(-4, 4), rng.uniform(1.5, 2.8), rng.uniform(-4, 4))
         lights.append(Light(type=POINT, position=tuple(float(x) for x in pos), intensity=float(rng.uniform(5, 50))))
     return Scene(geoms, mats, lights)
+
+
+def atrium(seed: int = 3, res: int = 2048, padding: int = 2, column_segments: Tuple[int, int] = (50, 20),
+           n_cloth: int = 100, cloth_grid: Tuple[int, int] = (22, 23), wall_grid: int = 22) -> Scene:
+    """Two-storey colonnaded courtyard (~262k triangles): 64 columns of
+    2,000-triangle cylinders (32 per storey on the courtyard edge), half-barrel
+    arches between neighbouring columns, tiled ground floor, gallery slabs and
+    roof, subdivided outer and courtyard walls, and 100 hanging cloth quads of
+    about 1,000 triangles.  25 materials with albedo U[0.1, 0.9]; 10 % of the
+    planar patches are emissive with radiance U[1, 5] (area lights); one sun
+    of radiance 20 and 8 point lights in the galleries."""
+    rng = np.random.default_rng(seed)
+    n_mat = 25
+    n_emissive = 3  # materials 22..24 are emissive
+    mats = [solid_material(rng.uniform(0.1, 0.9, 3), name=f"m{i}") for i in range(n_mat - n_emissive)]
+    mats += [solid_material(rng.uniform(0.6, 1.0, 3), emission=float(rng.uniform(1.0, 5.0)), name=f"e{i}")
+             for i in range(n_emissive)]
+    X, Z, H, S = 20.0, 15.0, 10.0, 5.0  # outer half-extents, height, storey height
+    CX, CZ = 14.0, 9.0                   # courtyard half-extents
+    patches: List[Patch] = []
+    mat_ids: List[int] = []
+    planar: List[int] = []  # geometry ids of planar patches (candidates for emission)
+
+    def add(p_list, mat, is_planar):
+        gid = len(mat_ids)
+        for p in p_list:
+            p.geom = gid
+            patches.append(p)
+        mat_ids.append(mat)
+        if is_planar:
+            planar.append(gid)
+        return gid
+
+    def quad(corner, eu, ev, nu=1, nv=1):
+        return Patch(0, "quad", np.asarray(corner, np.float64), np.asarray(eu, np.float64),
+                     np.asarray(ev, np.float64), nu, nv)
+
+    def rmat():
+        return int(rng.integers(0, n_mat - n_emissive))
+
+    # ground floor tiles: 5 m x 5 m patches of 1 m tiles, facing up
+    for x0 in np.arange(-X, X, 5.0):
+        for z0 in np.arange(-Z, Z, 5.0):
+            add([quad((x0, 0.0, z0), (0, 0, 5.0), (5.0, 0, 0), 5, 5)], rmat(), True)
+    # gallery slab (y = S, both faces) and roof (y = H, underside) over the ring
+    ring = [((-X, -Z), (2 * X, Z - CZ)), ((-X, CZ), (2 * X, Z - CZ)), ((-X, -CZ), (X - CX, 2 * CZ)),
+            ((CX, -CZ), (X - CX, 2 * CZ))]
+    for (x0, z0), (dx, dz) in ring:
+        nx, nz = max(1, int(dx / 2.5)), max(1, int(dz / 2.5))
+        add([quad((x0, S, z0), (0, 0, dz), (dx, 0, 0), nz, nx)], rmat(), True)           # slab top
+        add([quad((x0, S - 0.01, z0), (dx, 0, 0), (0, 0, dz), nx, nz)], rmat(), True)    # ceiling below
+        add([quad((x0, H, z0), (dx, 0, 0), (0, 0, dz), nx, nz)], rmat(), True)           # roof underside
+    # outer walls (inward) and courtyard-facing upper walls, per storey, as panels
+    for s in range(2):
+        y0 = s * S
+        for (c, eu) in (((-X, y0, -Z), (2 * X, 0, 0)), ((X, y0, Z), (-2 * X, 0, 0)),
+                        ((-X, y0, Z), (0, 0, -2 * Z)), ((X, y0, -Z), (0, 0, 2 * Z))):
+            L = np.linalg.norm(eu)
+            n_pan = int(L // 10)
+            step = np.asarray(eu, np.float64) / n_pan
+            for k in range(n_pan):
+                corner = np.asarray(c, np.float64) + k * step
+                add([quad(corner, step, (0, S, 0), wall_grid, wall_grid)], rmat(), True)
+    # 64 columns (2 storeys x 32 on the courtyard edge)
+    col_xz = []
+    for x in np.linspace(-CX, CX, 10):
+        col_xz += [(x, -CZ), (x, CZ)]
+    for z in np.linspace(-CZ, CZ, 8)[1:-1]:
+        col_xz += [(-CX, z), (CX, z)]
+    assert len(col_xz) == 32
+    nseg, nring = column_segments
+    for s in range(2):
+        for (x, z) in col_xz:
+            add([Patch(0, "cyl", np.array([x, s * S, z]), np.zeros(3), np.zeros(3), nseg, nring, radius=0.35,
+                       height=S - 1.0)], rmat(), False)
+    # arches between neighbouring columns along each courtyard side, per storey
+    for s in range(2):
+        ytop = s * S + (S - 1.0)
+        sides = [([(x, -CZ) for x in np.linspace(-CX, CX, 10)], (0, 0, 0.8)),
+                 ([(x, CZ) for x in np.linspace(-CX, CX, 10)], (0, 0, -0.8)),
+                 ([(-CX, z) for z in np.linspace(-CZ, CZ, 8)], (0.8, 0, 0)),
+                 ([(CX, z) for z in np.linspace(-CZ, CZ, 8)], (-0.8, 0, 0))]
+        for pts, depth in sides:
+            for a, b in zip(pts[:-1], pts[1:]):
+                mid = np.array([(a[0] + b[0]) / 2, ytop, (a[1] + b[1]) / 2])
+                half = np.array([(b[0] - a[0]) / 2, 0.0, (b[1] - a[1]) / 2])
+                d = np.asarray(depth, np.float64)
+                add([Patch(0, "arch", mid - d / 2, half, d, 16, 2)], rmat(), True)
+    # 100 hanging cloth quads in the courtyard and the galleries
+    nu, nv = cloth_grid
+    for _ in range(n_cloth):
+        w, h = rng.uniform(1.0, 3.0), rng.uniform(1.0, 3.0)
+        cx, cz = rng.uniform(-X + 2, X - 2), rng.uniform(-Z + 2, Z - 2)
+        top = rng.uniform(3.0, 9.5)
+        ang = rng.uniform(0, math.pi)
+        eu = np.array([math.cos(ang) * w, 0.0, math.sin(ang) * w])
+        corner = np.array([cx, top - h, cz]) - eu / 2
+        add([Patch(0, "cloth", corner, eu, np.array([0.0, h, 0.0]), nu, nv, radius=0.15 * min(w, h))], rmat(), False)
+    # 10 % of the planar patches emissive
+    n_em = max(1, len(planar) // 10)
+    for gid in rng.choice(planar, size=n_em, replace=False):
+        mat_ids[int(gid)] = int(rng.integers(n_mat - n_emissive, n_mat))
+    geoms = build_from_patches(patches, mat_ids, res, padding)
+    scene = Scene(geoms, mats, [])
+    scene.lights.append(Light(type=DIRECTIONAL, direction=tuple(float(x) for x in _normalize([-0.35, -1.0, -0.45])),
+                              intensity=20.0))
+    for _ in range(8):
+        side = rng.integers(0, 4)
+        if side < 2:
+            pos = (rng.uniform(-X + 1, X - 1), rng.uniform(1.5, 4.5) + S * rng.integers(0, 2),
+                   (Z - 3.0) * (1 if side == 0 else -1))
+        else:
+            pos = ((X - 3.0) * (1 if side == 2 else -1), rng.uniform(1.5, 4.5) + S * rng.integers(0, 2),
+                   rng.uniform(-Z + 1, Z - 1))
+        scene.lights.append(Light(type=POINT, position=tuple(float(v) for v in pos),
+                                  intensity=float(rng.uniform(5.0, 50.0))))
+    mark_area_lights(scene)
+    return scene
