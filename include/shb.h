@@ -265,6 +265,36 @@ SHB_API shb_status shb_bake(shb_scene* scene, const shb_gbuffer* g,
                             const shb_bake_config* cfg, shb_bake_output* out,
                             shb_bake_stats* stats);
 
+/* ---- batched bakes ------------------------------------------------------
+ * Many independent BakeSHLightMap calls (different scenes, sizes, spp and
+ * bounces) share waves of a persistent launch fed by a device list of
+ * (bake, texel tile) work items; with use_graph the whole launch sequence is
+ * captured in one CUDA graph.  Results are bit-identical to one shb_bake
+ * call per item.  All scenes must belong to `ctx`; outputs are device
+ * pointers of W*s x H*s texels. */
+typedef struct shb_batch_item {
+  shb_scene* scene;
+  const shb_gbuffer* gbuffer;
+  shb_raster_config raster;
+  shb_bake_config config;
+  float* sh;              /* device, 27 floats per texel */
+  float* env_visibility;  /* device, 1 float per texel */
+} shb_batch_item;
+
+typedef struct shb_batch_options {
+  int32_t use_graph;    /* 1: capture the waves in one CUDA graph            */
+  int32_t autotune;     /* 1: pick wave/tile/grid per shape class, cached   */
+  int32_t wave_paths;   /* paths per wave (0: default or tuned)             */
+  int32_t tile_texels;  /* texels per work tile (0: default or tuned)       */
+  int32_t grid_scale;   /* traversal grid multiplier (0: default or tuned)  */
+  int32_t reserved[3];
+  const char* tune_cache; /* tuning file; NULL: $SHB_TUNE_CACHE or
+                             $HOME/.cache/sh_baker_b200/autotune.txt        */
+} shb_batch_options;
+
+SHB_API shb_status shb_bake_batch(shb_context* ctx, const shb_batch_item* items, int32_t count,
+                                  const shb_batch_options* options, shb_bake_stats* stats);
+
 /* ---- DownsampleTexture (src/baker.cpp:151-182) ------------------------ */
 
 /* Box average over scale x scale blocks including invalid texels; channels

@@ -105,6 +105,17 @@ class PipelineConfig(C.Structure):
     ]
 
 
+class BatchItem(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("gbuffer", C.c_void_p), ("raster", RasterConfig), ("config", BakeConfig),
+                ("sh", C.c_void_p), ("env_visibility", C.c_void_p)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("use_graph", C.c_int32), ("autotune", C.c_int32), ("wave_paths", C.c_int32),
+                ("tile_texels", C.c_int32), ("grid_scale", C.c_int32), ("reserved", C.c_int32 * 3),
+                ("tune_cache", C.c_char_p)]
+
+
 class Options(C.Structure):
     _fields_ = [("device", C.c_int32), ("profiling", C.c_int32), ("reserved", C.c_int32 * 6)]
 
@@ -140,6 +151,7 @@ SIGNATURES = {
     "shb_find_occlusion": (C.c_int, [vp, vp, C.c_int64, vp, C.c_int32]),
     "shb_bake_pipeline": (C.c_int, [vp, C.POINTER(PipelineConfig), vp, vp, vp, C.POINTER(BakeStats)]),
     "shb_dilate_noalloc": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_int32]),
+    "shb_bake_batch": (C.c_int, [vp, vp, C.c_int32, C.POINTER(BatchOptions), C.POINTER(BakeStats)]),
 }
 
 _lib = None

@@ -279,6 +279,55 @@ def Dilate(width: int, height: int, pixels: np.ndarray, mask: np.ndarray, passes
 
 
 @dataclass
+class BatchBake:
+    """One bake of a batch: an uploaded scene, its device G-buffer and the
+    BakeSHLightMap arguments."""
+    scene: DeviceScene
+    gbuffer: GBuffer
+    raster: RasterConfig
+    config: BakeConfig
+
+
+def bake_batch(ctx: Context, bakes, use_graph: bool = True, autotune: bool = False, tune_cache: Optional[str] = None,
+               wave_paths: int = 0, tile_texels: int = 0, grid_scale: int = 0, outputs=None):
+    """Runs many bakes in one persistent launch (shb_bake_batch).  Returns
+    ([(sh, env)] device tensors of W*s*H*s*27 and W*s*H*s floats, stats).
+    `outputs` may supply those tensors (reused across calls)."""
+    import torch
+    n = len(bakes)
+    items = (A.BatchItem * max(1, n))()
+    outs = []
+    for i, b in enumerate(bakes):
+        texels = b.gbuffer.width * b.gbuffer.height
+        if outputs is not None:
+            sh, env = outputs[i]
+        else:
+            sh = torch.empty(texels * 27, dtype=torch.float32, device="cuda")
+            env = torch.empty(texels, dtype=torch.float32, device="cuda")
+        outs.append((sh, env))
+        items[i] = A.BatchItem(b.scene.h, b.gbuffer.h, b.raster.c(), b.config.c(), sh.data_ptr(), env.data_ptr())
+    opts = A.BatchOptions()
+    opts.use_graph = int(use_graph)
+    opts.autotune = int(autotune)
+    opts.wave_paths = wave_paths
+    opts.tile_texels = tile_texels
+    opts.grid_scale = grid_scale
+    opts.tune_cache = tune_cache.encode() if tune_cache else None
+    st = A.BakeStats()
+    A.check(ctx.lib.shb_bake_batch(ctx.h, C.addressof(items), n, C.byref(opts), C.byref(st)))
+    return outs, st
+
+
+def bake_plain_device(b: BatchBake, sh, env) -> A.BakeStats:
+    """One plain BakeSHLightMap (shb_bake) into device tensors."""
+    out = A.BakeOutput(sh.data_ptr(), env.data_ptr(), 1, 0)
+    st = A.BakeStats()
+    A.check(b.scene.lib.shb_bake(b.scene.h, b.gbuffer.h, C.byref(b.raster.c()), C.byref(b.config.c()), C.byref(out),
+                                 C.byref(st)))
+    return st
+
+
+@dataclass
 class LightmapResult:
     """Final lightmap at width x height: sh (H, W, 9, 3), env (H, W), mask."""
     sh: np.ndarray

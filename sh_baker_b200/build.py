@@ -25,6 +25,7 @@ SOURCES = {
     "shade.cu": ["-fmad=false"],
     "traverse.cu": ["-fmad=true"],
     "bvh_build.cu": ["-fmad=true"],
+    "batch.cu": ["-fmad=false"],
 }
 HEADERS = ["shb_internal.h", "shb_math.cuh", "wavefront.h"]
 

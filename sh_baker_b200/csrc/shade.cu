@@ -10,7 +10,10 @@
 #include <cub/cub.cuh>
 #include <thrust/iterator/counting_iterator.h>
 
+#include <algorithm>
 #include <chrono>
+#include <string>
+#include <vector>
 
 #include "shb_math.cuh"
 #include "wavefront.h"
@@ -22,6 +25,10 @@ __constant__ float c_srgb[256];
 namespace {
 
 constexpr int kThreads = 256;
+// Alpha branches per path kept apart for deterministic accumulation: the
+// wave is shrunk by 2^min(bounces, kMaxBranchLog).  Branch slots beyond that
+// (more than six transmissive bounces) fall back to atomic accumulation.
+constexpr int kMaxBranchLog = 6;
 constexpr double kTwoPiD = 6.283185307179586;
 
 struct MatInfo {
@@ -262,27 +269,30 @@ __device__ __forceinline__ f3 primary_dir(const SP& sp, uint32_t seed, uint32_t 
 }
 
 struct WaveArgs {
-  SceneView sc;
-  const shb_surface_point* pts;
-  const uint32_t* valid;
-  uint32_t t0;       // first valid-texel slot of the wave
-  uint32_t n_tex;    // texels in the wave
-  uint32_t spp;
-  uint32_t seed;
-  uint32_t sample_offset;
-  int nls;
-  int bounces;
+  const BakeItem* bakes;  // device table
+  int n_bakes;
+  const Tile* tiles;      // this wave's tiles (device)
+  int n_tiles;
+  int64_t P;              // paths in the wave
+  int64_t n_tex;          // texels in the wave
+  int NLS;                // max num_light_samples over the batch (NEE slot stride)
   ExtQueue ext[2];
   float4* hits;
   ShadowQueue sh;
+  PathInfo* info;
   float4* path_L;
   float4* nee_li;
   float4* nee_dir;
   int* cnt;
-  float* sh_out;
-  float* env_out;
   int ext_cap;  // capacity of each extend queue
   int sh_cap;   // capacity of the shadow queue
+  // With several light samples or alpha branching a path gets more than one
+  // hit-NEE contribution per depth; they then go to fixed slots
+  // (path, branch, sample) and k_commit adds them in that order, so results
+  // do not depend on atomic ordering.
+  int det;
+  int slots;    // branch slots per path (1 without alpha)
+  float4* pend;
 };
 
 // Queue slot within capacity, else the error flag is raised and the ray dropped.
@@ -292,58 +302,79 @@ __device__ __forceinline__ bool slot_ok(const WaveArgs& a, int slot, int cap) {
   return false;
 }
 
+// Tile containing wave position `x` (a path when BY_PATH, else a texel).
+template <bool BY_PATH>
+__device__ __forceinline__ int find_tile(const WaveArgs& a, int64_t x) {
+  int lo = 0, hi = a.n_tiles;
+  while (hi - lo > 1) {
+    int mid = (lo + hi) >> 1;
+    int64_t off = BY_PATH ? a.tiles[mid].path_off : a.tiles[mid].tex_off;
+    if (off <= x) lo = mid;
+    else hi = mid;
+  }
+  return lo;
+}
+
 // ------------------------------------------------------------- generate --
 __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
-  const int64_t P = (int64_t)a.n_tex * a.spp;
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const int64_t warp_id = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
-  for (int64_t base = warp_id * 32; base < P; base += warps * 32) {
+  for (int64_t base = warp_id * 32; base < a.P; base += warps * 32) {
     int64_t p = base + lane;
-    bool active = p < P;
+    bool active = p < a.P;
     f3 o = {0.f, 0.f, 0.f}, dw = {0.f, 0.f, 1.f}, P0 = o, N = o;
-    uint32_t texel = 0, sample = 0;
+    uint32_t texel = 0, sample = 0, b = 0;
+    const BakeItem* B = a.bakes;
     if (active) {
-      uint32_t slot = (uint32_t)(p / a.spp);
-      sample = (uint32_t)(p % a.spp) + a.sample_offset;
-      texel = a.valid[a.t0 + slot];
-      SP sp = load_sp(a.pts, texel);
+      const Tile t = a.tiles[find_tile<true>(a, p)];
+      b = t.bake;
+      B = a.bakes + b;
+      int64_t local = p - t.path_off;
+      uint32_t slot = t.t0 + (uint32_t)(local / t.spp);
+      sample = (uint32_t)(local % t.spp) + B->sample_offset;
+      texel = B->valid[slot];
+      SP sp = load_sp(B->pts, texel);
       P0 = sp.pos;
       N = sp.nrm;
-      dw = primary_dir(sp, a.seed, texel, sample);
+      dw = primary_dir(sp, B->seed, texel, sample);
       o = sp.pos + sp.nrm * 0.001f;
       a.path_L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+      a.info[p] = make_uint4(b, texel, sample, 0u);
+      if (a.det)
+        for (int k = 0; k < a.slots * a.NLS; ++k) a.pend[p * a.slots * a.NLS + k] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
     // texel-level NEE (src/light.cpp:191-293), origin without offset
     Event ev;
-    ev.init(a.seed, texel, sample, 0, EV_NEE);
+    ev.init(active ? B->seed : 0u, texel, sample, 0, EV_NEE);
     const f3 zero3 = {0.f, 0.f, 0.f};
     float wcache[kWeightCache];
-    float sum = active ? light_weight_sum<false>(a.sc, P0, N, ev, zero3, zero3, wcache) : 0.f;
+    float sum = active ? light_weight_sum<false>(B->sc, P0, N, ev, zero3, zero3, wcache) : 0.f;
     bool any_light = active && !(sum < 1e-6f);
-    for (int j = 0; j < a.nls; ++j) {
+    const int nls = active ? B->nls : 0;
+    for (int j = 0; j < a.NLS; ++j) {
       LightEval e;
       bool ok = false;
-      if (any_light) {
-        ok = pick_light<false>(a.sc, P0, N, ev, zero3, zero3, sum, ev.u(3 * (int)a.sc.area_light_count + j), wcache,
-                               e);
+      if (any_light && j < nls) {
+        ok = pick_light<false>(B->sc, P0, N, ev, zero3, zero3, sum, ev.u(3 * (int)B->sc.area_light_count + j),
+                               wcache, e);
         if (ok) {
           float pdf = e.w / sum;
           float joint = pdf * e.apdf;
           ok = !(joint < 1e-3f);
           if (ok) {
-            f3 Li = e.rad / (joint * (float)a.nls);
-            a.nee_li[p * a.nls + j] = make_float4(Li.x, Li.y, Li.z, 0.f);
-            a.nee_dir[p * a.nls + j] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, 0.f);
+            f3 Li = e.rad / (joint * (float)nls);
+            a.nee_li[p * a.NLS + j] = make_float4(Li.x, Li.y, Li.z, 0.f);
+            a.nee_dir[p * a.NLS + j] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, 0.f);
           }
         }
       }
-      if (active && !ok) a.nee_li[p * a.nls + j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (active && !ok) a.nee_li[p * a.NLS + j] = make_float4(0.f, 0.f, 0.f, 0.f);
       int slot = warp_push(a.cnt + CNT_SHADOW, ok);
       if (ok && slot_ok(a, slot, a.sh_cap)) {
         a.sh.o[slot] = make_float4(P0.x, P0.y, P0.z, e.tfar);
-        a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float((uint32_t)(p * a.nls + j)));
-        a.sh.c[slot] = make_float4(0.f, 0.f, 0.f, __uint_as_float(1u));
+        a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float((uint32_t)(p * a.NLS + j)));
+        a.sh.c[slot] = make_float4(0.f, 0.f, 0.f, __uint_as_float(1u | (b << 2)));
       }
     }
     int slot = warp_push(a.cnt + CNT_EXT0, active);
@@ -357,7 +388,7 @@ __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
 
 // --------------------------------------------------------------- shade ---
 // One path vertex of Trace (src/baker.cpp:70-149) in throughput form.
-__global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int depth, int can_extend) {
+__global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int depth) {
   const int n = min(a.cnt[cur], a.ext_cap);
   const int nxt = cur ^ 1;
   const int warps = gridDim.x * (blockDim.x >> 5);
@@ -369,10 +400,12 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
     int i = base + lane;
     bool active = i < n;
     bool hit = false;
-    uint32_t path = 0, vertex = 0, texel = 0, sample = 0;
+    uint32_t path = 0, vertex = 0, texel = 0, sample = 0, b = 0;
+    const BakeItem* B = a.bakes;
     f3 d = {0.f, 0.f, 1.f}, beta = {0.f, 0.f, 0.f}, pos = {0.f, 0.f, 0.f}, N = {0.f, 0.f, 1.f};
     f2 uv = {0.f, 0.f};
     float alpha = 1.f;
+    bool can_extend = false;
     DMat mat;
     if (active) {
       float4 qo = q.o[i], qd = q.d[i], qb = q.beta[i], h = a.hits[i];
@@ -385,30 +418,34 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
         if (depth == 0) a.path_L[path].w += 1.0f;
       } else {
         hit = true;
-        uint32_t slot = path / a.spp;
-        texel = a.valid[a.t0 + slot];
-        sample = path % a.spp + a.sample_offset;
+        PathInfo pi = a.info[path];
+        b = pi.x;
+        B = a.bakes + b;
+        texel = pi.y;
+        sample = pi.z;
+        can_extend = depth < B->bounces;
+        const SceneView& sc = B->sc;
         f3 o = {qo.x, qo.y, qo.z};
         pos = o + d * h.x;
         float u = h.y, v = h.z;
         float w = 1.0f - u - v;
-        uint32_t g = a.sc.tri_geom[prim];
-        DGeom G = a.sc.geoms[g];
-        uint32_t i0 = a.sc.tri_vidx[3 * prim], i1 = a.sc.tri_vidx[3 * prim + 1], i2 = a.sc.tri_vidx[3 * prim + 2];
+        uint32_t g = sc.tri_geom[prim];
+        DGeom G = sc.geoms[g];
+        uint32_t i0 = sc.tri_vidx[3 * prim], i1 = sc.tri_vidx[3 * prim + 1], i2 = sc.tri_vidx[3 * prim + 2];
         if (G.flags & GEOM_HAS_NORMALS) {
-          N = normalized(w * ld3(a.sc.obj_n, i0) + u * ld3(a.sc.obj_n, i1) + v * ld3(a.sc.obj_n, i2));
+          N = normalized(w * ld3(sc.obj_n, i0) + u * ld3(sc.obj_n, i1) + v * ld3(sc.obj_n, i2));
         } else {
-          f3 v0 = ld3(a.sc.world_v, i0), v1 = ld3(a.sc.world_v, i1), v2 = ld3(a.sc.world_v, i2);
+          f3 v0 = ld3(sc.world_v, i0), v1 = ld3(sc.world_v, i1), v2 = ld3(sc.world_v, i2);
           N = normalized(cross(v1 - v0, v2 - v0));
         }
         if (G.flags & GEOM_HAS_TEXUV)
-          uv = w * ld2(a.sc.tex_uv, i0) + u * ld2(a.sc.tex_uv, i1) + v * ld2(a.sc.tex_uv, i2);
-        mat = load_mat(a.sc, G.material_id);
-        alpha = get_alpha(a.sc, mat, uv);
+          uv = w * ld2(sc.tex_uv, i0) + u * ld2(sc.tex_uv, i1) + v * ld2(sc.tex_uv, i2);
+        mat = load_mat(sc, G.material_id);
+        alpha = get_alpha(sc, mat, uv);
       }
     }
     // transmission (src/baker.cpp:99-105)
-    if (a.sc.has_alpha) {
+    if (__any_sync(0xFFFFFFFFu, hit && B->sc.has_alpha)) {
       bool tr = hit && alpha < 1.0f && can_extend;
       int slot = warp_push(a.cnt + nxt, tr);
       if (tr && slot_ok(a, slot, a.ext_cap)) {
@@ -422,7 +459,7 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
     bool opaque_hit = hit && alpha != 0.0f;
     f3 hit_pos = pos, aop = {0.f, 0.f, 0.f};
     if (opaque_hit) {
-      f3 alb = get_albedo(a.sc, mat, uv);
+      f3 alb = get_albedo(B->sc, mat, uv);
       aop = alb / 3.14159265358979323846f;
       if (depth == 0) {
         f3 em = mat.emission > 0.0f ? alb * mat.emission : f3{0.f, 0.f, 0.f};
@@ -437,29 +474,37 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
     // NEE at the hit (src/light.cpp:82-189)
     f3 wo = -d;
     Event ev;
-    ev.init(a.seed, texel, sample, vertex, EV_NEE);
+    ev.init(opaque_hit ? B->seed : 0u, texel, sample, vertex, EV_NEE);
     float wcache[kWeightCache];
-    float sum = opaque_hit ? light_weight_sum<true>(a.sc, hit_pos, N, ev, wo, aop, wcache) : 0.f;
+    float sum = opaque_hit ? light_weight_sum<true>(B->sc, hit_pos, N, ev, wo, aop, wcache) : 0.f;
     bool any_light = opaque_hit && !(sum < 1e-6f);
-    for (int j = 0; j < a.nls; ++j) {
+    const int nls = opaque_hit ? B->nls : 0;
+    for (int j = 0; j < a.NLS; ++j) {
       LightEval e;
       bool ok = false;
       f3 c = {0.f, 0.f, 0.f};
-      if (any_light) {
-        ok = pick_light<true>(a.sc, hit_pos, N, ev, wo, aop, sum, ev.u(3 * (int)a.sc.area_light_count + j), wcache,
+      if (any_light && j < nls) {
+        ok = pick_light<true>(B->sc, hit_pos, N, ev, wo, aop, sum, ev.u(3 * (int)B->sc.area_light_count + j), wcache,
                               e);
         if (ok) {
           float pdf = e.w / sum;
           float joint = pdf * e.apdf;
           ok = !(joint < 1e-3f);
-          if (ok) c = cmul(beta, alpha * ((e.rad / joint) / (float)a.nls));
+          if (ok) c = cmul(beta, alpha * ((e.rad / joint) / (float)nls));
         }
       }
       int slot = warp_push(a.cnt + CNT_SHADOW, ok);
       if (ok && slot_ok(a, slot, a.sh_cap)) {
+        uint32_t target = path, kind = 0u;
+        const uint32_t vslot = vertex - (1u << depth);
+        if (a.det && vslot < (uint32_t)a.slots) {
+          target = ((path * (uint32_t)a.slots + vslot) * (uint32_t)a.NLS + (uint32_t)j);
+          a.pend[target] = make_float4(c.x, c.y, c.z, 0.f);
+          kind = 2u;
+        }
         a.sh.o[slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, e.tfar);
-        a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float(path));
-        a.sh.c[slot] = make_float4(c.x, c.y, c.z, __uint_as_float(0u));
+        a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float(target));
+        a.sh.c[slot] = make_float4(c.x, c.y, c.z, __uint_as_float(kind | (b << 2)));
       }
     }
     // indirect (src/material.cpp:113-162, src/baker.cpp:131-148)
@@ -467,16 +512,16 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
     f3 nd = {0.f, 0.f, 1.f}, nb = {0.f, 0.f, 0.f};
     if (opaque_hit && can_extend) {
       Event eb;
-      eb.init(a.seed, texel, sample, vertex, EV_BSDF);
+      eb.init(B->seed, texel, sample, vertex, EV_BSDF);
       f3 t = fabsf(N.x) > fabsf(N.z) ? f3{-N.y, N.x, 0.0f} : f3{0.0f, -N.z, N.y};
       t = normalized(t);
-      f3 b = cross(N, t);
+      f3 bb = cross(N, t);
       float r1 = eb.u(0), r2 = eb.u(1);
       float phi = (float)(kTwoPiD * (double)r1);
       float theta = acosf(sqrtf(r2));
       float sin_theta = sinf(theta);
       f3 local = {cosf(phi) * sin_theta, sinf(phi) * sin_theta, cosf(theta)};
-      nd = normalized(t * local.x + b * local.y + N * local.z);
+      nd = normalized(t * local.x + bb * local.y + N * local.z);
       float pdf = (float)((double)local.z / 3.14159265358979323846);
       if (!(pdf < 1e-3f)) {
         bool zero = dot(N, nd) <= 0.0f || dot(N, wo) <= 0.0f;
@@ -492,6 +537,35 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
       qn.d[slot] = make_float4(nd.x, nd.y, nd.z, __uint_as_float(2u * vertex));
       qn.beta[slot] = make_float4(nb.x, nb.y, nb.z, 0.f);
     }
+  }
+}
+
+// Adds the pending hit-NEE contributions of one depth to the path radiance
+// in (branch, light sample) order and clears them: the same sum however the
+// shadow rays were scheduled.  Unoccluded slots keep the value k_shade
+// wrote, occluded ones were cleared by k_shadow, unused ones stay zero.
+__global__ void __launch_bounds__(kThreads) k_commit(WaveArgs a, int depth) {
+  const int used = min(1 << min(depth, 30), a.slots);
+  const int stride = a.slots * a.NLS;
+  for (int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; p < a.P; p += (int64_t)gridDim.x * blockDim.x) {
+    float4* pend = a.pend + p * stride;
+    float4 L = a.path_L[p];
+    bool any = false;
+    for (int v = 0; v < used; ++v) {
+      f3 s = {0.f, 0.f, 0.f};
+      for (int j = 0; j < a.NLS; ++j) {
+        float4 c = pend[v * a.NLS + j];
+        if (c.x != 0.f || c.y != 0.f || c.z != 0.f || __float_as_uint(c.w) != 0u) {
+          s = s + f3{c.x, c.y, c.z};
+          pend[v * a.NLS + j] = make_float4(0.f, 0.f, 0.f, 0.f);
+          any = true;
+        }
+      }
+      L.x += s.x;
+      L.y += s.y;
+      L.z += s.z;
+    }
+    if (any) a.path_L[p] = L;
   }
 }
 
@@ -520,28 +594,33 @@ __device__ __forceinline__ void sh_accumulate(f3 L, f3 d, float acc[27]) {
 // (src/sh_coeffs.cpp:50-78), the warp reduces with shuffles, and lanes
 // 0..27 store the 27 coefficients and the environment visibility.
 __global__ void __launch_bounds__(kThreads) k_resolve(WaveArgs a) {
-  const int warps = gridDim.x * (blockDim.x >> 5);
-  const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
+  const int64_t warp_id = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
   const float two_pi = (float)kTwoPiD;
-  for (uint32_t slot = warp_id; slot < a.n_tex; slot += warps) {
-    uint32_t texel = a.valid[a.t0 + slot];
-    SP sp = load_sp(a.pts, texel);
+  for (int64_t wt = warp_id; wt < a.n_tex; wt += warps) {
+    const Tile t = a.tiles[find_tile<false>(a, wt)];
+    const BakeItem* B = a.bakes + t.bake;
+    const int64_t local = wt - t.tex_off;
+    const uint32_t texel = B->valid[t.t0 + (uint32_t)local];
+    const int64_t pbase = t.path_off + local * t.spp;
+    const int nls = B->nls;
+    SP sp = load_sp(B->pts, texel);
     float acc[27];
 #pragma unroll
     for (int k = 0; k < 27; ++k) acc[k] = 0.f;
     float env = 0.f;
-    for (uint32_t s = lane; s < a.spp; s += 32) {
-      int64_t p = (int64_t)slot * a.spp + s;
-      for (int j = 0; j < a.nls; ++j) {
-        float4 li = a.nee_li[p * a.nls + j];
+    for (uint32_t s = lane; s < t.spp; s += 32) {
+      int64_t p = pbase + s;
+      for (int j = 0; j < nls; ++j) {
+        float4 li = a.nee_li[p * a.NLS + j];
         if (li.x != 0.f || li.y != 0.f || li.z != 0.f) {
-          float4 nd = a.nee_dir[p * a.nls + j];
+          float4 nd = a.nee_dir[p * a.NLS + j];
           sh_accumulate(f3{li.x, li.y, li.z}, f3{nd.x, nd.y, nd.z}, acc);
         }
       }
       float4 L = a.path_L[p];
-      f3 dw = primary_dir(sp, a.seed, texel, s + a.sample_offset);
+      f3 dw = primary_dir(sp, B->seed, texel, s + B->sample_offset);
       sh_accumulate(f3{L.x, L.y, L.z} * two_pi, dw, acc);
       env += L.w;
     }
@@ -551,13 +630,13 @@ __global__ void __launch_bounds__(kThreads) k_resolve(WaveArgs a) {
       for (int k = 0; k < 27; ++k) acc[k] += __shfl_xor_sync(0xFFFFFFFFu, acc[k], off);
       env += __shfl_xor_sync(0xFFFFFFFFu, env, off);
     }
-    const float inv = 1.0f / (float)a.spp;
+    const float inv = 1.0f / (float)t.spp;
     float mine = 0.f;
 #pragma unroll
     for (int k = 0; k < 27; ++k)
       if (lane == k) mine = acc[k];
-    if (lane < 27) a.sh_out[(int64_t)texel * 27 + lane] = mine * inv;
-    else if (lane == 27) a.env_out[texel] = env * inv;
+    if (lane < 27) B->sh_out[(int64_t)texel * 27 + lane] = mine * inv;
+    else if (lane == 27) B->env_out[texel] = env * inv;
   }
 }
 
@@ -646,63 +725,153 @@ shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n,
   return SHB_OK;
 }
 
-// BakeSHLightMap on a device G-buffer: waves of (texels x samples) paths.
-shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int H, const shb_bake_config* cfg,
-                       float* d_sh, float* d_env, shb_bake_stats* stats) {
-  shb_context* c = s->ctx;
+// ------------------------------------------------------------ batches ----
+
+namespace {
+
+struct Wave {
+  int tile_begin, n_tiles;
+  int64_t P, n_tex;
+  int max_bounces;
+};
+
+// Splits every bake's valid texels into tiles of whole texels (all their
+// samples) and packs consecutive tiles into waves of at most `wave_paths`
+// paths.
+void plan_waves(const std::vector<BakeSpec>& specs, const std::vector<int>& n_valid, int64_t wave_paths,
+                int64_t tile_texels, std::vector<Tile>& tiles, std::vector<Wave>& waves) {
+  tiles.clear();
+  waves.clear();
+  Wave cur{0, 0, 0, 0, 0};
+  for (size_t b = 0; b < specs.size(); ++b) {
+    const int64_t spp = specs[b].cfg.samples;
+    int64_t per_tile = std::max<int64_t>(1, std::min<int64_t>(tile_texels, wave_paths / spp));
+    for (int64_t t0 = 0; t0 < n_valid[b]; t0 += per_tile) {
+      int64_t nt = std::min<int64_t>(per_tile, n_valid[b] - t0);
+      int64_t paths = nt * spp;
+      if (cur.n_tiles > 0 && cur.P + paths > wave_paths) {
+        waves.push_back(cur);
+        cur = Wave{(int)tiles.size(), 0, 0, 0, 0};
+      }
+      Tile t;
+      t.bake = (uint32_t)b;
+      t.t0 = (uint32_t)t0;
+      t.n_tex = (uint32_t)nt;
+      t.spp = (uint32_t)spp;
+      t.path_off = cur.P;
+      t.tex_off = cur.n_tex;
+      tiles.push_back(t);
+      cur.n_tiles++;
+      cur.P += paths;
+      cur.n_tex += nt;
+      cur.max_bounces = std::max(cur.max_bounces, specs[b].cfg.bounces);
+    }
+  }
+  if (cur.n_tiles > 0) waves.push_back(cur);
+}
+
+}  // namespace
+
+// Runs a batch of bakes.  Each bake's outputs are zeroed, its valid texels
+// compacted, and then all bakes share waves of paths.
+shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs, const BatchParams& prm,
+                             shb_bake_stats* stats) {
   cudaStream_t st = c->stream;
-  const int64_t total = (int64_t)W * H;
-  const int spp = cfg->samples, B = cfg->bounces;
-  const int nls = cfg->num_light_samples;
-  SHB_CUDA(cudaMemsetAsync(d_sh, 0, sizeof(float) * 27 * (size_t)total, st));
-  SHB_CUDA(cudaMemsetAsync(d_env, 0, sizeof(float) * (size_t)total, st));
-  // compact valid texels (material_id >= 0), stable order
-  SHB_TRY(c->scratch[10].reserve(sizeof(uint32_t) * (size_t)(total + 1)));
-  SHB_TRY(c->counters.reserve(sizeof(int) * CNT_COUNT + sizeof(Counters64)));
-  uint32_t* valid = c->scratch[10].as<uint32_t>();
+  const int nb = (int)specs.size();
+  if (nb == 0) return SHB_OK;
+  int NLS = 1;
+  int64_t total_texels = 0;
+  bool any_alpha = false;
+  int max_b = 0;
+  for (const BakeSpec& s : specs) {
+    NLS = std::max(NLS, s.cfg.num_light_samples);
+    total_texels += (int64_t)s.W * s.H;
+    any_alpha = any_alpha || s.scene->has_alpha;
+    max_b = std::max(max_b, s.cfg.bounces);
+  }
+  // outputs and valid-texel lists
+  SHB_TRY(c->scratch[10].reserve(sizeof(uint32_t) * (size_t)(total_texels + nb)));
+  SHB_TRY(c->counters.reserve(sizeof(int) * CNT_COUNT + sizeof(Counters64) + sizeof(int) * (size_t)nb));
   int* cnt = c->counters.as<int>();
   Counters64* c64 = reinterpret_cast<Counters64*>(cnt + CNT_COUNT);
-  SHB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * CNT_COUNT + sizeof(Counters64), st));
+  int* nsel = reinterpret_cast<int*>(c64 + 1);
+  SHB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * CNT_COUNT + sizeof(Counters64) + sizeof(int) * (size_t)nb, st));
+  std::vector<BakeItem> items(nb);
+  uint32_t* valid_all = c->scratch[10].as<uint32_t>();
+  int64_t voff = 0;
   thrust::counting_iterator<uint32_t> it(0);
-  size_t tb = 0;
-  int* nsel = cnt + CNT_COUNT - 1;
-  cub::DeviceSelect::If(nullptr, tb, it, valid, nsel, (int)total, ValidPred{d_pts}, st);
-  SHB_TRY(c->scratch[11].reserve(tb));
-  SHB_CUDA(cub::DeviceSelect::If(c->scratch[11].ptr, tb, it, valid, nsel, (int)total, ValidPred{d_pts}, st));
-  count_launch(c, 1);
-  int n_valid = 0;
-  SHB_CUDA(cudaMemcpyAsync(&n_valid, nsel, sizeof(int), cudaMemcpyDeviceToHost, st));
+  for (int b = 0; b < nb; ++b) {
+    const BakeSpec& s = specs[b];
+    const int64_t n = (int64_t)s.W * s.H;
+    SHB_CUDA(cudaMemsetAsync(s.sh, 0, sizeof(float) * 27 * (size_t)n, st));
+    SHB_CUDA(cudaMemsetAsync(s.env, 0, sizeof(float) * (size_t)n, st));
+    size_t tb = 0;
+    cub::DeviceSelect::If(nullptr, tb, it, valid_all + voff, nsel + b, (int)n, ValidPred{s.pts}, st);
+    SHB_TRY(c->scratch[11].reserve(tb));
+    SHB_CUDA(cub::DeviceSelect::If(c->scratch[11].ptr, tb, it, valid_all + voff, nsel + b, (int)n, ValidPred{s.pts},
+                                   st));
+    count_launch(c, 1);
+    BakeItem& I = items[b];
+    I.sc = s.scene->view();
+    I.bvh = s.scene->bvh();
+    I.pts = s.pts;
+    I.valid = valid_all + voff;
+    I.sh_out = s.sh;
+    I.env_out = s.env;
+    I.spp = (uint32_t)s.cfg.samples;
+    I.seed = s.cfg.seed;
+    I.sample_offset = (uint32_t)s.cfg.sample_offset;
+    I.nls = s.cfg.num_light_samples;
+    I.bounces = s.cfg.bounces;
+    I.pad = 0;
+    voff += n;
+  }
+  std::vector<int> n_valid(nb, 0);
+  SHB_CUDA(cudaMemcpyAsync(n_valid.data(), nsel, sizeof(int) * (size_t)nb, cudaMemcpyDeviceToHost, st));
+  SHB_TRY(c->scratch[19].reserve(sizeof(BakeItem) * (size_t)nb));
+  BakeItem* d_items = c->scratch[19].as<BakeItem>();
+  SHB_CUDA(cudaMemcpyAsync(d_items, items.data(), sizeof(BakeItem) * (size_t)nb, cudaMemcpyHostToDevice, st));
   SHB_CUDA(cudaStreamSynchronize(st));
 
-  // wave sizing: paths per wave, queue capacity per depth
-  const int64_t kPathsPerWave = 1 << 23;
-  int64_t tex_per_wave = kPathsPerWave / spp;
-  if (tex_per_wave < 1) tex_per_wave = 1;
+  // plan tiles and waves
+  int64_t wave_paths = prm.wave_paths;
   int64_t mult = 1;
-  if (s->has_alpha) {
-    int sh = B < 4 ? B : 4;
-    mult = (int64_t)1 << sh;
-    tex_per_wave = tex_per_wave / mult > 0 ? tex_per_wave / mult : 1;
+  if (any_alpha) {
+    int shift = max_b < kMaxBranchLog ? max_b : kMaxBranchLog;
+    mult = (int64_t)1 << shift;
+    wave_paths = std::max<int64_t>(wave_paths / mult, 1 << 16);
   }
-  if (tex_per_wave > n_valid && n_valid > 0) tex_per_wave = n_valid;
-  const int64_t P = tex_per_wave * spp;
-  const int64_t ext_cap = P * mult;
-  const int64_t sh_cap = (P + ext_cap) * nls;
+  // Several hit-NEE contributions per path and depth (light samples or
+  // alpha branches) are summed in a fixed order by k_commit.
+  const bool det = NLS > 1 || any_alpha;
+  const int slots = (int)mult;
+  std::vector<Tile> tiles;
+  std::vector<Wave> waves;
+  plan_waves(specs, n_valid, wave_paths, prm.tile_texels, tiles, waves);
+  int64_t Pmax = 0;
+  for (const Wave& w : waves) Pmax = std::max(Pmax, w.P);
+  const int64_t ext_cap = std::max<int64_t>(Pmax * mult, 1);
+  const int64_t sh_cap = (Pmax + ext_cap) * NLS;
+  if (ext_cap > INT32_MAX || sh_cap > INT32_MAX) {
+    set_error("wave too large");
+    return SHB_ERR_INVALID_ARG;
+  }
   SHB_TRY(c->scratch[12].reserve(sizeof(float4) * 3 * (size_t)ext_cap));
   SHB_TRY(c->scratch[13].reserve(sizeof(float4) * 3 * (size_t)ext_cap));
   SHB_TRY(c->scratch[14].reserve(sizeof(float4) * (size_t)ext_cap));
   SHB_TRY(c->scratch[15].reserve(sizeof(float4) * 3 * (size_t)sh_cap));
-  SHB_TRY(c->scratch[16].reserve(sizeof(float4) * (size_t)P));
-  SHB_TRY(c->scratch[17].reserve(sizeof(float4) * 2 * (size_t)P * nls));
+  SHB_TRY(c->scratch[16].reserve(sizeof(float4) * (size_t)std::max<int64_t>(Pmax, 1)));
+  SHB_TRY(c->scratch[17].reserve(sizeof(float4) * 2 * (size_t)std::max<int64_t>(Pmax, 1) * NLS));
+  SHB_TRY(c->scratch[18].reserve(sizeof(PathInfo) * (size_t)std::max<int64_t>(Pmax, 1)));
+  if (det) SHB_TRY(c->scratch[24].reserve(sizeof(float4) * (size_t)std::max<int64_t>(Pmax, 1) * slots * NLS));
+  SHB_TRY(c->scratch[23].reserve(sizeof(Tile) * std::max<size_t>(tiles.size(), 1)));
+  Tile* d_tiles = c->scratch[23].as<Tile>();
+  if (!tiles.empty())
+    SHB_CUDA(cudaMemcpyAsync(d_tiles, tiles.data(), sizeof(Tile) * tiles.size(), cudaMemcpyHostToDevice, st));
   WaveArgs a;
-  a.sc = s->view();
-  a.pts = d_pts;
-  a.valid = valid;
-  a.spp = (uint32_t)spp;
-  a.seed = cfg->seed;
-  a.sample_offset = (uint32_t)cfg->sample_offset;
-  a.nls = nls;
-  a.bounces = B;
+  a.bakes = d_items;
+  a.n_bakes = nb;
+  a.NLS = NLS;
   for (int k = 0; k < 2; ++k) {
     float4* base = c->scratch[12 + k].as<float4>();
     a.ext[k] = ExtQueue{base, base + ext_cap, base + 2 * ext_cap};
@@ -714,82 +883,110 @@ shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int 
   }
   a.path_L = c->scratch[16].as<float4>();
   a.nee_li = c->scratch[17].as<float4>();
-  a.nee_dir = a.nee_li + P * nls;
+  a.nee_dir = a.nee_li + std::max<int64_t>(Pmax, 1) * NLS;
+  a.info = c->scratch[18].as<PathInfo>();
   a.cnt = cnt;
-  a.sh_out = d_sh;
-  a.env_out = d_env;
   a.ext_cap = (int)ext_cap;
   a.sh_cap = (int)sh_cap;
+  a.det = det ? 1 : 0;
+  a.slots = slots;
+  a.pend = det ? c->scratch[24].as<float4>() : nullptr;
 
-  const BvhView bvh = s->bvh();
-  const int tgrid = traversal_grid(c->device);
+  const int tgrid = traversal_grid(c->device) * std::max(1, prm.grid_scale);
   const int sgrid = 148 * 8;
-  cudaEvent_t ev[2] = {nullptr, nullptr};
-  double ext_ms = 0.0, sh_ms = 0.0;
+  const bool timed = c->profiling && !prm.use_graph;
+  struct Pair {
+    cudaEvent_t a, b;
+    int kind;
+  };
+  std::vector<Pair> timed_pairs;
+  auto stamp = [&](int kind) -> Pair {
+    Pair p{nullptr, nullptr, kind};
+    if (timed) {
+      cudaEventCreate(&p.a);
+      cudaEventCreate(&p.b);
+      cudaEventRecord(p.a, st);
+    }
+    return p;
+  };
+  auto close_stamp = [&](Pair p) {
+    if (timed) {
+      cudaEventRecord(p.b, st);
+      timed_pairs.push_back(p);
+    }
+  };
   uint64_t ext_launches = 0, sh_launches = 0;
-  std::vector<cudaEvent_t> evs;
+  cudaEvent_t t_begin = nullptr, t_end = nullptr;
   if (c->profiling) {
-    cudaEventCreate(&ev[0]);
-    cudaEventCreate(&ev[1]);
-    cudaEventRecord(ev[0], st);
+    cudaEventCreate(&t_begin);
+    cudaEventCreate(&t_end);
+    cudaEventRecord(t_begin, st);
   }
-  int waves = 0;
-  struct Pair { cudaEvent_t a, b; int kind; };
-  std::vector<Pair> timed;
-  for (int64_t t0 = 0; t0 < n_valid; t0 += tex_per_wave) {
-    a.t0 = (uint32_t)t0;
-    a.n_tex = (uint32_t)((n_valid - t0) < tex_per_wave ? (n_valid - t0) : tex_per_wave);
-    SHB_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * CNT_FETCH_SHADOW + sizeof(int), st));
-    k_generate<<<grid_for((int64_t)a.n_tex * spp), kThreads, 0, st>>>(a);
-    count_launch(c);
-    for (int k = 0; k <= B; ++k) {
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  if (prm.use_graph) SHB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  uint64_t launches = 0;
+  for (const Wave& w : waves) {
+    a.tiles = d_tiles + w.tile_begin;
+    a.n_tiles = w.n_tiles;
+    a.P = w.P;
+    a.n_tex = w.n_tex;
+    cudaMemsetAsync(cnt, 0, sizeof(int) * (CNT_FETCH_SHADOW + 1), st);
+    k_generate<<<grid_for(w.P), kThreads, 0, st>>>(a);
+    launches++;
+    for (int k = 0; k <= w.max_bounces; ++k) {
       int cur = k & 1, nxt = cur ^ 1;
-      SHB_CUDA(cudaMemsetAsync(cnt + nxt, 0, sizeof(int), st));
-      SHB_CUDA(cudaMemsetAsync(cnt + CNT_FETCH_EXT, 0, sizeof(int) * 2, st));
-      Pair pe{nullptr, nullptr, 0};
-      if (c->profiling) {
-        cudaEventCreate(&pe.a);
-        cudaEventCreate(&pe.b);
-        cudaEventRecord(pe.a, st);
-      }
-      launch_extend(st, tgrid, bvh, a.ext[cur], cnt + cur, a.ext_cap, a.hits, cnt + CNT_FETCH_EXT, cnt + CNT_ERROR, c64);
-      if (c->profiling) {
-        cudaEventRecord(pe.b, st);
-        timed.push_back(pe);
-      }
-      k_shade<<<sgrid, kThreads, 0, st>>>(a, cur, k, k < B ? 1 : 0);
-      Pair ps{nullptr, nullptr, 1};
-      if (c->profiling) {
-        cudaEventCreate(&ps.a);
-        cudaEventCreate(&ps.b);
-        cudaEventRecord(ps.a, st);
-      }
-      launch_shadow(st, tgrid, bvh, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, cnt + CNT_FETCH_SHADOW,
+      cudaMemsetAsync(cnt + nxt, 0, sizeof(int), st);
+      cudaMemsetAsync(cnt + CNT_FETCH_EXT, 0, sizeof(int) * 2, st);
+      Pair pe = stamp(0);
+      launch_extend(st, tgrid, d_items, nb, a.info, a.ext[cur], cnt + cur, a.ext_cap, a.hits, cnt + CNT_FETCH_EXT,
                     cnt + CNT_ERROR, c64);
-      if (c->profiling) {
-        cudaEventRecord(ps.b, st);
-        timed.push_back(ps);
+      close_stamp(pe);
+      k_shade<<<sgrid, kThreads, 0, st>>>(a, cur, k);
+      Pair ps = stamp(1);
+      launch_shadow(st, tgrid, d_items, nb, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, a.pend,
+                    cnt + CNT_FETCH_SHADOW, cnt + CNT_ERROR, c64);
+      close_stamp(ps);
+      cudaMemsetAsync(cnt + CNT_SHADOW, 0, sizeof(int), st);
+      launches += 3;
+      if (det) {
+        k_commit<<<grid_for(w.P), kThreads, 0, st>>>(a, k);
+        launches++;
       }
-      SHB_CUDA(cudaMemsetAsync(cnt + CNT_SHADOW, 0, sizeof(int), st));
-      count_launch(c, 3);
       ext_launches++;
       sh_launches++;
     }
-    k_resolve<<<grid_for((int64_t)a.n_tex * 32), kThreads, 0, st>>>(a);
-    count_launch(c);
-    SHB_CUDA(cudaGetLastError());
-    waves++;
+    k_resolve<<<grid_for(w.n_tex * 32), kThreads, 0, st>>>(a);
+    launches++;
   }
+  if (prm.use_graph) {
+    cudaError_t e = cudaStreamEndCapture(st, &graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+      cudaGraphDestroy(graph);
+      return cuda_fail(e, "cudaGraphInstantiate");
+    }
+    e = cudaGraphLaunch(exec, st);
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGraphLaunch");
+  }
+  count_launch(c, launches);
+  SHB_CUDA(cudaGetLastError());
   int err = 0;
   Counters64 h64{0, 0};
   SHB_CUDA(cudaMemcpyAsync(&err, cnt + CNT_ERROR, sizeof(int), cudaMemcpyDeviceToHost, st));
   SHB_CUDA(cudaMemcpyAsync(&h64, c64, sizeof(Counters64), cudaMemcpyDeviceToHost, st));
-  if (c->profiling) cudaEventRecord(ev[1], st);
+  if (c->profiling) cudaEventRecord(t_end, st);
   SHB_CUDA(cudaStreamSynchronize(st));
+  double ext_ms = 0.0, sh_ms = 0.0;
   float total_ms = 0.f;
   if (c->profiling) {
-    cudaEventElapsedTime(&total_ms, ev[0], ev[1]);
-    for (auto& pr : timed) {
+    cudaEventElapsedTime(&total_ms, t_begin, t_end);
+    cudaEventDestroy(t_begin);
+    cudaEventDestroy(t_end);
+    for (auto& pr : timed_pairs) {
       float ms = 0.f;
       cudaEventElapsedTime(&ms, pr.a, pr.b);
       if (pr.kind == 0) ext_ms += ms;
@@ -797,16 +994,19 @@ shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int 
       cudaEventDestroy(pr.a);
       cudaEventDestroy(pr.b);
     }
-    cudaEventDestroy(ev[0]);
-    cudaEventDestroy(ev[1]);
   }
   if (stats) {
-    stats->texel_samples = (uint64_t)n_valid * (uint64_t)spp;
-    stats->valid_texels = (uint64_t)n_valid;
+    uint64_t ts = 0, vt = 0;
+    for (int b = 0; b < nb; ++b) {
+      ts += (uint64_t)n_valid[b] * (uint64_t)specs[b].cfg.samples;
+      vt += (uint64_t)n_valid[b];
+    }
+    stats->texel_samples = ts;
+    stats->valid_texels = vt;
     stats->extend_rays = h64.extend_rays;
     stats->shadow_rays = h64.shadow_rays;
     stats->error_flags = (uint32_t)err;
-    stats->waves = (uint32_t)waves;
+    stats->waves = (uint32_t)waves.size();
     stats->trace_ms = total_ms;
     stats->extend_kernel_ms = ext_ms;
     stats->shadow_kernel_ms = sh_ms;
@@ -814,10 +1014,19 @@ shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int 
     stats->shadow_launches = sh_launches;
   }
   if (err) {
-    set_error(std::string("bounded device failure:") + (err & ERR_STACK ? " traversal stack overflow" : "") + (err & ERR_QUEUE ? " ray queue overflow" : "") + (err & ERR_ITER ? " traversal iteration limit" : ""));
+    set_error(std::string("bounded device failure:") + (err & ERR_STACK ? " traversal stack overflow" : "") +
+              (err & ERR_QUEUE ? " ray queue overflow" : "") + (err & ERR_ITER ? " traversal iteration limit" : ""));
     return SHB_ERR_INTERNAL;
   }
   return SHB_OK;
+}
+
+// BakeSHLightMap on a device G-buffer: a batch of one.
+shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int H, const shb_bake_config* cfg,
+                       float* d_sh, float* d_env, shb_bake_stats* stats) {
+  BakeSpec spec{s, d_pts, W, H, *cfg, d_sh, d_env};
+  BatchParams prm;
+  return bake_batch_device(s->ctx, {spec}, prm, stats);
 }
 
 }  // namespace shb

@@ -135,7 +135,7 @@ struct shb_context {
   cudaStream_t stream = nullptr;
   uint64_t launches = 0;
   // scratch reused across calls
-  shb::DevBuf scratch[24];
+  shb::DevBuf scratch[26];
   shb::DevBuf counters;
   void* host_pinned = nullptr;
   size_t host_pinned_bytes = 0;
@@ -181,6 +181,27 @@ shb_status downsample_device(shb_context* c, const float* in, int w, int h, int 
 shb_status dilate_device(shb_context* c, int kind, int w, int h, void* pixels, uint8_t* mask, int passes);
 shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int H,
                        const shb_bake_config* cfg, float* d_sh, float* d_env, shb_bake_stats* stats);
+
+// One bake of a batch, with device G-buffer and device outputs.
+struct BakeSpec {
+  shb_scene* scene;
+  const shb_surface_point* pts;
+  int W, H;  // supersampled texel dims
+  shb_bake_config cfg;
+  float* sh;
+  float* env;
+};
+
+// Launch-structure parameters (chosen by the autotuner for batches).
+struct BatchParams {
+  int64_t wave_paths = int64_t(1) << 23;  // paths in flight per wave (queue depth)
+  int64_t tile_texels = int64_t(1) << 30; // texels per work tile
+  int grid_scale = 1;                     // traversal grid = grid_scale x SMs x occupancy
+  bool use_graph = false;                 // capture the waves in one CUDA graph
+};
+
+shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs, const BatchParams& prm,
+                             shb_bake_stats* stats);
 shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n, shb_hit* d_hits);
 
 // sRGB -> linear table (computed on the host with powf, colorspace.h:10-14)

@@ -245,12 +245,14 @@ __device__ __forceinline__ void load_ray(TravRay& r, float4 o, float4 d) {
 }
 
 // Persistent queue consumer: lanes refill from the queue as their rays end.
-template <bool SHADOW, class Q, class Fin>
-__device__ __forceinline__ void consume(const BvhView& bvh, const Q& q, int n, int* fetch, int* err, Fin&& finish) {
+// `bvh_of(i, o, d)` gives the BVH of queue entry i (its bake's).
+template <bool SHADOW, class Q, class B, class Fin>
+__device__ __forceinline__ void consume(const Q& q, int n, int* fetch, int* err, B&& bvh_of, Fin&& finish) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   uint2 stack[kStack];
   Walk w;
+  BvhView bvh;
   int ray = -1;
   bool exhausted = false;
   while (true) {
@@ -266,6 +268,7 @@ __device__ __forceinline__ void consume(const BvhView& bvh, const Q& q, int n, i
         if (r < n) {
           ray = r;
           float4 o = q.o[r], d = q.d[r];
+          bvh = bvh_of(r, o, d);
           load_ray(w.r, o, d);
           walk_init(w, bvh, 0.001f, SHADOW ? o.w : INFINITY);
         } else {
@@ -283,26 +286,39 @@ __device__ __forceinline__ void consume(const BvhView& bvh, const Q& q, int n, i
   }
 }
 
-__global__ void __launch_bounds__(kTravThreads) k_extend(BvhView bvh, ExtQueue q, const int* __restrict__ n_ptr, int cap,
+__global__ void __launch_bounds__(kTravThreads) k_extend(const BakeItem* __restrict__ bakes, int n_bakes,
+                                                        const PathInfo* __restrict__ info, ExtQueue q,
+                                                        const int* __restrict__ n_ptr, int cap,
                                                         float4* __restrict__ hits, int* fetch, int* err,
                                                         Counters64* stats) {
   const int n = min(*n_ptr, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&stats->extend_rays, (unsigned long long)n);
-  consume<false>(bvh, q, n, fetch, err, [&](int i, const Walk& w) {
+  const BvhView bvh0 = bakes[0].bvh;
+  auto bvh_of = [&](int, float4 o, float4) {
+    return n_bakes == 1 ? bvh0 : bakes[info[__float_as_uint(o.w)].x].bvh;
+  };
+  consume<false>(q, n, fetch, err, bvh_of, [&](int i, const Walk& w) {
     hits[i] = w.hit ? make_float4(w.tmax, w.u, w.v, __uint_as_float(w.prim))
                     : make_float4(0.f, 0.f, 0.f, __uint_as_float(kMissPrim));
   });
 }
 
-__global__ void __launch_bounds__(kTravThreads) k_shadow(BvhView bvh, ShadowQueue q, const int* __restrict__ n_ptr, int cap,
+__global__ void __launch_bounds__(kTravThreads) k_shadow(const BakeItem* __restrict__ bakes, int n_bakes, ShadowQueue q,
+                                                        const int* __restrict__ n_ptr, int cap,
                                                         float4* __restrict__ path_L, float4* __restrict__ nee_li,
-                                                        int* fetch, int* err, Counters64* stats) {
+                                                        float4* __restrict__ pend, int* fetch, int* err,
+                                                        Counters64* stats) {
   const int n = min(*n_ptr, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&stats->shadow_rays, (unsigned long long)n);
-  consume<true>(bvh, q, n, fetch, err, [&](int i, const Walk& w) {
+  const BvhView bvh0 = bakes[0].bvh;
+  auto bvh_of = [&](int i, float4, float4) {
+    return n_bakes == 1 ? bvh0 : bakes[__float_as_uint(q.c[i].w) >> 2].bvh;
+  };
+  consume<true>(q, n, fetch, err, bvh_of, [&](int i, const Walk& w) {
     float4 c = q.c[i];
     uint32_t target = __float_as_uint(q.d[i].w);
-    if (__float_as_uint(c.w) == 0u) {
+    const uint32_t kind = __float_as_uint(c.w) & 3u;
+    if (kind == 0u) {
       if (!w.hit) {
         float4* L = path_L + target;
         atomicAdd(&L->x, c.x);
@@ -310,7 +326,7 @@ __global__ void __launch_bounds__(kTravThreads) k_shadow(BvhView bvh, ShadowQueu
         atomicAdd(&L->z, c.z);
       }
     } else if (w.hit) {
-      nee_li[target] = make_float4(0.f, 0.f, 0.f, 0.f);
+      (kind == 1u ? nee_li : pend)[target] = make_float4(0.f, 0.f, 0.f, 0.f);
     }
   });
 }
@@ -347,14 +363,14 @@ int traversal_grid(int device) {
   return sms * per_sm;
 }
 
-void launch_extend(cudaStream_t st, int grid, const BvhView& bvh, ExtQueue q, const int* n, int cap, float4* hits,
-                   int* fetch, int* err, Counters64* stats) {
-  k_extend<<<grid, kTravThreads, 0, st>>>(bvh, q, n, cap, hits, fetch, err, stats);
+void launch_extend(cudaStream_t st, int grid, const BakeItem* bakes, int n_bakes, const PathInfo* info, ExtQueue q,
+                   const int* n, int cap, float4* hits, int* fetch, int* err, Counters64* stats) {
+  k_extend<<<grid, kTravThreads, 0, st>>>(bakes, n_bakes, info, q, n, cap, hits, fetch, err, stats);
 }
 
-void launch_shadow(cudaStream_t st, int grid, const BvhView& bvh, ShadowQueue q, const int* n, int cap, float4* path_L,
-                   float4* nee_li, int* fetch, int* err, Counters64* stats) {
-  k_shadow<<<grid, kTravThreads, 0, st>>>(bvh, q, n, cap, path_L, nee_li, fetch, err, stats);
+void launch_shadow(cudaStream_t st, int grid, const BakeItem* bakes, int n_bakes, ShadowQueue q, const int* n, int cap,
+                   float4* path_L, float4* nee_li, float4* pend, int* fetch, int* err, Counters64* stats) {
+  k_shadow<<<grid, kTravThreads, 0, st>>>(bakes, n_bakes, q, n, cap, path_L, nee_li, pend, fetch, err, stats);
 }
 
 void launch_closest_rays(cudaStream_t st, const BvhView& bvh, const shb_ray* rays, int64_t n, float4* hits, int* err) {

@@ -22,7 +22,8 @@ struct ExtQueue {
 //   o = (origin.xyz, tfar), d = (direction.xyz, target bits),
 //   c = (contribution.xyz, kind bits): kind 0 adds c to the path radiance
 //   of `target` when unoccluded; kind 1 clears texel-NEE slot `target`
-//   when occluded.
+//   when occluded; kind 2 clears pending hit-NEE slot `target` when
+//   occluded (deterministic accumulation, see k_commit).
 struct ShadowQueue {
   float4* o;
   float4* d;
@@ -46,11 +47,39 @@ struct Counters64 {
   unsigned long long shadow_rays;
 };
 
+// One bake of a batch (device table entry).  A single BakeSHLightMap call
+// is a batch of one.
+struct BakeItem {
+  SceneView sc;
+  BvhView bvh;
+  const shb_surface_point* pts;  // (W*s) x (H*s) G-buffer
+  const uint32_t* valid;         // compacted indices of valid texels
+  float* sh_out;                 // 27 floats per texel
+  float* env_out;
+  uint32_t spp, seed, sample_offset;
+  int32_t nls, bounces, pad;
+};
+
+// A tile of a wave: texel slots [t0, t0 + n_tex) of bake `bake` with all
+// their samples; its paths start at `path_off` and its texels at `tex_off`
+// within the wave.
+struct Tile {
+  uint32_t bake, t0, n_tex, spp;
+  int64_t path_off;
+  int64_t tex_off;
+};
+
+// Per-path record written by generate: (bake, texel, sample, unused).
+using PathInfo = uint4;
+
+// Shadow-queue kind bits: bits 0-1 = kind (0 path radiance, 1 texel-NEE
+// slot, 2 pending hit-NEE slot), bits 2.. = bake index.
+
 // Launch helpers for the persistent traversal kernels (traverse.cu).
-void launch_extend(cudaStream_t st, int grid, const BvhView& bvh, ExtQueue q, const int* n, int cap, float4* hits,
-                   int* fetch, int* err, Counters64* stats);
-void launch_shadow(cudaStream_t st, int grid, const BvhView& bvh, ShadowQueue q, const int* n, int cap, float4* path_L,
-                   float4* nee_li, int* fetch, int* err, Counters64* stats);
+void launch_extend(cudaStream_t st, int grid, const BakeItem* bakes, int n_bakes, const PathInfo* info, ExtQueue q,
+                   const int* n, int cap, float4* hits, int* fetch, int* err, Counters64* stats);
+void launch_shadow(cudaStream_t st, int grid, const BakeItem* bakes, int n_bakes, ShadowQueue q, const int* n, int cap,
+                   float4* path_L, float4* nee_li, float4* pend, int* fetch, int* err, Counters64* stats);
 void launch_closest_rays(cudaStream_t st, const BvhView& bvh, const shb_ray* rays, int64_t n, float4* hits,
                          int* err);
 int traversal_grid(int device);

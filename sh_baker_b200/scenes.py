@@ -61,37 +61,68 @@ class Patch:
         return 2.0 * math.pi * self.radius, self.height
 
 
+def _shelf_try(order, cws, chs, res: int, padding: int):
+    rects = [None] * len(cws)
+    x = y = shelf_h = 0
+    for i in order:
+        cw, ch = cws[i], chs[i]
+        ow, oh = cw + padding, ch + padding
+        if ow > res:
+            return None
+        if x + ow > res:
+            x = 0
+            y += shelf_h
+            shelf_h = 0
+        if y + oh > res:
+            return None
+        rects[i] = (x + padding // 2, y + padding // 2, cw, ch)
+        x += ow
+        if oh > shelf_h:
+            shelf_h = oh
+    return rects
+
+
 def shelf_pack(sizes: List[Tuple[float, float]], res: int, padding: int):
     """Packs world-size charts into a res x res atlas at one texel density.
-    Returns (texel_size, [(x0, y0, cw, ch)]) in texels."""
+    The density starts at 55 % fill and coarsens by 4 % steps until the
+    shelves fit.  Returns (texel_size, [(x0, y0, cw, ch)]) in texels."""
+    if len(sizes) * (1 + padding) ** 2 > res * res:
+        raise RuntimeError("chart packing failed")
     total = sum(w * h for w, h in sizes)
-    s = math.sqrt(total / (res * res * 0.55)) if total > 0 else 1.0
+    s0 = math.sqrt(total / (res * res * 0.55)) if total > 0 else 1.0
     order = sorted(range(len(sizes)), key=lambda i: -sizes[i][1])
-    for _ in range(200):
-        rects = [None] * len(sizes)
-        x = y = shelf_h = 0
-        ok = True
-        for i in order:
-            cw = max(1, int(math.ceil(sizes[i][0] / s)))
-            ch = max(1, int(math.ceil(sizes[i][1] / s)))
-            ow, oh = cw + padding, ch + padding
-            if ow > res:
-                ok = False
-                break
-            if x + ow > res:
-                x = 0
-                y += shelf_h
-                shelf_h = 0
-            if y + oh > res:
-                ok = False
-                break
-            rects[i] = (x + padding // 2, y + padding // 2, cw, ch)
-            x += ow
-            shelf_h = max(shelf_h, oh)
-        if ok:
+    W = np.array([w for w, _ in sizes], np.float64)
+    H = np.array([h for _, h in sizes], np.float64)
+
+    def attempt(k):
+        s = s0 * (1.04 ** k) if k else s0
+        # the same arithmetic as a scalar loop: ceil(size / s), at least 1
+        cws = [max(1, int(math.ceil(w / s))) for w in W.tolist()]
+        chs = [max(1, int(math.ceil(h / s))) for h in H.tolist()]
+        return s, _shelf_try(order, cws, chs, res, padding)
+
+    for k in range(12):  # most atlases fit within a few steps
+        s, rects = attempt(k)
+        if rects is not None:
             return s, rects
-        s *= 1.04
-    raise RuntimeError("chart packing failed")
+    lo, hi, step, k = 11, None, 1, 12
+    while k < 200:  # grow the step exponentially, then bisect
+        if attempt(k)[1] is not None:
+            hi = k
+            break
+        lo = k
+        step *= 2
+        k = lo + step if lo < 199 else 200
+        k = min(k, 199) if lo < 199 else k
+    if hi is None:
+        raise RuntimeError("chart packing failed")
+    while hi - lo > 1:
+        mid = (lo + hi) // 2
+        if attempt(mid)[1] is not None:
+            hi = mid
+        else:
+            lo = mid
+    return attempt(hi)
 
 
 class MeshBuilder:
@@ -172,9 +203,27 @@ class MeshBuilder:
         return out
 
 
+def grid_pack(sizes: List[Tuple[float, float]], res: int):
+    """Fallback for atlases too small for one texel-aligned chart per patch:
+    a uniform grid of cells, each patch scaled into its cell (charts may be
+    smaller than a texel; the rasteriser's centroid rule then covers them)."""
+    n = len(sizes)
+    cols = max(1, int(math.ceil(math.sqrt(n))))
+    cell = res / cols
+    rects = []
+    for i, (w, h) in enumerate(sizes):
+        s = 0.8 * cell / max(w, h, 1e-9)
+        cx, cy = (i % cols) * cell, (i // cols) * cell
+        rects.append((cx + 0.1 * cell, cy + 0.1 * cell, w * s, h * s))
+    return rects
+
+
 def build_from_patches(patches: List[Patch], material_ids: List[int], res: int, padding: int) -> List[Geometry]:
     sizes = [p.world_size() for p in patches]
-    _, rects = shelf_pack(sizes, res, padding)
+    try:
+        _, rects = shelf_pack(sizes, res, padding)
+    except RuntimeError:
+        rects = grid_pack(sizes, res)
     mb = MeshBuilder(len(material_ids))
     for p, r in zip(patches, rects):
         mb.add_patch(p, r, res)
@@ -235,6 +284,59 @@ def unit_quad() -> Scene:
     return Scene([g], [Material(name="grey")], lights)
 
 
+def _box_faces(lo: np.ndarray, hi: np.ndarray, inward: bool):
+    """The six (corner, eu, ev) faces of each box, in box_patches' order,
+    eu x ev pointing out of the box (or into it when inward)."""
+    d = hi - lo
+    n = len(lo)
+    X = np.zeros((n, 3)); X[:, 0] = d[:, 0]
+    Y = np.zeros((n, 3)); Y[:, 1] = d[:, 1]
+    Z = np.zeros((n, 3)); Z[:, 2] = d[:, 2]
+    corners = np.stack([lo, lo + X, lo, lo + Y, lo, lo + Z], 1)
+    eu = np.stack([Z, Y, X, Z, Y, X], 1)
+    ev = np.stack([Y, Z, Z, X, X, Y], 1)
+    if inward:
+        eu, ev = ev, eu
+    return corners.reshape(-1, 3), eu.reshape(-1, 3), ev.reshape(-1, 3)
+
+
+def _box_geometries(corners, eu, ev, n_geoms: int, material_ids: List[int], res: int, padding: int):
+    """Axis-aligned single-quad charts (6 per geometry), packed and turned
+    into geometries with the same arithmetic as MeshBuilder.add_patch."""
+    wu = np.abs(eu).max(1)  # |eu| of an axis-aligned vector, exact
+    wv = np.abs(ev).max(1)
+    sizes = list(zip(wu.tolist(), wv.tolist()))
+    try:
+        _, rects = shelf_pack(sizes, res, padding)
+    except RuntimeError:
+        rects = grid_pack(sizes, res)
+    R = np.asarray(rects, np.float64)
+    x0, y0, cw, ch = R[:, 0:1], R[:, 1:2], R[:, 2:3], R[:, 3:4]
+    A = np.array([0.0, 1.0, 0.0, 1.0])
+    B = np.array([0.0, 0.0, 1.0, 1.0])
+    pos = corners[:, None, :] + A[None, :, None] * eu[:, None, :] + B[None, :, None] * ev[:, None, :]
+    cr = np.cross(eu, ev)
+    nrm = cr / np.sqrt((cr * cr).sum(1))[:, None]
+    tan = eu / np.sqrt((eu * eu).sum(1))[:, None]
+    luv = np.stack([(x0 + A[None, :] * cw) / res, (y0 + B[None, :] * ch) / res], 2)
+    nf = len(corners)
+    V = pos.astype(np.float32)
+    N = np.repeat(nrm[:, None, :], 4, 1).astype(np.float32)
+    T = np.concatenate([np.repeat(tan[:, None, :], 4, 1), np.ones((nf, 4, 1))], 2).astype(np.float32)
+    TUV = np.repeat(np.stack([A, B], 1)[None], nf, 0).astype(np.float32)
+    LUV = luv.astype(np.float32)
+    quad = np.array([0, 1, 3, 0, 3, 2], np.uint32)
+    out = []
+    per = nf // n_geoms
+    for g in range(n_geoms):
+        f = slice(g * per, (g + 1) * per)
+        idx = (quad[None, :] + 4 * np.arange(per, dtype=np.uint32)[:, None]).reshape(-1)
+        out.append(Geometry(vertices=V[f].reshape(-1, 3), indices=idx, normals=N[f].reshape(-1, 3),
+                            texture_uvs=TUV[f].reshape(-1, 2), lightmap_uvs=LUV[f].reshape(-1, 2),
+                            tangents=T[f].reshape(-1, 4), material_id=material_ids[g]))
+    return out
+
+
 def procedural_room(seed: int = 2, n_boxes: int = 200, res: int = 1024, padding: int = 2,
                     n_materials: int = 8, n_point_lights: int = 4, box_subdiv: int = 1) -> Scene:
     """Closed 10x3x10 room (12 inward triangles) plus `n_boxes` axis-aligned
@@ -244,14 +346,25 @@ def procedural_room(seed: int = 2, n_boxes: int = 200, res: int = 1024, padding:
     rng = np.random.default_rng(seed)
     mats = [solid_material(rng.uniform(0.1, 0.9, 3), name=f"m{i}") for i in range(n_materials)]
     room_lo, room_hi = np.array([-5.0, 0.0, -5.0]), np.array([5.0, 3.0, 5.0])
-    patches = box_patches(0, room_lo, room_hi, inward=True)
     mat_ids = [0]
+    los, his = [], []
     for b in range(n_boxes):
         size = rng.uniform(0.1, 1.0, 3)
         lo = rng.uniform(room_lo, room_hi - size)
-        patches += box_patches(b + 1, lo, lo + size, inward=False, subdiv=box_subdiv)
+        los.append(lo)
+        his.append(lo + size)
         mat_ids.append(int(rng.integers(0, n_materials)))
-    geoms = build_from_patches(patches, mat_ids, res, padding)
+    if box_subdiv == 1:
+        rc, ru, rv = _box_faces(room_lo[None], room_hi[None], inward=True)
+        if n_boxes:
+            bc, bu, bv = _box_faces(np.array(los), np.array(his), inward=False)
+            rc, ru, rv = np.vstack([rc, bc]), np.vstack([ru, bu]), np.vstack([rv, bv])
+        geoms = _box_geometries(rc, ru, rv, n_boxes + 1, mat_ids, res, padding)
+    else:
+        patches = box_patches(0, room_lo, room_hi, inward=True)
+        for b in range(n_boxes):
+            patches += box_patches(b + 1, los[b], his[b], inward=False, subdiv=box_subdiv)
+        geoms = build_from_patches(patches, mat_ids, res, padding)
     d = _normalize([rng.uniform(-0.5, 0.5), -1.0, rng.uniform(-0.5, 0.5)])
     lights = [Light(type=DIRECTIONAL, direction=tuple(float(x) for x in d), intensity=3.0)]
     for _ in range(n_point_lights):
@@ -376,3 +489,22 @@ def atrium(seed: int = 3, res: int = 2048, padding: int = 2, column_segments: Tu
                                   intensity=float(rng.uniform(5.0, 50.0))))
     mark_area_lights(scene)
     return scene
+
+
+def batched_mix(seed: int = 4, n: int = 64):
+    """The batched-bake mix: `n` independent procedural rooms with triangle
+    counts log-uniform in [1k, 100k], lightmaps of {128, 256, 512, 1024}^2,
+    {32, 64, 128, 256} spp, 2-4 bounces and 1-8 point lights each.  Returns
+    a list of dicts (scene, width, height, spp, bounces, seed)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        tris = math.exp(rng.uniform(math.log(1_000), math.log(100_000)))
+        n_boxes = max(1, int(round((tris - 12) / 12)))
+        res = int(rng.choice([128, 256, 512, 1024]))
+        spp = int(rng.choice([32, 64, 128, 256]))
+        bounces = int(rng.integers(2, 5))
+        lights = int(rng.integers(1, 9))
+        sc = procedural_room(seed=1000 + i, n_boxes=n_boxes, res=res, n_point_lights=lights)
+        out.append({"scene": sc, "width": res, "height": res, "spp": spp, "bounces": bounces, "seed": 77 + i})
+    return out
