@@ -283,6 +283,115 @@ def run_batched(args):
     ctx.close()
 
 
+def run_adjoint(args):
+    """Adjoint bake: procedural room (2,412 triangles) at lightmap 512^2,
+    supersample 3 (the room workload's), 64 spp, 3 bounces.  Loss = sum (SH - SH_target)^2 with the
+    target baked at albedos x U[0.8, 1.2] and light intensities x U[0.5, 2].
+    A step = forward bake + dLoss/dSH + path-replay backward; both halves are
+    timed with CUDA events.  The gradient of all 8x3 albedos and 5 intensities
+    is compared with central differences (h = 1e-3, common random numbers)."""
+    import numpy as np
+    import torch
+
+    from oracle.pyoracle import srgb_to_linear
+    from sh_baker_b200 import api, scenes
+    from sh_baker_b200 import build as B
+    B.build()
+    torch.cuda.set_device(0)
+    res, spp, bounces = 512, 64, 3
+    sc = scenes.procedural_room(seed=2, res=res)
+    ctx = api.Context(device=0)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    ds = api.DeviceScene(ctx, sc)
+    rc = api.RasterConfig(res, res, 3)
+    g = api.rasterize_to_device(ds, rc)
+    bake = api.BatchBake(ds, g, rc, api.BakeConfig(samples=spp, bounces=bounces, seed=2))
+    lut = np.array([srgb_to_linear(i) for i in range(256)], np.float32)
+    albedo = np.stack([lut[m.albedo.pixel_data[:3]] for m in sc.materials]).astype(np.float32)
+    inten = np.array([l.intensity for l in sc.lights], np.float32)
+    rng = np.random.default_rng(5)
+    n = g.width * g.height
+    sh = torch.empty(n * 27, dtype=torch.float32, device="cuda")
+    env = torch.empty(n, dtype=torch.float32, device="cuda")
+    target = torch.empty_like(sh)
+    ds.set_params(albedo * rng.uniform(0.8, 1.2, albedo.shape).astype(np.float32),
+                  inten * rng.uniform(0.5, 2.0, inten.shape).astype(np.float32))
+    api.bake_plain_device(bake, target, env)
+    ds.set_params(albedo, inten)
+
+    def ev():
+        return torch.cuda.Event(enable_timing=True)
+
+    def step():
+        e0, e1, e2 = ev(), ev(), ev()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            st = api.bake_plain_device(bake, sh, env)
+            e1.record(stream)
+            dsh = 2.0 * (sh - target)
+        d_alb, d_li = api.Backward(bake, dsh)
+        e2.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), e1.elapsed_time(e2), st.texel_samples, (d_alb, d_li)
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(0)
+    clocks.start()
+    l0 = ctx.kernel_launches()
+    f_ms = b_ms = 0.0
+    ts = 0
+    for _ in range(args.steps):
+        fm, bm, t, grads = step()
+        f_ms += fm
+        b_ms += bm
+        ts += t
+    launches = ctx.kernel_launches() - l0
+    clk = clocks.stop()
+    # central differences under common random numbers (same seed)
+
+    def loss(a, i):
+        ds.set_params(a, i)
+        with torch.cuda.stream(stream):
+            api.bake_plain_device(bake, sh, env)
+            v = float(((sh.double() - target.double()) ** 2).sum())
+        return v
+
+    h = 1e-3
+    fd_alb = np.zeros_like(albedo, dtype=np.float64)
+    fd_li = np.zeros_like(inten, dtype=np.float64)
+    for m in range(albedo.shape[0]):
+        for c in range(3):
+            ap, am = albedo.copy(), albedo.copy()
+            ap[m, c] += h
+            am[m, c] -= h
+            fd_alb[m, c] = (loss(ap, inten) - loss(am, inten)) / (float(ap[m, c]) - float(am[m, c]))
+    for l in range(len(inten)):
+        ip, im = inten.copy(), inten.copy()
+        ip[l] *= 1 + h
+        im[l] *= 1 - h
+        fd_li[l] = (loss(albedo, ip) - loss(albedo, im)) / (float(ip[l]) - float(im[l]))
+    ds.set_params(albedo, inten)
+    d_alb, d_li = grads
+    got = np.concatenate([d_alb.reshape(-1), d_li * inten])
+    fd = np.concatenate([fd_alb.reshape(-1), fd_li * inten])
+    rel = float(np.linalg.norm(got - fd) / np.linalg.norm(fd))
+    worst = float(np.max(np.abs(got - fd)) / np.max(np.abs(fd)))
+    line = {"metric": METRIC, "value": ts / (b_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": (f_ms + b_ms) / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "adjoint bake: procedural room 2,412 triangles, lightmap 512x512, supersample 3, "
+                                   "64 spp, 3 bounces; loss sum (SH - SH_target)^2, 8x3 albedos + 5 intensities",
+                       "texel_samples_per_step": ts // args.steps},
+            "forward_ms": f_ms / args.steps, "backward_ms": b_ms / args.steps,
+            "backward_over_forward": b_ms / f_ms,
+            "fd_check": {"h": h, "rel_l2_err": rel, "max_err_over_max": worst},
+            "gpu_launches": int(launches), "clocks": clk}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def config_of(w, scene):
     return {"workload": f"procedural {w['kind']}: {scene.triangle_count} triangles, lightmap {w['width']}x{w['height']}"
                         f" supersample {w['ss']}, {w['spp']} spp, {w['bounces']} bounces, dilation {w['dilation']}",
@@ -299,15 +408,15 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="room", choices=sorted(WORKLOADS) + ["batched"])
+    ap.add_argument("--workload", default="room", choices=sorted(WORKLOADS) + ["batched", "adjoint"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=5.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     args = ap.parse_args()
-    if args.workload == "batched":
+    if args.workload in ("batched", "adjoint"):
         if args.impl == "ours" and int(os.environ.get("RANK", "0")) == 0:
-            run_batched(args)
+            (run_batched if args.workload == "batched" else run_adjoint)(args)
         return
     w = WORKLOADS[args.workload]
 

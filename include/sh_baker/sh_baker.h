@@ -350,6 +350,103 @@ inline Texture32F DownsampleEnvironmentVisibilityTexture(const Texture32F& input
   return out;
 }
 
+// ---- differentiable bake (no counterpart in the reference) ------------------
+
+// Adjoint parameters: a linear base colour per material that replaces its
+// albedo texture, and an intensity per light.  Empty vectors keep the
+// scene's own values.
+struct BakeParams {
+  std::vector<Vector3f> albedo;
+  std::vector<float> light_intensity;
+};
+
+// dLoss / d BakeParams: 3 per material (materials without an override: 0)
+// and 1 per light (area lights: 0; their radiance is the emissive
+// material's albedo times its emission).
+struct BakeGradients {
+  std::vector<double> d_albedo;
+  std::vector<double> d_light_intensity;
+};
+
+namespace detail {
+inline void set_params(shb_scene* s, const Scene& scene, const BakeParams& p) {
+  if (!p.albedo.empty() && p.albedo.size() != scene.materials.size())
+    throw Error(SHB_ERR_INVALID_ARG, "BakeParams::albedo: one entry per material");
+  if (!p.light_intensity.empty() && p.light_intensity.size() != scene.lights.size())
+    throw Error(SHB_ERR_INVALID_ARG, "BakeParams::light_intensity: one entry per light");
+  std::vector<float> rgb;
+  for (const Vector3f& a : p.albedo)
+    for (int k = 0; k < 3; ++k) rgb.push_back(a[k]);
+  check(shb_scene_set_params(s, rgb.empty() ? nullptr : rgb.data(), nullptr,
+                             p.light_intensity.empty() ? nullptr : p.light_intensity.data()));
+}
+inline shb_bake_config bake_config(const BakeConfig& config, uint32_t seed) {
+  shb_bake_config bc{};
+  bc.samples = config.samples;
+  bc.bounces = config.bounces;
+  bc.num_light_samples = config.num_light_samples;
+  bc.seed = seed;
+  bc.rng_mode = SHB_RNG_PHILOX;
+  return bc;
+}
+}  // namespace detail
+
+// BakeSHLightMap with adjoint parameters applied.
+inline BakeResult BakeSHLightMap(const Scene& scene, const std::vector<SurfacePoint>& surface_points,
+                                 const RasterConfig& raster_config, const BakeConfig& config,
+                                 const BakeParams& params, uint32_t seed = 12345) {
+  detail::SceneHandle s;
+  detail::upload(scene, &s);
+  detail::set_params(s.s, scene, params);
+  const int W = raster_config.width * raster_config.supersample_scale;
+  const int H = raster_config.height * raster_config.supersample_scale;
+  BakeResult r;
+  r.sh_texture.width = W;
+  r.sh_texture.height = H;
+  r.sh_texture.pixels.resize((size_t)W * H);
+  r.environment_visibility_texture.width = W;
+  r.environment_visibility_texture.height = H;
+  r.environment_visibility_texture.pixel_data.resize((size_t)W * H);
+  shb_gbuffer* g = nullptr;
+  check(shb_gbuffer_upload(detail::context(), reinterpret_cast<const shb_surface_point*>(surface_points.data()), W,
+                           H, &g));
+  shb_raster_config rc{raster_config.width, raster_config.height, raster_config.supersample_scale};
+  shb_bake_config bc = detail::bake_config(config, seed);
+  shb_bake_output out{reinterpret_cast<float*>(r.sh_texture.pixels.data()),
+                      r.environment_visibility_texture.pixel_data.data(), 0, 0};
+  shb_status st = shb_bake(s.s, g, &rc, &bc, &out, nullptr);
+  shb_gbuffer_destroy(g);
+  check(st);
+  return r;
+}
+
+// Path-replay adjoint of the bake above: d_sh = dLoss/dSH per texel of the
+// supersampled G-buffer; returns dLoss/d params.  Same seed, same paths.
+inline BakeGradients Backward(const Scene& scene, const std::vector<SurfacePoint>& surface_points,
+                              const RasterConfig& raster_config, const BakeConfig& config,
+                              const BakeParams& params, const SHTexture& d_sh, uint32_t seed = 12345) {
+  const int W = raster_config.width * raster_config.supersample_scale;
+  const int H = raster_config.height * raster_config.supersample_scale;
+  if (d_sh.pixels.size() != (size_t)W * H || surface_points.size() != (size_t)W * H)
+    throw Error(SHB_ERR_INVALID_ARG, "Backward: d_sh and surface_points must have W*s x H*s texels");
+  detail::SceneHandle s;
+  detail::upload(scene, &s);
+  detail::set_params(s.s, scene, params);
+  shb_gbuffer* g = nullptr;
+  check(shb_gbuffer_upload(detail::context(), reinterpret_cast<const shb_surface_point*>(surface_points.data()), W,
+                           H, &g));
+  shb_raster_config rc{raster_config.width, raster_config.height, raster_config.supersample_scale};
+  shb_bake_config bc = detail::bake_config(config, seed);
+  BakeGradients out;
+  out.d_albedo.assign(3 * scene.materials.size(), 0.0);
+  out.d_light_intensity.assign(scene.lights.size(), 0.0);
+  shb_status st = shb_backward(s.s, g, &rc, &bc, reinterpret_cast<const float*>(d_sh.pixels.data()), 0,
+                               out.d_albedo.data(), out.d_light_intensity.data(), nullptr);
+  shb_gbuffer_destroy(g);
+  check(st);
+  return out;
+}
+
 // ---- src/dilation.h:14-16 --------------------------------------------------
 
 template <typename T>

@@ -295,6 +295,36 @@ typedef struct shb_batch_options {
 SHB_API shb_status shb_bake_batch(shb_context* ctx, const shb_batch_item* items, int32_t count,
                                   const shb_batch_options* options, shb_bake_stats* stats);
 
+/* ---- Differentiable bake (no counterpart in the reference) ------------ */
+
+/* Adjoint parameters.  albedo_rgb (material_count x 3, nullable): a linear
+ * base colour that replaces the albedo texture lookup of every material with
+ * use_override[m] != 0 (use_override NULL: all materials; alpha still comes
+ * from the texture).  light_intensity (light_count, nullable) replaces
+ * shb_light_desc.intensity.  Materials without an override keep their
+ * texture and get no gradient.  The BVH is not rebuilt. */
+SHB_API shb_status shb_scene_set_params(shb_scene* scene, const float* albedo_rgb,
+                                        const uint8_t* use_override, const float* light_intensity);
+
+/* Path-replay adjoint of shb_bake with the same G-buffer and config:
+ * regenerates every path from its counter-based random stream (nothing is
+ * stored by the forward bake) and accumulates, for Loss with
+ * dLoss/dSH = d_sh (27 floats per texel of the W*s x H*s G-buffer; device
+ * memory when device_ptr, else host):
+ *   d_albedo[3m + c] = dLoss / d albedo_rgb[3m + c]  (override materials,
+ *                      through reflection, hit NEE, depth-0 emission and
+ *                      area-light emission; 0 elsewhere)
+ *   d_light[l]       = dLoss / d intensity of point, spot and directional
+ *                      lights (area lights: 0, their radiance is the
+ *                      emissive material's albedo x emission)
+ * as host arrays.  Light-selection probabilities are held constant (the
+ * estimator of the gradient of the expected bake).  At most 16 bounces and
+ * 12288 parameters (3 x materials + lights). */
+SHB_API shb_status shb_backward(shb_scene* scene, const shb_gbuffer* gbuffer,
+                                const shb_raster_config* raster, const shb_bake_config* config,
+                                const float* d_sh, int32_t device_ptr, double* d_albedo,
+                                double* d_light, shb_bake_stats* stats);
+
 /* ---- DownsampleTexture (src/baker.cpp:151-182) ------------------------ */
 
 /* Box average over scale x scale blocks including invalid texels; channels

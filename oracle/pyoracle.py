@@ -66,6 +66,9 @@ def lib():
         f.oracle_sample_area_light.argtypes = [vp, C.c_int, C.c_uint32, vp]
         f.oracle_light_radiance_unit_brdf.argtypes = [vp, C.c_int, vp, vp, vp, vp]
         f.oracle_philox4x32_10.argtypes = [vp, vp, vp]
+        f.oracle_scene_set_params.argtypes = [vp, vp, vp, vp]
+        f.oracle_bake_grad.restype = C.c_int
+        f.oracle_bake_grad.argtypes = [vp, vp, C.POINTER(A.RasterConfig), C.POINTER(BakeArgs), vp, vp, vp]
     return _lib
 
 
@@ -123,6 +126,38 @@ class OracleScene:
             out["var"] = var.reshape(H, W, 9, 3)
             out["mean64"] = m64.reshape(H, W, 9, 3)
         return out
+
+    def set_params(self, albedo=None, light_intensity=None, use_override=None) -> None:
+        nm, nl = len(self.scene.materials), len(self.scene.lights)
+        alb = None if albedo is None else _f(albedo).reshape(nm, 3)
+        use = None if use_override is None else np.ascontiguousarray(use_override, np.uint8).reshape(nm)
+        li = None if light_intensity is None else _f(light_intensity).reshape(nl)
+        lib().oracle_scene_set_params(self.h, None if alb is None else alb.ctypes.data,
+                                      None if use is None else use.ctypes.data, None if li is None else li.ctypes.data)
+
+    def bake_grad(self, points: np.ndarray, width: int, height: int, scale: int, samples: int, bounces: int,
+                  dsh: np.ndarray, seed: int = 12345, num_light_samples: int = 1, subset=None, threads: int = 0,
+                  sample_offset: int = 0):
+        """FP64 forward-mode gradient of sum(dsh * SH): (d_albedo (M, 3), d_light (L,))."""
+        pts = np.ascontiguousarray(points, dtype=SURFACE_POINT_DTYPE)
+        g = np.ascontiguousarray(dsh, np.float32).reshape(-1)
+        if g.size != pts.size * 27:
+            raise ValueError("dsh must hold 27 floats per texel")
+        a = BakeArgs()
+        a.samples, a.bounces, a.num_light_samples = samples, bounces, num_light_samples
+        a.seed, a.sample_offset, a.rng_mode, a.fp64, a.threads = seed & 0xFFFFFFFF, sample_offset, RNG_PHILOX, 1, threads
+        sub = None
+        if subset is not None:
+            sub = np.ascontiguousarray(subset, dtype=np.int64)
+            a.texel_subset = sub.ctypes.data_as(C.POINTER(C.c_int64))
+            a.subset_count = sub.size
+        d_alb = np.zeros((len(self.scene.materials), 3), np.float64)
+        d_li = np.zeros(max(1, len(self.scene.lights)), np.float64)
+        rc = lib().oracle_bake_grad(self.h, pts.ctypes.data, C.byref(A.RasterConfig(width, height, scale)),
+                                    C.byref(a), g.ctypes.data, d_alb.ctypes.data, d_li.ctypes.data)
+        if rc != 0:
+            raise ValueError(f"oracle_bake_grad failed ({rc})")
+        return d_alb, d_li[:len(self.scene.lights)]
 
     def find_occlusion(self, rays: np.ndarray) -> np.ndarray:
         from sh_baker_b200.api import HIT_DTYPE

@@ -121,6 +121,8 @@ struct Mat {
   std::vector<uint8_t> pixels;
   uint32_t w = 0, h = 0, c = 0;
   float emission = 0.f;
+  int use_override = 0;  // adjoint parameter: linear base colour replaces the texture
+  float ovr[3] = {0.f, 0.f, 0.f};
 };
 
 struct Lgt {
@@ -261,6 +263,7 @@ R get_alpha(const Mat& m, V2<R> uv) {
 // material.cpp:69-85
 template <class R>
 V3<R> get_albedo(const Mat& m, V2<R> uv) {
+  if (m.use_override) return V3<R>{(R)m.ovr[0], (R)m.ovr[1], (R)m.ovr[2]};
   V3<R> albedo{R(0.8), R(0.8), R(0.8)};
   if (!m.pixels.empty()) {
     int idx = tex_index(m, uv);
@@ -1227,6 +1230,267 @@ void dilate_t(int w, int h, T* pixels, uint8_t* mask, int passes) {
 }
 }  // namespace
 
+
+// ============================================================ gradient ===
+//
+// FP64 forward-mode derivative of the Philox-stream bake with respect to the
+// adjoint parameters: 3 per material (linear base colour, only materials
+// with an override; channel c of the radiance depends on channel c of the
+// albedo only) and 1 per light (intensity of point, spot and directional
+// lights).  A recursive tracer of its own, structured like trace() above,
+// that carries next to every radiance value its dense tangent.  The
+// light-selection weights are the forward's values and are held constant,
+// so this is the derivative of the estimator of the expected bake.  The loss
+// is linear in the SH output: Loss = sum(dsh * SH).
+
+namespace {
+
+using V3d = V3<double>;
+
+struct GradCtx {
+  const oracle_scene* s;
+  const Bvh<double>* bvh;
+  int max_depth;
+  unsigned nls;
+  int n_mat3, P;
+};
+
+struct Dual {
+  V3d v{};
+  std::vector<V3d> d;
+  explicit Dual(int P) : d((size_t)P) {}
+};
+
+inline void add_scaled(Dual& y, const Dual& x, double a) {
+  y.v += x.v * a;
+  for (size_t p = 0; p < y.d.size(); ++p) y.d[p] += x.d[p] * a;
+}
+
+inline void add_channel(std::vector<V3d>& d, int base, V3d v) {
+  d[base + 0].x += v.x;
+  d[base + 1].y += v.y;
+  d[base + 2].z += v.z;
+}
+
+inline bool is_param(const GradCtx& c, int mat) {
+  return mat >= 0 && mat < (int)c.s->mats.size() && c.s->mats[mat].use_override;
+}
+
+// d(incoming radiance before the BRDF) / d(light parameter): per channel.
+// light = true: the light's intensity (parameter n_mat3 + l); else the
+// emissive material's albedo (parameters 3 mL + c), when it is a parameter.
+struct LightDeriv {
+  V3d dv{};
+  int param = -1;
+  bool light = false;
+};
+
+LightDeriv light_deriv(const GradCtx& c, int li, V3d P, const AreaSample<double>& as, const LightEval<double>& e) {
+  const Lgt& L = c.s->lights[li];
+  LightDeriv out;
+  if (e.cos_n < 0.0) return out;
+  V3d color{L.color.x, L.color.y, L.color.z};
+  if (L.type == SHB_LIGHT_DIRECTIONAL) {
+    out.dv = color;
+    out.param = c.n_mat3 + li;
+    out.light = true;
+    return out;
+  }
+  V3d target = L.type == SHB_LIGHT_AREA ? as.point : V3d{L.position.x, L.position.y, L.position.z};
+  V3d Lv = target - P;
+  double dist = std::sqrt(sqnorm(Lv));
+  if (L.type == SHB_LIGHT_POINT || L.type == SHB_LIGHT_SPOT) {
+    double falloff = 1.0;
+    if (L.type == SHB_LIGHT_SPOT) {
+      V3d u = Lv / dist;
+      double cos_l = dot(V3d{L.direction.x, L.direction.y, L.direction.z}, -u);
+      falloff = std::clamp((cos_l - (double)L.cos_outer) / ((double)L.cos_inner - (double)L.cos_outer), 0.0, 1.0);
+    }
+    out.dv = color / (dist * dist) * falloff;
+    out.param = c.n_mat3 + li;
+    out.light = true;
+    return out;
+  }
+  if (is_param(c, L.material) && c.s->mats[L.material].emission > 0.0f) {
+    double em = c.s->mats[L.material].emission;
+    out.dv = V3d{em, em, em} / (dist * dist);
+    out.param = 3 * L.material;
+  }
+  return out;
+}
+
+inline void add_light_deriv(std::vector<V3d>& d, const LightDeriv& ld, V3d dv) {
+  if (ld.param < 0) return;
+  if (ld.light) d[ld.param] += dv;
+  else add_channel(d, ld.param, dv);
+}
+
+inline void sh_basis(V3d dir, double Y[9]) {
+  V3d acc[9];
+  accumulate_radiance<double>(V3d{1.0, 1.0, 1.0}, dir, acc);
+  for (int k = 0; k < 9; ++k) Y[k] = acc[k].x;
+}
+
+// sum_k g[3k + c] Y_k(dir) * scale, per channel
+inline V3d sh_adjoint(const float* g, V3d dir, double scale) {
+  double Y[9];
+  sh_basis(dir, Y);
+  V3d a{};
+  for (int k = 0; k < 9; ++k) {
+    a.x += (double)g[3 * k] * Y[k];
+    a.y += (double)g[3 * k + 1] * Y[k];
+    a.z += (double)g[3 * k + 2] * Y[k];
+  }
+  return a * scale;
+}
+
+// EvaluateLightSamples (light.cpp:82-189) with tangents.
+Dual light_samples_grad(GradCtx& c, V3d P, V3d N, V3d wo, int mat_id, const Mat& mat, V2<double> uv,
+                        PhiloxEvent ev) {
+  const oracle_scene* s = c.s;
+  size_t nl = s->lights.size();
+  std::vector<LightEval<double>> evs(nl);
+  std::vector<AreaSample<double>> ass(nl);
+  std::vector<float> weights(nl);
+  std::vector<V3d> brdfs(nl);
+  int area_ord = 0;
+  for (size_t i = 0; i < nl; ++i) {
+    const Lgt& L = s->lights[i];
+    if (L.type == SHB_LIGHT_AREA) ass[i] = sample_area_light<double>(s, L, ev, 3 * area_ord++);
+    LightEval<double> e = incoming<double>(L, P, N, &ass[i]);
+    if (e.cos_n < 0.0) {
+      e.radiance = V3d{};
+    } else {
+      brdfs[i] = eval_material<double>(mat, uv, N, e.incident, wo);
+      e.radiance = cmul(e.radiance, e.cos_n * brdfs[i]);
+    }
+    evs[i] = e;
+    weights[i] = (float)max_coeff(e.radiance);
+  }
+  Dual out(c.P);
+  float sum = std::accumulate(weights.begin(), weights.end(), 0.0f);
+  if (sum < 1e-6f) return out;
+  auto picker = ev.picker(weights, sum, 3 * area_ord);
+  const bool own = is_param(c, mat_id);
+  for (unsigned j = 0; j < c.nls; ++j) {
+    int idx = picker.pick((int)j);
+    const LightEval<double>& e = evs[idx];
+    if (occluded(*c.bvh, e.ray_o, e.ray_d, e.tnear, e.tfar)) continue;
+    double joint = (double)weights[idx] / (double)sum * e.area_pdf;
+    if (joint < 1e-3) continue;
+    out.v += e.radiance / joint;
+    if (e.cos_n < 0.0) continue;
+    const bool lit = !(dot(N, wo) <= 0.0 || dot(N, e.incident) <= 0.0);
+    if (own && lit) {
+      LightEval<double> pre = incoming<double>(s->lights[idx], P, N, &ass[idx]);
+      add_channel(out.d, 3 * mat_id, pre.radiance * (e.cos_n / kPi / joint));
+    }
+    LightDeriv ld = light_deriv(c, idx, P, ass[idx], e);
+    add_light_deriv(out.d, ld, cmul(ld.dv, e.cos_n * brdfs[idx]) / joint);
+  }
+  out.v = out.v / (double)c.nls;
+  for (V3d& x : out.d) x = x / (double)c.nls;
+  return out;
+}
+
+// Trace (baker.cpp:70-149) with tangents.
+Dual trace_grad(GradCtx& c, const PhiloxRng& rng, V3d origin, V3d dir, int depth, uint32_t vertex) {
+  Dual color(c.P);
+  if (depth > c.max_depth) return color;
+  Occ<double> occ = find_occlusion<double>(c.s, *c.bvh, origin, dir, 0.001, std::numeric_limits<double>::infinity());
+  if (!occ.hit) return color;
+  static const Mat kDefault{};
+  const bool valid = occ.material_id >= 0 && occ.material_id < (int)c.s->mats.size();
+  const Mat& mat = valid ? c.s->mats[occ.material_id] : kDefault;
+  const int mid = valid ? occ.material_id : -1;
+  double alpha = get_alpha(mat, occ.uv);
+  if (alpha < 1.0) {
+    Dual tr = trace_grad(c, rng, occ.position + dir * 0.001, dir, depth + 1, 2 * vertex + 1);
+    add_scaled(color, tr, 1.0 - alpha);
+  }
+  if (alpha == 0.0) return color;
+  V3d emission = get_emission(mat, occ.uv);
+  if (!is_zero(emission) && depth == 0) {
+    color.v += alpha * emission;
+    if (is_param(c, mid)) add_channel(color.d, 3 * mid, V3d{1.0, 1.0, 1.0} * (alpha * (double)mat.emission));
+  }
+  V3d hit_pos = occ.position + occ.normal * 0.001;
+  Dual direct = light_samples_grad(c, hit_pos, occ.normal, -dir, mid, mat, occ.uv, rng.event(vertex, EV_NEE));
+  add_scaled(color, direct, alpha);
+  ReflSample<double> smp = sample_material<double>(occ.normal, rng.event(vertex, EV_BSDF));
+  if (smp.pdf < 1e-3) return color;
+  Dual inc = trace_grad(c, rng, hit_pos, smp.direction, depth + 1, 2 * vertex);
+  V3d brdf = eval_material<double>(mat, occ.uv, occ.normal, smp.direction, -dir);
+  double k = dot(occ.normal, smp.direction) / smp.pdf;
+  color.v += cmul(inc.v, brdf) * (k * alpha);
+  for (int p = 0; p < c.P; ++p) color.d[p] += cmul(inc.d[p], brdf) * (k * alpha);
+  const bool lit = !(dot(occ.normal, -dir) <= 0.0 || dot(occ.normal, smp.direction) <= 0.0);
+  if (is_param(c, mid) && lit) add_channel(color.d, 3 * mid, inc.v * (k * alpha / kPi));
+  return color;
+}
+
+// One texel: gradient of sum_k,c dsh[k,c] SH[k,c] (baker.cpp:244-295).
+void texel_grad(GradCtx& c, const shb_surface_point& sp, int samples, int sample_offset, uint32_t seed,
+                uint32_t texel, const float* g, std::vector<double>& grad) {
+  V3d P = pt_pos<double>(sp), N = pt_nrm<double>(sp);
+  V3d T{(double)sp.tangent[0], (double)sp.tangent[1], (double)sp.tangent[2]};
+  double Tw = sp.tangent[3];
+  V3d origin = P + N * 0.001;
+  const double inv = 1.0 / (double)samples;
+  for (int s = 0; s < samples; ++s) {
+    PhiloxRng rng{seed, texel, (uint32_t)(s + sample_offset)};
+    auto hev = rng.event(0, EV_HEMI);
+    float u1 = hev.u(0);
+    float u2 = hev.u(1);
+    double r = std::sqrt(1.0 - (double)u1 * (double)u1);
+    double phi = 2.0 * kPi * (double)u2;
+    V3d dl{r * std::cos(phi), r * std::sin(phi), (double)u1};
+    V3d bitangent = cross(N, T) * Tw;
+    V3d dw = T * dl.x + bitangent * dl.y + N * dl.z;
+    // texel-level NEE (light.cpp:191-293): no BRDF, unnormalised direction
+    {
+      PhiloxEvent ev = rng.event(0, EV_NEE);
+      size_t nl = c.s->lights.size();
+      std::vector<LightEval<double>> evs(nl);
+      std::vector<AreaSample<double>> ass(nl);
+      std::vector<float> weights(nl);
+      int area_ord = 0;
+      for (size_t i = 0; i < nl; ++i) {
+        const Lgt& L = c.s->lights[i];
+        if (L.type == SHB_LIGHT_AREA) ass[i] = sample_area_light<double>(c.s, L, ev, 3 * area_ord++);
+        evs[i] = incoming<double>(L, P, N, &ass[i]);
+        weights[i] = (float)max_coeff(evs[i].radiance);
+      }
+      float sum = std::accumulate(weights.begin(), weights.end(), 0.0f);
+      if (!(sum < 1e-6f)) {
+        auto picker = ev.picker(weights, sum, 3 * area_ord);
+        for (unsigned j = 0; j < c.nls; ++j) {
+          int idx = picker.pick((int)j);
+          const LightEval<double>& e = evs[idx];
+          if (occluded(*c.bvh, e.ray_o, e.ray_d, e.tnear, e.tfar)) continue;
+          double joint = (double)weights[idx] / (double)sum * e.area_pdf;
+          if (joint < 1e-3) continue;
+          LightDeriv ld = light_deriv(c, idx, P, ass[idx], e);
+          if (ld.param < 0) continue;
+          V3d a = sh_adjoint(g, e.ray_d, inv);
+          V3d dLi = ld.dv / (joint * (double)c.nls);
+          if (ld.light) grad[ld.param] += a.x * dLi.x + a.y * dLi.y + a.z * dLi.z;
+          else {
+            grad[ld.param] += a.x * dLi.x;
+            grad[ld.param + 1] += a.y * dLi.y;
+            grad[ld.param + 2] += a.z * dLi.z;
+          }
+        }
+      }
+    }
+    Dual Li = trace_grad(c, rng, origin, dw, 0, 1);
+    V3d a = sh_adjoint(g, dw, 2.0 * kPi * inv);
+    for (int p = 0; p < c.P; ++p) grad[p] += a.x * Li.d[p].x + a.y * Li.d[p].y + a.z * Li.d[p].z;
+  }
+}
+
+}  // namespace
+
 // ================================================================ C API ===
 
 extern "C" {
@@ -1426,6 +1690,58 @@ void oracle_dilate(int kind, int w, int h, void* pixels, uint8_t* mask, int pass
   if (kind == SHB_DILATE_SH9) dilate_t<float, 27>(w, h, (float*)pixels, mask, passes);
   else if (kind == SHB_DILATE_F32) dilate_t<float, 1>(w, h, (float*)pixels, mask, passes);
   else dilate_t<uint8_t, 1>(w, h, (uint8_t*)pixels, mask, passes);
+}
+
+void oracle_scene_set_params(oracle_scene* s, const float* albedo_rgb, const uint8_t* use_override,
+                             const float* light_intensity) {
+  if (albedo_rgb)
+    for (size_t m = 0; m < s->mats.size(); ++m) {
+      s->mats[m].use_override = (!use_override || use_override[m]) ? 1 : 0;
+      for (int c = 0; c < 3; ++c) s->mats[m].ovr[c] = albedo_rgb[3 * m + c];
+    }
+  if (light_intensity)
+    for (size_t l = 0; l < s->lights.size(); ++l) s->lights[l].intensity = light_intensity[l];
+}
+
+int oracle_bake_grad(const oracle_scene* s, const shb_surface_point* pts, const shb_raster_config* rc,
+                     oracle_bake_args* a, const float* dsh, double* d_albedo, double* d_light) {
+  if (a->samples <= 0 || !dsh) return 1;
+  auto bvh = get_bvh<double>(s);
+  const int64_t total = (int64_t)rc->width * rc->supersample_scale * rc->height * rc->supersample_scale;
+  std::vector<int64_t> work;
+  if (a->texel_subset) work.assign(a->texel_subset, a->texel_subset + a->subset_count);
+  else {
+    work.resize(total);
+    std::iota(work.begin(), work.end(), 0);
+  }
+  const int n_mat3 = 3 * (int)s->mats.size();
+  const int P = n_mat3 + (int)s->lights.size();
+  int nthreads = a->threads > 0 ? a->threads : (int)std::max(1u, std::thread::hardware_concurrency());
+  std::atomic<int64_t> next{0};
+  std::vector<std::vector<double>> part((size_t)nthreads, std::vector<double>((size_t)P, 0.0));
+  auto worker = [&](int t) {
+    GradCtx c{s, bvh.get(), a->bounces, (unsigned)a->num_light_samples, n_mat3, P};
+    while (true) {
+      int64_t begin = next.fetch_add(8);
+      if (begin >= (int64_t)work.size()) break;
+      int64_t end = std::min<int64_t>(begin + 8, work.size());
+      for (int64_t k = begin; k < end; ++k) {
+        int64_t idx = work[k];
+        if (idx < 0 || idx >= total || pts[idx].material_id < 0) continue;
+        texel_grad(c, pts[idx], a->samples, a->sample_offset, a->seed, (uint32_t)idx, dsh + idx * 27, part[t]);
+      }
+    }
+  };
+  std::vector<std::thread> th;
+  for (int i = 0; i < nthreads; ++i) th.emplace_back(worker, i);
+  for (auto& t : th) t.join();
+  for (int p = 0; p < P; ++p) {
+    double v = 0.0;
+    for (int t = 0; t < nthreads; ++t) v += part[t][p];
+    if (p < n_mat3) d_albedo[p] = v;
+    else d_light[p - n_mat3] = v;
+  }
+  return 0;
 }
 
 int oracle_bake(const oracle_scene* s, const shb_surface_point* pts, const shb_raster_config* raster,

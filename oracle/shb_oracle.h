@@ -64,6 +64,21 @@ void oracle_dilate(int kind, int w, int h, void* pixels, uint8_t* mask, int pass
 int oracle_bake(const oracle_scene* s, const shb_surface_point* pts,
                 const shb_raster_config* raster, oracle_bake_args* args);
 
+/* Adjoint parameters, as shb_scene_set_params: per material a linear base
+ * colour replacing the albedo texture (use_override NULL: all), per light
+ * an intensity.  NULL arrays leave the values unchanged. */
+void oracle_scene_set_params(oracle_scene* s, const float* albedo_rgb, const uint8_t* use_override,
+                             const float* light_intensity);
+
+/* FP64 forward-mode gradient of Loss = sum(dsh * SH) over the texels of
+ * args (Philox stream, fp64 regardless of args->fp64; sh/env outputs
+ * unused): d_albedo[3m + c] (override materials), d_light[l] (intensity of
+ * point/spot/directional lights).  Light-selection weights are held
+ * constant, as in the GPU adjoint. */
+int oracle_bake_grad(const oracle_scene* s, const shb_surface_point* pts,
+                     const shb_raster_config* raster, oracle_bake_args* args,
+                     const float* dsh, double* d_albedo, double* d_light);
+
 /* src/occlusion.cpp:9-107 for a batch of rays. */
 void oracle_find_occlusion(const oracle_scene* s, const shb_ray* rays, int64_t n,
                            shb_hit* hits);

@@ -152,6 +152,9 @@ SIGNATURES = {
     "shb_bake_pipeline": (C.c_int, [vp, C.POINTER(PipelineConfig), vp, vp, vp, C.POINTER(BakeStats)]),
     "shb_dilate_noalloc": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_int32]),
     "shb_bake_batch": (C.c_int, [vp, vp, C.c_int32, C.POINTER(BatchOptions), C.POINTER(BakeStats)]),
+    "shb_scene_set_params": (C.c_int, [vp, vp, vp, vp]),
+    "shb_backward": (C.c_int, [vp, vp, C.POINTER(RasterConfig), C.POINTER(BakeConfig), vp, C.c_int32, vp, vp,
+                               C.POINTER(BakeStats)]),
 }
 
 _lib = None

@@ -102,6 +102,20 @@ class DeviceScene:
         h = C.c_void_p()
         A.check(self.lib.shb_scene_upload(ctx.h, C.byref(desc), C.byref(h)))
         self.h = h
+        self.n_materials = len(scene.materials)
+        self.n_lights = len(scene.lights)
+
+    def set_params(self, albedo=None, light_intensity=None, use_override=None) -> None:
+        """Adjoint parameters (shb_scene_set_params): albedo (materials, 3)
+        linear base colours replacing the albedo textures (of the materials
+        where use_override is true; None: all), light_intensity (lights,)."""
+        alb = None if albedo is None else np.ascontiguousarray(albedo, np.float32).reshape(self.n_materials, 3)
+        use = None if use_override is None else np.ascontiguousarray(use_override, np.uint8).reshape(self.n_materials)
+        li = None if light_intensity is None else np.ascontiguousarray(light_intensity, np.float32).reshape(
+            self.n_lights)
+        A.check(self.lib.shb_scene_set_params(self.h, None if alb is None else alb.ctypes.data,
+                                              None if use is None else use.ctypes.data,
+                                              None if li is None else li.ctypes.data))
 
     def bvh_info(self):
         n, t, d = C.c_uint32(), C.c_uint32(), C.c_uint32()
@@ -325,6 +339,34 @@ def bake_plain_device(b: BatchBake, sh, env) -> A.BakeStats:
     A.check(b.scene.lib.shb_bake(b.scene.h, b.gbuffer.h, C.byref(b.raster.c()), C.byref(b.config.c()), C.byref(out),
                                  C.byref(st)))
     return st
+
+
+def Backward(b: BatchBake, d_sh, stats: bool = False):
+    """Path-replay adjoint of BakeSHLightMap (shb_backward) for the bake
+    `b` (same scene parameters, G-buffer and config as its forward bake).
+    d_sh: dLoss/dSH, W*s*H*s*27 floats, a CUDA tensor or a host array.
+    Returns (d_albedo (materials, 3), d_light_intensity (lights,)) as
+    float64 arrays, and the stats when asked."""
+    ds = b.scene
+    n = b.gbuffer.width * b.gbuffer.height * 27
+    on_device = hasattr(d_sh, "is_cuda") and d_sh.is_cuda
+    if on_device:
+        import torch
+        if d_sh.numel() != n or not d_sh.is_contiguous() or d_sh.dtype != torch.float32:
+            raise ValueError("d_sh must be a contiguous float32 tensor of W*s*H*s*27 values")
+        torch.cuda.current_stream(d_sh.device).synchronize()  # d_sh may come from torch's stream
+        ptr = d_sh.data_ptr()
+    else:
+        host = np.ascontiguousarray(d_sh, np.float32).reshape(-1)
+        if host.size != n:
+            raise ValueError("d_sh must hold W*s*H*s*27 floats")
+        ptr = host.ctypes.data
+    d_alb = np.zeros((ds.n_materials, 3), np.float64)
+    d_li = np.zeros(ds.n_lights, np.float64)
+    st = A.BakeStats()
+    A.check(ds.lib.shb_backward(ds.h, b.gbuffer.h, C.byref(b.raster.c()), C.byref(b.config.c()), ptr,
+                                int(on_device), d_alb.ctypes.data, d_li.ctypes.data, C.byref(st)))
+    return (d_alb, d_li, st) if stats else (d_alb, d_li)
 
 
 @dataclass

@@ -29,6 +29,11 @@ constexpr int kThreads = 256;
 // wave is shrunk by 2^min(bounces, kMaxBranchLog).  Branch slots beyond that
 // (more than six transmissive bounces) fall back to atomic accumulation.
 constexpr int kMaxBranchLog = 6;
+// Adjoint limits: the per-block gradient accumulator lives in shared memory
+// (3 x materials + lights floats) and a throughput tangent list holds at
+// most one entry per bounce.
+constexpr size_t kMaxGradSmem = 48 * 1024;
+constexpr int kMaxTangents = 16;
 constexpr double kTwoPiD = 6.283185307179586;
 
 struct MatInfo {
@@ -118,15 +123,29 @@ struct LightEval {
   float tfar;
   float apdf;
   float w;
+  // Adjoint only (BWD): light index; d rad / d(light parameter) per channel
+  // (point/spot/directional: intensity, lpar = 1; area: the emissive
+  // material's linear albedo, pmat >= 0 when that material is a parameter);
+  // d rad_c / d albedo_c of the receiving material (HIT).
+  uint32_t idx;
+  int lpar, pmat;
+  f3 dpar, dalb;
 };
 
 // Incoming radiance without visibility (src/light.h:34-49,72-95,117-144,
 // 166-188); with HIT, times cos x BRDF (src/light.h:51-203).
-template <bool HIT>
+template <bool HIT, bool BWD = false>
 __device__ LightEval eval_light(const SceneView& sc, uint32_t li, f3 P, f3 N, Event& ev, f3 wo, f3 aop) {
   DLight L = sc.lights[li];
   LightEval e;
   e.apdf = 1.0f;
+  if (BWD) {
+    e.idx = li;
+    e.lpar = 0;
+    e.pmat = -1;
+    e.dpar = {0.f, 0.f, 0.f};
+    e.dalb = {0.f, 0.f, 0.f};
+  }
   f3 color = {L.cr, L.cg, L.cb};
   float cos_n;
   f3 incident;
@@ -137,6 +156,10 @@ __device__ LightEval eval_light(const SceneView& sc, uint32_t li, f3 P, f3 N, Ev
     cos_n = dot(N, -dir);
     incident = -dir;
     e.rad = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : L.intensity * color;
+    if (BWD) {
+      e.lpar = 1;
+      e.dpar = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : color;
+    }
   } else if (L.type == SHB_LIGHT_POINT || L.type == SHB_LIGHT_SPOT || L.type == SHB_LIGHT_AREA) {
     f3 target, arad = {0.f, 0.f, 0.f};
     if (L.type == SHB_LIGHT_AREA) sample_area(sc, L, ev, 3 * L.area_ord, target, arad, e.apdf);
@@ -151,13 +174,28 @@ __device__ LightEval eval_light(const SceneView& sc, uint32_t li, f3 P, f3 N, Ev
     cos_n = dot(N, Lv);
     if (L.type == SHB_LIGHT_POINT) {
       e.rad = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : L.intensity * color / (dist * dist);
+      if (BWD) {
+        e.lpar = 1;
+        e.dpar = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : color / (dist * dist);
+      }
     } else if (L.type == SHB_LIGHT_SPOT) {
       float cos_l = dot(f3{L.dx, L.dy, L.dz}, -Lv);
       float falloff = (cos_l - L.cos_outer) / (L.cos_inner - L.cos_outer);
       falloff = fminf(fmaxf(falloff, 0.0f), 1.0f);
       e.rad = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : L.intensity * color / (dist * dist) * falloff;
+      if (BWD) {
+        e.lpar = 1;
+        e.dpar = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : color / (dist * dist) * falloff;
+      }
     } else {
       e.rad = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : arad / (dist * dist);
+      if (BWD && L.mat >= 0 && (uint32_t)L.mat < sc.mat_count) {
+        const DMat& em = sc.mats[L.mat];
+        if (em.use_override && em.emission > 0.0f && cos_n >= 0.f) {
+          e.pmat = L.mat;
+          e.dpar = f3{em.emission, em.emission, em.emission} / (dist * dist);
+        }
+      }
     }
   } else {
     e.rad = {0.f, 0.f, 0.f};
@@ -169,9 +207,14 @@ __device__ LightEval eval_light(const SceneView& sc, uint32_t li, f3 P, f3 N, Ev
   if (HIT) {
     if (cos_n < 0.f) {
       e.rad = {0.f, 0.f, 0.f};
+      if (BWD) e.dpar = {0.f, 0.f, 0.f};
     } else {
       bool zero = dot(N, wo) <= 0.0f || dot(N, incident) <= 0.0f;
       f3 brdf = zero ? f3{0.f, 0.f, 0.f} : aop;
+      if (BWD) {
+        e.dpar = cmul(e.dpar, cos_n * brdf);
+        e.dalb = zero ? f3{0.f, 0.f, 0.f} : e.rad * (cos_n / 3.14159265358979323846f);
+      }
       e.rad = cmul(e.rad, cos_n * brdf);
     }
   }
@@ -187,7 +230,7 @@ __device__ LightEval eval_light(const SceneView& sc, uint32_t li, f3 P, f3 N, Ev
 // re-evaluated (same values either way: evaluation is deterministic).
 constexpr uint32_t kWeightCache = 32;
 
-template <bool HIT>
+template <bool HIT, bool BWD = false>
 __device__ bool pick_light(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3 aop, float sum, float u,
                            const float* wcache, LightEval& out) {
   float target = u * sum;
@@ -200,18 +243,18 @@ __device__ bool pick_light(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3
     if (cached) {
       w = wcache[i];
     } else {
-      e = eval_light<HIT>(sc, i, P, N, ev, wo, aop);
+      e = eval_light<HIT, BWD>(sc, i, P, N, ev, wo, aop);
       w = e.w;
     }
     cum += w;
     if (w > 0.f) last = (int)i;
     if (target < cum) {
-      out = cached ? eval_light<HIT>(sc, i, P, N, ev, wo, aop) : e;
+      out = cached ? eval_light<HIT, BWD>(sc, i, P, N, ev, wo, aop) : e;
       return true;
     }
   }
   if (last < 0) return false;
-  out = eval_light<HIT>(sc, (uint32_t)last, P, N, ev, wo, aop);
+  out = eval_light<HIT, BWD>(sc, (uint32_t)last, P, N, ev, wo, aop);
   return true;
 }
 
@@ -293,7 +336,87 @@ struct WaveArgs {
   int det;
   int slots;    // branch slots per path (1 without alpha)
   float4* pend;
+  // Adjoint (path replay).  path_L holds each path's adjoint weight
+  // dLoss/dL (RGB).  Every extend-queue entry carries the forward-mode
+  // tangent of its throughput, d beta_c / d albedo_{m,c}, as a list of
+  // (rgb, material) float4 in tan[queue][k * ext_cap + i], k < beta.w bits.
+  // Every shadow ray carries a gradient packet pk[k * sh_cap + slot],
+  // k < count in pend[slot].x bits: (value rgb, parameter) per material or
+  // (value, 0, 0, light | kLightFlag); k_shadow clears the count when the
+  // ray is occluded and k_apply adds the visible packets.
+  const float* dsh;   // dLoss/dSH of the bake, 27 per texel
+  float4* tan[2];
+  float4* pk;
+  int ntan, npk;
+  int n_mat3;         // 3 * mat_count: first light parameter
+  int n_params;       // 3 * mat_count + light_count
+  double* grad;
 };
+
+constexpr uint32_t kLightFlag = 0x80000000u;
+
+// sum_k g[3k + c] Y_k(d): the adjoint of sh_accumulate for one direction.
+__device__ __forceinline__ f3 sh_adjoint(const float* __restrict__ g, f3 d) {
+  const float x = d.x, y = d.y, z = d.z;
+  float sh[9];
+  sh[0] = 0.282095f;
+  sh[1] = 0.488603f * y;
+  sh[2] = 0.488603f * z;
+  sh[3] = 0.488603f * x;
+  sh[4] = 1.092548f * x * y;
+  sh[5] = 1.092548f * y * z;
+  sh[6] = 0.315392f * (3.0f * z * z - 1.0f);
+  sh[7] = 1.092548f * x * z;
+  sh[8] = 0.546274f * (x * x - y * y);
+  f3 a = {0.f, 0.f, 0.f};
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    a.x += __ldg(g + 3 * i) * sh[i];
+    a.y += __ldg(g + 3 * i + 1) * sh[i];
+    a.z += __ldg(g + 3 * i + 2) * sh[i];
+  }
+  return a;
+}
+
+// Warp-aggregated gradient add into the block's shared accumulator: lanes
+// holding the same parameter are summed with shuffles and one lane adds the
+// sum.  Every lane of the warp must call this.
+__device__ __forceinline__ void warp_grad_add(float* sg, int pid, float v, bool act) {
+  const int lane = threadIdx.x & 31;
+  unsigned pending = __ballot_sync(0xFFFFFFFFu, act && v != 0.f);
+  while (pending) {
+    const int leader = __ffs(pending) - 1;
+    const int key = __shfl_sync(0xFFFFFFFFu, pid, leader);
+    const bool mine = ((pending >> lane) & 1u) && pid == key;
+    float sum = mine ? v : 0.f;
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) sum += __shfl_xor_sync(0xFFFFFFFFu, sum, off);
+    if (lane == leader) atomicAdd(sg + key, sum);
+    pending &= ~__ballot_sync(0xFFFFFFFFu, mine);
+  }
+}
+
+// One packet entry: material m adds rgb to parameters 3m..3m+2, light l
+// adds x to parameter n_mat3 + l.  Every lane of the warp must call this.
+__device__ __forceinline__ void warp_grad_entry(float* sg, const WaveArgs& a, float4 e, bool act) {
+  const uint32_t id = __float_as_uint(e.w);
+  const bool light = (id & kLightFlag) != 0u;
+  const int p0 = light ? a.n_mat3 + (int)(id & ~kLightFlag) : 3 * (int)id;
+  act = act && p0 >= 0 && p0 + (light ? 0 : 2) < a.n_params;
+  warp_grad_add(sg, p0, e.x, act);
+  warp_grad_add(sg, p0 + 1, e.y, act && !light);
+  warp_grad_add(sg, p0 + 2, e.z, act && !light);
+}
+
+__device__ __forceinline__ void grad_zero(float* sg, int n) {
+  for (int i = threadIdx.x; i < n; i += blockDim.x) sg[i] = 0.f;
+  __syncthreads();
+}
+__device__ __forceinline__ void grad_flush(const float* sg, int n, double* g) {
+  __syncthreads();
+  for (int i = threadIdx.x; i < n; i += blockDim.x)
+    if (sg[i] != 0.f) atomicAdd(g + i, (double)sg[i]);
+}
 
 // Queue slot within capacity, else the error flag is raised and the ray dropped.
 __device__ __forceinline__ bool slot_ok(const WaveArgs& a, int slot, int cap) {
@@ -316,6 +439,7 @@ __device__ __forceinline__ int find_tile(const WaveArgs& a, int64_t x) {
 }
 
 // ------------------------------------------------------------- generate --
+template <bool BWD>
 __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const int64_t warp_id = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -326,6 +450,8 @@ __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
     f3 o = {0.f, 0.f, 0.f}, dw = {0.f, 0.f, 1.f}, P0 = o, N = o;
     uint32_t texel = 0, sample = 0, b = 0;
     const BakeItem* B = a.bakes;
+    const float* g = nullptr;
+    float inv = 0.f;
     if (active) {
       const Tile t = a.tiles[find_tile<true>(a, p)];
       b = t.bake;
@@ -339,10 +465,18 @@ __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
       N = sp.nrm;
       dw = primary_dir(sp, B->seed, texel, sample);
       o = sp.pos + sp.nrm * 0.001f;
-      a.path_L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
       a.info[p] = make_uint4(b, texel, sample, 0u);
-      if (a.det)
-        for (int k = 0; k < a.slots * a.NLS; ++k) a.pend[p * a.slots * a.NLS + k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (BWD) {
+        // dLoss/dL of this path: sh_out = (1/spp) sum 2pi L Y(dw) (k_resolve)
+        g = a.dsh + (int64_t)texel * 27;
+        inv = 1.0f / (float)t.spp;
+        f3 adj = sh_adjoint(g, dw) * ((float)kTwoPiD * inv);
+        a.path_L[p] = make_float4(adj.x, adj.y, adj.z, 0.f);
+      } else {
+        a.path_L[p] = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (a.det)
+          for (int k = 0; k < a.slots * a.NLS; ++k) a.pend[p * a.slots * a.NLS + k] = make_float4(0.f, 0.f, 0.f, 0.f);
+      }
     }
     // texel-level NEE (src/light.cpp:191-293), origin without offset
     Event ev;
@@ -355,40 +489,67 @@ __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
     for (int j = 0; j < a.NLS; ++j) {
       LightEval e;
       bool ok = false;
+      float joint = 1.f;
       if (any_light && j < nls) {
-        ok = pick_light<false>(B->sc, P0, N, ev, zero3, zero3, sum, ev.u(3 * (int)B->sc.area_light_count + j),
-                               wcache, e);
+        ok = pick_light<false, BWD>(B->sc, P0, N, ev, zero3, zero3, sum,
+                                    ev.u(3 * (int)B->sc.area_light_count + j), wcache, e);
         if (ok) {
           float pdf = e.w / sum;
-          float joint = pdf * e.apdf;
+          joint = pdf * e.apdf;
           ok = !(joint < 1e-3f);
-          if (ok) {
+          if (ok && !BWD) {
             f3 Li = e.rad / (joint * (float)nls);
             a.nee_li[p * a.NLS + j] = make_float4(Li.x, Li.y, Li.z, 0.f);
             a.nee_dir[p * a.NLS + j] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, 0.f);
           }
         }
       }
-      if (active && !ok) a.nee_li[p * a.NLS + j] = make_float4(0.f, 0.f, 0.f, 0.f);
+      if (!BWD && active && !ok) a.nee_li[p * a.NLS + j] = make_float4(0.f, 0.f, 0.f, 0.f);
       int slot = warp_push(a.cnt + CNT_SHADOW, ok);
       if (ok && slot_ok(a, slot, a.sh_cap)) {
         a.sh.o[slot] = make_float4(P0.x, P0.y, P0.z, e.tfar);
-        a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float((uint32_t)(p * a.NLS + j)));
-        a.sh.c[slot] = make_float4(0.f, 0.f, 0.f, __uint_as_float(1u | (b << 2)));
+        if (BWD) {
+          // Li = rad / (joint nls) projected along the unnormalised ray
+          // direction (k_resolve); the selection pdf is held constant.
+          f3 adj = sh_adjoint(g, e.ray_d) * inv;
+          const float k = 1.0f / (joint * (float)nls);
+          uint32_t n = 0;
+          if (e.lpar) {
+            a.pk[(int64_t)n++ * a.sh_cap + slot] =
+                make_float4(dot(adj, e.dpar) * k, 0.f, 0.f, __uint_as_float(e.idx | kLightFlag));
+          } else if (e.pmat >= 0) {
+            f3 v = cmul(adj, e.dpar) * k;
+            a.pk[(int64_t)n++ * a.sh_cap + slot] = make_float4(v.x, v.y, v.z, __uint_as_float((uint32_t)e.pmat));
+          }
+          a.pend[slot] = make_float4(__uint_as_float(n), 0.f, 0.f, 0.f);
+          a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float((uint32_t)slot));
+          a.sh.c[slot] = make_float4(0.f, 0.f, 0.f, __uint_as_float(2u | (b << 2)));
+        } else {
+          a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float((uint32_t)(p * a.NLS + j)));
+          a.sh.c[slot] = make_float4(0.f, 0.f, 0.f, __uint_as_float(1u | (b << 2)));
+        }
       }
     }
     int slot = warp_push(a.cnt + CNT_EXT0, active);
     if (active && slot_ok(a, slot, a.ext_cap)) {
       a.ext[0].o[slot] = make_float4(o.x, o.y, o.z, __uint_as_float((uint32_t)p));
       a.ext[0].d[slot] = make_float4(dw.x, dw.y, dw.z, __uint_as_float(1u));
-      a.ext[0].beta[slot] = make_float4(1.f, 1.f, 1.f, 0.f);
+      a.ext[0].beta[slot] = make_float4(1.f, 1.f, 1.f, 0.f);  // w: tangent count 0
     }
   }
 }
 
 // --------------------------------------------------------------- shade ---
 // One path vertex of Trace (src/baker.cpp:70-149) in throughput form.
+// BWD: the same vertex replayed for the adjoint.  The contributions are
+// multilinear in the parameters once the light-selection pdfs are held
+// constant, so the gradient follows from the throughput tangents: d(beta X)
+// = D X + beta dX for a collected term X, and the child tangent of a bounce
+// with factor f = alpha rho h is D f + [m] beta alpha h.
+template <bool BWD>
 __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int depth) {
+  extern __shared__ float sgrad[];
+  if (BWD) grad_zero(sgrad, a.n_params);
   const int n = min(a.cnt[cur], a.ext_cap);
   const int nxt = cur ^ 1;
   const int warps = gridDim.x * (blockDim.x >> 5);
@@ -400,22 +561,29 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
     int i = base + lane;
     bool active = i < n;
     bool hit = false;
-    uint32_t path = 0, vertex = 0, texel = 0, sample = 0, b = 0;
+    uint32_t path = 0, vertex = 0, texel = 0, sample = 0, b = 0, ntan = 0;
     const BakeItem* B = a.bakes;
     f3 d = {0.f, 0.f, 1.f}, beta = {0.f, 0.f, 0.f}, pos = {0.f, 0.f, 0.f}, N = {0.f, 0.f, 1.f};
+    f3 adj = {0.f, 0.f, 0.f};
     f2 uv = {0.f, 0.f};
     float alpha = 1.f;
     bool can_extend = false;
-    DMat mat;
+    int mat_id = -1;
+    DMat mat{};
     if (active) {
       float4 qo = q.o[i], qd = q.d[i], qb = q.beta[i], h = a.hits[i];
       path = __float_as_uint(qo.w);
       vertex = __float_as_uint(qd.w);
       d = {qd.x, qd.y, qd.z};
       beta = {qb.x, qb.y, qb.z};
+      if (BWD) {
+        ntan = __float_as_uint(qb.w);
+        float4 ad = a.path_L[path];
+        adj = {ad.x, ad.y, ad.z};
+      }
       uint32_t prim = __float_as_uint(h.w);
       if (prim == kMissPrim) {
-        if (depth == 0) a.path_L[path].w += 1.0f;
+        if (!BWD && depth == 0) a.path_L[path].w += 1.0f;
       } else {
         hit = true;
         PathInfo pi = a.info[path];
@@ -441,9 +609,12 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
         if (G.flags & GEOM_HAS_TEXUV)
           uv = w * ld2(sc.tex_uv, i0) + u * ld2(sc.tex_uv, i1) + v * ld2(sc.tex_uv, i2);
         mat = load_mat(sc, G.material_id);
+        mat_id = G.material_id;
         alpha = get_alpha(sc, mat, uv);
       }
     }
+    // is the hit material an adjoint parameter
+    const bool param = BWD && hit && mat_id >= 0 && (uint32_t)mat_id < B->sc.mat_count && mat.use_override;
     // transmission (src/baker.cpp:99-105)
     if (__any_sync(0xFFFFFFFFu, hit && B->sc.has_alpha)) {
       bool tr = hit && alpha < 1.0f && can_extend;
@@ -453,7 +624,13 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
         f3 bt = beta * (1.0f - alpha);
         qn.o[slot] = make_float4(hp.x, hp.y, hp.z, __uint_as_float(path));
         qn.d[slot] = make_float4(d.x, d.y, d.z, __uint_as_float(2u * vertex + 1u));
-        qn.beta[slot] = make_float4(bt.x, bt.y, bt.z, 0.f);
+        qn.beta[slot] = make_float4(bt.x, bt.y, bt.z, __uint_as_float(BWD ? ntan : 0u));
+        if (BWD)
+          for (uint32_t k = 0; k < ntan; ++k) {
+            float4 t = a.tan[cur][(int64_t)k * a.ext_cap + i];
+            a.tan[nxt][(int64_t)k * a.ext_cap + slot] =
+                make_float4(t.x * (1.0f - alpha), t.y * (1.0f - alpha), t.z * (1.0f - alpha), t.w);
+          }
       }
     }
     bool opaque_hit = hit && alpha != 0.0f;
@@ -463,13 +640,20 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
       aop = alb / 3.14159265358979323846f;
       if (depth == 0) {
         f3 em = mat.emission > 0.0f ? alb * mat.emission : f3{0.f, 0.f, 0.f};
-        if (!is_zero_eigen(em)) {
+        if (!is_zero_eigen(em) && !BWD) {
           f3 c = cmul(beta, alpha * em);
           float4 L = a.path_L[path];
           a.path_L[path] = make_float4(L.x + c.x, L.y + c.y, L.z + c.z, L.w);
         }
       }
       hit_pos = pos + N * 0.001f;
+    }
+    if (BWD) {
+      // emission at depth 0: d(beta alpha rho e)/d rho = beta alpha e (no tangents yet)
+      bool em_on = param && opaque_hit && depth == 0 && mat.emission > 0.0f &&
+                   !is_zero_eigen(get_albedo(B->sc, mat, uv) * mat.emission);
+      f3 v = cmul(adj, beta) * (alpha * mat.emission);
+      warp_grad_entry(sgrad, a, make_float4(v.x, v.y, v.z, __uint_as_float((uint32_t)max(mat_id, 0))), em_on);
     }
     // NEE at the hit (src/light.cpp:82-189)
     f3 wo = -d;
@@ -483,24 +667,51 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
       LightEval e;
       bool ok = false;
       f3 c = {0.f, 0.f, 0.f};
+      float scale = 0.f;
       if (any_light && j < nls) {
-        ok = pick_light<true>(B->sc, hit_pos, N, ev, wo, aop, sum, ev.u(3 * (int)B->sc.area_light_count + j), wcache,
-                              e);
+        ok = pick_light<true, BWD>(B->sc, hit_pos, N, ev, wo, aop, sum,
+                                   ev.u(3 * (int)B->sc.area_light_count + j), wcache, e);
         if (ok) {
           float pdf = e.w / sum;
           float joint = pdf * e.apdf;
           ok = !(joint < 1e-3f);
           if (ok) c = cmul(beta, alpha * ((e.rad / joint) / (float)nls));
+          scale = alpha / (joint * (float)nls);
         }
       }
       int slot = warp_push(a.cnt + CNT_SHADOW, ok);
       if (ok && slot_ok(a, slot, a.sh_cap)) {
         uint32_t target = path, kind = 0u;
-        const uint32_t vslot = vertex - (1u << depth);
-        if (a.det && vslot < (uint32_t)a.slots) {
-          target = ((path * (uint32_t)a.slots + vslot) * (uint32_t)a.NLS + (uint32_t)j);
-          a.pend[target] = make_float4(c.x, c.y, c.z, 0.f);
+        if (BWD) {
+          // packet: tangents x X, own albedo, light parameter
+          const f3 X = e.rad * scale;
+          uint32_t np = 0;
+          for (uint32_t k = 0; k < ntan; ++k) {
+            float4 t = a.tan[cur][(int64_t)k * a.ext_cap + i];
+            f3 v = cmul(adj, cmul(f3{t.x, t.y, t.z}, X));
+            a.pk[(int64_t)np++ * a.sh_cap + slot] = make_float4(v.x, v.y, v.z, t.w);
+          }
+          if (param) {
+            f3 v = cmul(adj, cmul(beta, e.dalb * scale));
+            a.pk[(int64_t)np++ * a.sh_cap + slot] = make_float4(v.x, v.y, v.z, __uint_as_float((uint32_t)mat_id));
+          }
+          if (e.lpar) {
+            a.pk[(int64_t)np++ * a.sh_cap + slot] =
+                make_float4(dot(cmul(adj, beta), e.dpar) * scale, 0.f, 0.f, __uint_as_float(e.idx | kLightFlag));
+          } else if (e.pmat >= 0) {
+            f3 v = cmul(adj, cmul(beta, e.dpar * scale));
+            a.pk[(int64_t)np++ * a.sh_cap + slot] = make_float4(v.x, v.y, v.z, __uint_as_float((uint32_t)e.pmat));
+          }
+          a.pend[slot] = make_float4(__uint_as_float(np), 0.f, 0.f, 0.f);
+          target = (uint32_t)slot;
           kind = 2u;
+        } else {
+          const uint32_t vslot = vertex - (1u << depth);
+          if (a.det && vslot < (uint32_t)a.slots) {
+            target = ((path * (uint32_t)a.slots + vslot) * (uint32_t)a.NLS + (uint32_t)j);
+            a.pend[target] = make_float4(c.x, c.y, c.z, 0.f);
+            kind = 2u;
+          }
         }
         a.sh.o[slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, e.tfar);
         a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float(target));
@@ -509,7 +720,8 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
     }
     // indirect (src/material.cpp:113-162, src/baker.cpp:131-148)
     bool ext = false;
-    f3 nd = {0.f, 0.f, 1.f}, nb = {0.f, 0.f, 0.f};
+    f3 nd = {0.f, 0.f, 1.f}, nb = {0.f, 0.f, 0.f}, fac = {0.f, 0.f, 0.f};
+    float hscale = 0.f;
     if (opaque_hit && can_extend) {
       Event eb;
       eb.init(B->seed, texel, sample, vertex, EV_BSDF);
@@ -527,17 +739,62 @@ __global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int dep
         bool zero = dot(N, nd) <= 0.0f || dot(N, wo) <= 0.0f;
         f3 brdf = zero ? f3{0.f, 0.f, 0.f} : aop;
         float cos_term = dot(N, nd);
-        nb = cmul(beta, alpha * (brdf * (cos_term / pdf)));
+        fac = alpha * (brdf * (cos_term / pdf));
+        nb = cmul(beta, fac);
         ext = !(nb.x == 0.f && nb.y == 0.f && nb.z == 0.f);
+        if (BWD && !zero) hscale = alpha * ((cos_term / pdf) / 3.14159265358979323846f);
       }
     }
     int slot = warp_push(a.cnt + nxt, ext);
     if (ext && slot_ok(a, slot, a.ext_cap)) {
+      uint32_t nt = 0;
+      if (BWD) {
+        // child tangents: D f, plus beta alpha h for the own albedo (merged)
+        bool merged = false;
+        for (uint32_t k = 0; k < ntan; ++k) {
+          float4 t = a.tan[cur][(int64_t)k * a.ext_cap + i];
+          f3 v = cmul(f3{t.x, t.y, t.z}, fac);
+          if (param && __float_as_uint(t.w) == (uint32_t)mat_id) {
+            v = v + beta * hscale;
+            merged = true;
+          }
+          a.tan[nxt][(int64_t)nt++ * a.ext_cap + slot] = make_float4(v.x, v.y, v.z, t.w);
+        }
+        if (param && !merged) {
+          if ((int)nt < a.ntan) {
+            f3 v = beta * hscale;
+            a.tan[nxt][(int64_t)nt++ * a.ext_cap + slot] = make_float4(v.x, v.y, v.z, __uint_as_float((uint32_t)mat_id));
+          } else {
+            atomicOr(a.cnt + CNT_ERROR, ERR_QUEUE);
+          }
+        }
+      }
       qn.o[slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, __uint_as_float(path));
       qn.d[slot] = make_float4(nd.x, nd.y, nd.z, __uint_as_float(2u * vertex));
-      qn.beta[slot] = make_float4(nb.x, nb.y, nb.z, 0.f);
+      qn.beta[slot] = make_float4(nb.x, nb.y, nb.z, __uint_as_float(nt));
     }
   }
+  if (BWD) grad_flush(sgrad, a.n_params, a.grad);
+}
+
+// Adds the gradient packets of the visible shadow rays (BWD): count in
+// pend[slot].x, cleared by k_shadow for occluded rays.
+__global__ void __launch_bounds__(kThreads) k_apply(WaveArgs a) {
+  extern __shared__ float sgrad[];
+  grad_zero(sgrad, a.n_params);
+  const int n = min(a.cnt[CNT_SHADOW], a.sh_cap);
+  const int stride = gridDim.x * blockDim.x;
+  for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+    const int i = base + (threadIdx.x & 31);
+    const bool active = i < n;
+    const uint32_t cnt = active ? min(__float_as_uint(a.pend[i].x), (uint32_t)a.npk) : 0u;
+    for (int k = 0; k < a.npk; ++k) {
+      const bool act = (uint32_t)k < cnt;
+      float4 e = act ? a.pk[(int64_t)k * a.sh_cap + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+      warp_grad_entry(sgrad, a, e, act);
+    }
+  }
+  grad_flush(sgrad, a.n_params, a.grad);
 }
 
 // Adds the pending hit-NEE contributions of one depth to the path radiance
@@ -779,6 +1036,23 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   cudaStream_t st = c->stream;
   const int nb = (int)specs.size();
   if (nb == 0) return SHB_OK;
+  const bool bwd = prm.backward;
+  int n_params = 0;
+  if (bwd) {
+    if (nb != 1 || !specs[0].dsh || !prm.grad) {
+      set_error("backward takes one bake with dLoss/dSH and a gradient buffer");
+      return SHB_ERR_INVALID_ARG;
+    }
+    n_params = 3 * (int)specs[0].scene->mat_count + (int)specs[0].scene->light_count;
+    if ((size_t)n_params * sizeof(float) > kMaxGradSmem) {
+      set_error("backward: more than " + std::to_string(kMaxGradSmem / 4) + " parameters (3 x materials + lights)");
+      return SHB_ERR_INVALID_ARG;
+    }
+    if (specs[0].cfg.bounces > kMaxTangents) {
+      set_error("backward: at most " + std::to_string(kMaxTangents) + " bounces");
+      return SHB_ERR_INVALID_ARG;
+    }
+  }
   int NLS = 1;
   int64_t total_texels = 0;
   bool any_alpha = false;
@@ -803,8 +1077,10 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   for (int b = 0; b < nb; ++b) {
     const BakeSpec& s = specs[b];
     const int64_t n = (int64_t)s.W * s.H;
-    SHB_CUDA(cudaMemsetAsync(s.sh, 0, sizeof(float) * 27 * (size_t)n, st));
-    SHB_CUDA(cudaMemsetAsync(s.env, 0, sizeof(float) * (size_t)n, st));
+    if (!bwd) {
+      SHB_CUDA(cudaMemsetAsync(s.sh, 0, sizeof(float) * 27 * (size_t)n, st));
+      SHB_CUDA(cudaMemsetAsync(s.env, 0, sizeof(float) * (size_t)n, st));
+    }
     size_t tb = 0;
     cub::DeviceSelect::If(nullptr, tb, it, valid_all + voff, nsel + b, (int)n, ValidPred{s.pts}, st);
     SHB_TRY(c->scratch[11].reserve(tb));
@@ -843,7 +1119,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   }
   // Several hit-NEE contributions per path and depth (light samples or
   // alpha branches) are summed in a fixed order by k_commit.
-  const bool det = NLS > 1 || any_alpha;
+  const bool det = !bwd && (NLS > 1 || any_alpha);
   const int slots = (int)mult;
   std::vector<Tile> tiles;
   std::vector<Wave> waves;
@@ -864,6 +1140,12 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   SHB_TRY(c->scratch[17].reserve(sizeof(float4) * 2 * (size_t)std::max<int64_t>(Pmax, 1) * NLS));
   SHB_TRY(c->scratch[18].reserve(sizeof(PathInfo) * (size_t)std::max<int64_t>(Pmax, 1)));
   if (det) SHB_TRY(c->scratch[24].reserve(sizeof(float4) * (size_t)std::max<int64_t>(Pmax, 1) * slots * NLS));
+  const int ntan = bwd ? std::max(max_b, 1) : 0, npk = ntan + 2;
+  if (bwd) {
+    SHB_TRY(c->scratch[24].reserve(sizeof(float4) * (size_t)sh_cap));
+    SHB_TRY(c->scratch[25].reserve(sizeof(float4) * ((size_t)2 * ntan * ext_cap + (size_t)npk * sh_cap)));
+    SHB_CUDA(cudaMemsetAsync(prm.grad, 0, sizeof(double) * (size_t)n_params, st));
+  }
   SHB_TRY(c->scratch[23].reserve(sizeof(Tile) * std::max<size_t>(tiles.size(), 1)));
   Tile* d_tiles = c->scratch[23].as<Tile>();
   if (!tiles.empty())
@@ -890,7 +1172,22 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   a.sh_cap = (int)sh_cap;
   a.det = det ? 1 : 0;
   a.slots = slots;
-  a.pend = det ? c->scratch[24].as<float4>() : nullptr;
+  a.pend = (det || bwd) ? c->scratch[24].as<float4>() : nullptr;
+  a.dsh = bwd ? specs[0].dsh : nullptr;
+  a.ntan = ntan;
+  a.npk = npk;
+  a.tan[0] = a.tan[1] = nullptr;
+  a.pk = nullptr;
+  if (bwd) {
+    float4* base = c->scratch[25].as<float4>();
+    a.tan[0] = base;
+    a.tan[1] = base + (size_t)ntan * ext_cap;
+    a.pk = base + (size_t)2 * ntan * ext_cap;
+  }
+  a.n_mat3 = bwd ? 3 * (int)specs[0].scene->mat_count : 0;
+  a.n_params = n_params;
+  a.grad = prm.grad;
+  const size_t gsmem = bwd ? sizeof(float) * (size_t)n_params : 0;
 
   const int tgrid = traversal_grid(c->device) * std::max(1, prm.grid_scale);
   const int sgrid = 148 * 8;
@@ -932,7 +1229,8 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
     a.P = w.P;
     a.n_tex = w.n_tex;
     cudaMemsetAsync(cnt, 0, sizeof(int) * (CNT_FETCH_SHADOW + 1), st);
-    k_generate<<<grid_for(w.P), kThreads, 0, st>>>(a);
+    if (bwd) k_generate<true><<<grid_for(w.P), kThreads, 0, st>>>(a);
+    else k_generate<false><<<grid_for(w.P), kThreads, 0, st>>>(a);
     launches++;
     for (int k = 0; k <= w.max_bounces; ++k) {
       int cur = k & 1, nxt = cur ^ 1;
@@ -942,11 +1240,16 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       launch_extend(st, tgrid, d_items, nb, a.info, a.ext[cur], cnt + cur, a.ext_cap, a.hits, cnt + CNT_FETCH_EXT,
                     cnt + CNT_ERROR, c64);
       close_stamp(pe);
-      k_shade<<<sgrid, kThreads, 0, st>>>(a, cur, k);
+      if (bwd) k_shade<true><<<sgrid, kThreads, gsmem, st>>>(a, cur, k);
+      else k_shade<false><<<sgrid, kThreads, 0, st>>>(a, cur, k);
       Pair ps = stamp(1);
       launch_shadow(st, tgrid, d_items, nb, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, a.pend,
                     cnt + CNT_FETCH_SHADOW, cnt + CNT_ERROR, c64);
       close_stamp(ps);
+      if (bwd) {
+        k_apply<<<sgrid, kThreads, gsmem, st>>>(a);
+        launches++;
+      }
       cudaMemsetAsync(cnt + CNT_SHADOW, 0, sizeof(int), st);
       launches += 3;
       if (det) {
@@ -956,8 +1259,10 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       ext_launches++;
       sh_launches++;
     }
-    k_resolve<<<grid_for(w.n_tex * 32), kThreads, 0, st>>>(a);
-    launches++;
+    if (!bwd) {
+      k_resolve<<<grid_for(w.n_tex * 32), kThreads, 0, st>>>(a);
+      launches++;
+    }
   }
   if (prm.use_graph) {
     cudaError_t e = cudaStreamEndCapture(st, &graph);
@@ -1026,6 +1331,15 @@ shb_status bake_device(shb_scene* s, const shb_surface_point* d_pts, int W, int 
                        float* d_sh, float* d_env, shb_bake_stats* stats) {
   BakeSpec spec{s, d_pts, W, H, *cfg, d_sh, d_env};
   BatchParams prm;
+  return bake_batch_device(s->ctx, {spec}, prm, stats);
+}
+
+shb_status backward_device(shb_scene* s, const shb_surface_point* d_pts, int W, int H, const shb_bake_config* cfg,
+                           const float* d_dsh, double* d_grad, shb_bake_stats* stats) {
+  BakeSpec spec{s, d_pts, W, H, *cfg, nullptr, nullptr, d_dsh};
+  BatchParams prm;
+  prm.backward = true;
+  prm.grad = d_grad;
   return bake_batch_device(s->ctx, {spec}, prm, stats);
 }
 

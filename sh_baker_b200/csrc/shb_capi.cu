@@ -388,6 +388,8 @@ shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene
   s->raster_ready = raster_ready;
   s->raster_error = raster_error;
   s->h_geoms = geoms;
+  s->h_mats = mats;
+  s->h_lights = lights;
   shb_status rc = SHB_OK;
   auto chk = [&](shb_status x) {
     if (rc == SHB_OK) rc = x;
@@ -592,6 +594,75 @@ shb_status shb_bake(shb_scene* s, const shb_gbuffer* g, const shb_raster_config*
     SHB_CUDA(cudaMemcpyAsync(out->env_visibility, denv, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream));
   }
   SHB_CUDA(cudaStreamSynchronize(c->stream));
+  if (stats) {
+    stats->kernel_launches = c->launches - l0;
+    stats->bvh_build_ms = s->bvh_build_ms;
+  }
+  return SHB_OK;
+}
+
+shb_status shb_scene_set_params(shb_scene* s, const float* albedo_rgb, const uint8_t* use_override,
+                                const float* light_intensity) {
+  if (!s) return bad("NULL scene");
+  SHB_CUDA(cudaSetDevice(s->ctx->device));
+  if (albedo_rgb)
+    for (uint32_t m = 0; m < s->mat_count; ++m)
+      for (int c = 0; c < 3; ++c)
+        if ((!use_override || use_override[m]) && !(std::isfinite(albedo_rgb[3 * m + c]) && albedo_rgb[3 * m + c] >= 0.f))
+          return bad("material " + std::to_string(m) + ": albedo override must be finite and >= 0");
+  if (light_intensity)
+    for (uint32_t l = 0; l < s->light_count; ++l)
+      if (!std::isfinite(light_intensity[l])) return bad("light " + std::to_string(l) + ": intensity not finite");
+  if (albedo_rgb)
+    for (uint32_t m = 0; m < s->mat_count; ++m) {
+      DMat& M = s->h_mats[m];
+      M.use_override = (!use_override || use_override[m]) ? 1 : 0;
+      for (int c = 0; c < 3; ++c) M.override_rgb[c] = albedo_rgb[3 * m + c];
+    }
+  if (light_intensity)
+    for (uint32_t l = 0; l < s->light_count; ++l) s->h_lights[l].intensity = light_intensity[l];
+  cudaStream_t st = s->ctx->stream;
+  if (albedo_rgb && s->mat_count)
+    SHB_CUDA(cudaMemcpyAsync(s->mats.ptr, s->h_mats.data(), sizeof(DMat) * s->mat_count, cudaMemcpyHostToDevice, st));
+  if (light_intensity && s->light_count)
+    SHB_CUDA(cudaMemcpyAsync(s->lights.ptr, s->h_lights.data(), sizeof(DLight) * s->light_count,
+                             cudaMemcpyHostToDevice, st));
+  SHB_CUDA(cudaStreamSynchronize(st));
+  return SHB_OK;
+}
+
+shb_status shb_backward(shb_scene* s, const shb_gbuffer* g, const shb_raster_config* rc, const shb_bake_config* cfg,
+                        const float* d_sh, int32_t device_ptr, double* d_albedo, double* d_light,
+                        shb_bake_stats* stats) {
+  if (!s || !g || !rc || !cfg || !d_sh) return bad("NULL argument");
+  if ((s->mat_count && !d_albedo) || (s->light_count && !d_light)) return bad("NULL gradient output");
+  if (cfg->samples <= 0) return bad("samples must be positive");
+  if (cfg->bounces < 0 || cfg->bounces > 30) return bad("bounces must be in [0, 30]");
+  if (cfg->num_light_samples <= 0) return bad("num_light_samples must be positive");
+  if (cfg->rng_mode != SHB_RNG_PHILOX) return bad("unknown rng_mode");
+  int64_t W = (int64_t)rc->width * rc->supersample_scale, H = (int64_t)rc->height * rc->supersample_scale;
+  if (W != g->width || H != g->height) return bad("G-buffer size does not match raster_config (W*s x H*s)");
+  if (s->bvh_depth > 64) return bad("BVH deeper than the traversal stack");
+  SHB_CUDA(cudaSetDevice(s->ctx->device));
+  shb_context* c = s->ctx;
+  uint64_t l0 = c->launches;
+  const size_t n = (size_t)W * H;
+  const size_t np = 3 * (size_t)s->mat_count + s->light_count;
+  SHB_TRY(c->scratch[21].reserve(sizeof(double) * std::max<size_t>(np, 1) + (device_ptr ? 0 : sizeof(float) * 27 * n)));
+  double* dgrad = c->scratch[21].as<double>();
+  const float* dsh = d_sh;
+  if (!device_ptr) {
+    float* tmp = reinterpret_cast<float*>(dgrad + std::max<size_t>(np, 1));
+    SHB_CUDA(cudaMemcpyAsync(tmp, d_sh, sizeof(float) * 27 * n, cudaMemcpyHostToDevice, c->stream));
+    dsh = tmp;
+  }
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  SHB_TRY(backward_device(s, g->points.as<shb_surface_point>(), (int)W, (int)H, cfg, dsh, dgrad, stats));
+  std::vector<double> h(np);
+  if (np) SHB_CUDA(cudaMemcpyAsync(h.data(), dgrad, sizeof(double) * np, cudaMemcpyDeviceToHost, c->stream));
+  SHB_CUDA(cudaStreamSynchronize(c->stream));
+  for (size_t i = 0; i < 3 * (size_t)s->mat_count; ++i) d_albedo[i] = h[i];
+  for (size_t l = 0; l < s->light_count; ++l) d_light[l] = h[3 * (size_t)s->mat_count + l];
   if (stats) {
     stats->kernel_launches = c->launches - l0;
     stats->bvh_build_ms = s->bvh_build_ms;

@@ -152,6 +152,8 @@ struct shb_scene {
   bool raster_ready = true;  // every geometry has normals, tangents, lightmap uvs
   std::string raster_error;
   std::vector<shb::DGeom> h_geoms;
+  std::vector<shb::DMat> h_mats;      // host copies, edited by shb_scene_set_params
+  std::vector<shb::DLight> h_lights;
   // BVH
   shb::DevBuf bvh_nodes, bvh_tris;
   uint32_t bvh_node_count = 0, bvh_tri_count = 0, bvh_depth = 0;
@@ -190,6 +192,7 @@ struct BakeSpec {
   shb_bake_config cfg;
   float* sh;
   float* env;
+  const float* dsh = nullptr;  // backward: dLoss/dSH, 27 floats per texel (device)
 };
 
 // Launch-structure parameters (chosen by the autotuner for batches).
@@ -198,11 +201,19 @@ struct BatchParams {
   int64_t tile_texels = int64_t(1) << 30; // texels per work tile
   int grid_scale = 1;                     // traversal grid = grid_scale x SMs x occupancy
   bool use_graph = false;                 // capture the waves in one CUDA graph
+  // Path-replay adjoint instead of the forward bake (one bake): gradients of
+  // sum(dsh * SH) accumulate into grad[3 * mat_count + light_count] (device,
+  // zeroed by the call).
+  bool backward = false;
+  double* grad = nullptr;
 };
 
 shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs, const BatchParams& prm,
                              shb_bake_stats* stats);
 shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n, shb_hit* d_hits);
+// Path-replay adjoint of bake_device: grad[3 * mat_count + light_count] (device).
+shb_status backward_device(shb_scene* s, const shb_surface_point* d_pts, int W, int H, const shb_bake_config* cfg,
+                           const float* d_dsh, double* d_grad, shb_bake_stats* stats);
 
 // sRGB -> linear table (computed on the host with powf, colorspace.h:10-14)
 void srgb_table(float out[256]);

@@ -129,12 +129,53 @@ static void BakeSimpleQuad() {
   for (int c = 0; c < 9; ++c) EXPECT(ds.pixels[0].coeffs[c][0] == 1.0f);
 }
 
+// Backward(): a directional light on a quad with an overridden albedo.  The
+// texel-level NEE does not see the albedo, so with bounces = 0 the loss
+// sum(SH) is linear in the light intensity only: dLoss/dI = sum(SH) / I.
+void BackwardLinearInIntensity() {
+  Scene scene;
+  scene.geometries.push_back(Quad());
+  Material mat;
+  mat.albedo.pixel_data = {200, 200, 200};
+  mat.albedo.width = mat.albedo.height = 1;
+  mat.albedo.channels = 3;
+  scene.materials.push_back(mat);
+  Light light;
+  light.type = Light::Type::Directional;
+  light.direction = Vector3f(0, 0, -1);
+  light.intensity = 2.0f;
+  scene.lights.push_back(light);
+  RasterConfig rc;
+  rc.width = rc.height = 8;
+  std::vector<SurfacePoint> pts = RasterizeScene(scene, rc);
+  BakeConfig config;
+  config.samples = 16;
+  config.bounces = 0;
+  BakeParams params;
+  params.albedo = {Vector3f(0.5f, 0.5f, 0.5f)};
+  params.light_intensity = {2.0f};
+  BakeResult r = BakeSHLightMap(scene, pts, rc, config, params);
+  SHTexture ones;
+  ones.width = ones.height = 8;
+  ones.pixels.resize(64);
+  for (auto& p : ones.pixels)
+    for (auto& c : p.coeffs) c = Vector3f(1.0f, 1.0f, 1.0f);
+  BakeGradients g = Backward(scene, pts, rc, config, params, ones);
+  double total = 0.0;
+  for (const auto& p : r.sh_texture.pixels)
+    for (const auto& c : p.coeffs) total += (double)c[0] + c[1] + c[2];
+  EXPECT(total > 1.0);
+  EXPECT(std::fabs(g.d_light_intensity[0] - total / 2.0) <= 1e-4 * std::fabs(total));
+  EXPECT(g.d_albedo.size() == 3);
+}
+
 int main() {
   try {
     RasterizeQuad();
     Masks();
     Dilation();
     BakeSimpleQuad();
+    BackwardLinearInIntensity();
   } catch (const std::exception& e) {
     std::printf("exception: %s\n", e.what());
     return 2;
