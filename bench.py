@@ -434,6 +434,7 @@ def main():
     from sh_baker_b200 import _capi as A
     from sh_baker_b200 import api
     from sh_baker_b200 import build as B
+    from sh_baker_b200.replicas import job_rate
 
     B.build()
     torch.cuda.set_device(local)
@@ -483,14 +484,7 @@ def main():
     launches = ctx.kernel_launches() - launches0
     clk = clocks.stop()
     ts = sum(s.texel_samples for s in stats)
-    if dist:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-        tt = torch.tensor([float(ts)], device="cuda", dtype=torch.float64)
-        dist.all_reduce(tt)
-        ts = int(tt.item())
-    value = ts / (ms / 1e3)
+    ms, ts, value = job_rate(ms, ts, dist)
 
     # roofline of the dominant kernel (closest-hit or any-hit traversal)
     ext_ms = sum(s.extend_kernel_ms for s in stats)
@@ -546,15 +540,8 @@ def main():
             if i >= args.warmup:
                 e_times.append(ea.elapsed_time(eb))
                 e_ts += st.texel_samples
-        e_ms = sum(e_times)
-        if dist:
-            t = torch.tensor([e_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_ms = float(t.item())
-            tt = torch.tensor([float(e_ts)], device="cuda", dtype=torch.float64)
-            dist.all_reduce(tt)
-            e_ts = int(tt.item())
-        e2e = {"value": e_ts / (e_ms / 1e3), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+        e_ms, e_ts, e_val = job_rate(sum(e_times), e_ts, dist)
+        e2e = {"value": e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(o_sh.nbytes + o_env.nbytes + o_mask.nbytes),
                "ms_per_step": e_ms / args.steps}
 
@@ -569,6 +556,11 @@ def main():
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": config_of(w, scene),
                 "roofline": roof, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches), "clocks": clk,
                 "bvh": ds.bvh_info(), "valid_texels": int(stats[0].valid_texels),
+                "traversal_per_step": {
+                    "closest_hit": {"rays": ext_rays // args.steps,
+                                    "launches": sum(s.extend_launches for s in stats) // args.steps},
+                    "any_hit": {"rays": sh_rays // args.steps,
+                                "launches": sum(s.shadow_launches for s in stats) // args.steps}},
                 "rays_per_texel_sample": (ext_rays + sh_rays) / max(ts, 1)}
         print(json.dumps(line), flush=True)
     del sh, env
