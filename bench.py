@@ -61,6 +61,18 @@ def bytes_per_ray(n_tris: int) -> int:
     return L * 80 + 4 * 48
 
 
+def dram_bytes_per_ray(kind: str, kernel: str):
+    """ncu DRAM bytes (read + write) per ray of a traversal kernel, from the
+    committed summary of the small case of the same scene
+    (profiles/traversal_dram_<kind>_small.md); None when absent."""
+    import re
+    p = ROOT / "profiles" / f"traversal_dram_{kind}_small.md"
+    if not p.exists():
+        return None
+    m = re.search(rf"^\| {kernel} \|.*\| ([0-9.]+) \|$", p.read_text(), re.M)
+    return float(m.group(1)) if m else None
+
+
 def measured_peak():
     p = ROOT / "MEASURED_PEAKS.json"
     try:
@@ -497,15 +509,8 @@ def main():
     k_launch = sum((s.extend_launches if dom == "closest_hit" else s.shadow_launches) for s in stats)
     achieved = k_rays * bpr / (k_ms / 1e3) / 1e9 if k_ms > 0 else 0.0
     peak, peak_kind = measured_peak()
-    traffic = None
-    tp = ROOT / "profiles" / "traversal_traffic.json"
-    if tp.exists():
-        try:
-            tj = json.loads(tp.read_text())
-            per_ray = tj[dom]["dram_bytes_per_ray"]
-            traffic = per_ray * (k_rays / max(k_launch, 1))
-        except Exception:
-            traffic = None
+    per_ray = dram_bytes_per_ray(w["kind"], dom)
+    traffic = per_ray * (k_rays / max(k_launch, 1)) if per_ray else None
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": traffic, "kernel": dom, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "bytes_per_ray": bpr, "rays_per_launch": k_rays / max(k_launch, 1),
