@@ -10,12 +10,14 @@
 //   BakeSHLightMap, DownsampleSHTexture,
 //   DownsampleEnvironmentVisibilityTexture                  (src/baker.h:25-36)
 //   Dilate<T> for SHCoeffs, float, uint8_t                  (src/dilation.h:14-16)
+//   SaveMode, SaveSHLightMap                                (src/saver.h:21-48)
 // Where the reference CHECK-fails these throw sh_baker::Error.  With Eigen
 // available the vector types are Eigen's; otherwise small POD stand-ins with
 // the same memory layout and accessors are used.
 #ifndef SH_BAKER_B200_SH_BAKER_H_
 #define SH_BAKER_B200_SH_BAKER_H_
 
+#include <algorithm>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -348,6 +350,24 @@ inline Texture32F DownsampleEnvironmentVisibilityTexture(const Texture32F& input
   check(shb_downsample(detail::context(), input.pixel_data.data(), (int)input.width, (int)input.height, 1, scale,
                        out.pixel_data.data(), 0));
   return out;
+}
+
+// ---- src/saver.h:21-48 -------------------------------------------------------
+
+enum class SaveMode { kCombined, kSplitChannels, kLuminancePacked };
+
+// Writes the SH lightmap as OpenEXR (half, ZIP) in the reference's layouts;
+// false on an empty texture or a write failure (the reference logs those).
+inline bool SaveSHLightMap(const SHTexture& sh_texture, const Texture32F& environment_visibility_texture,
+                           const std::string& path, SaveMode mode = SaveMode::kCombined) {
+  if (sh_texture.pixels.empty() || sh_texture.width <= 0 || sh_texture.height <= 0) return false;
+  const size_t n = (size_t)sh_texture.width * sh_texture.height;
+  std::vector<float> env(n, 0.0f);
+  const auto& e = environment_visibility_texture.pixel_data;
+  std::copy(e.begin(), e.begin() + std::min(e.size(), n), env.begin());
+  return shb_save_sh_lightmap(detail::context(), reinterpret_cast<const float*>(sh_texture.pixels.data()),
+                              env.data(), sh_texture.width, sh_texture.height, 0, path.c_str(),
+                              (int32_t)mode) == SHB_OK;
 }
 
 // ---- differentiable bake (no counterpart in the reference) ------------------

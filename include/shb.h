@@ -12,6 +12,7 @@
  *   DownsampleEnvironmentVisibilityTexture
  *                         (src/baker.h:35-36)        -> shb_downsample (channels = 1)
  *   Dilate<T>             (src/dilation.h:14-16)     -> shb_dilate (kind = SH9 / F32 / U8)
+ *   SaveSHLightMap        (src/saver.h:45-48)        -> shb_save_sh_lightmap
  *
  * Plain C types only: host pointers are owned by the caller, device objects
  * are owned by the opaque handles.  Every entry point returns a shb_status;
@@ -380,6 +381,25 @@ typedef struct shb_pipeline_config {
 SHB_API shb_status shb_bake_pipeline(shb_scene* scene, const shb_pipeline_config* cfg,
                                      float* sh_out, float* env_out, uint8_t* mask_out,
                                      shb_bake_stats* stats);
+
+/* ---- SaveSHLightMap (src/saver.h:45-48, src/saver.cpp:108-401) -------- */
+
+/* SaveMode (src/saver.h:21-25). */
+typedef enum shb_save_mode {
+  SHB_SAVE_COMBINED = 0,          /* one 28-channel file: L0.R .. L22.B, EnvVisibility */
+  SHB_SAVE_SPLIT_CHANNELS = 1,    /* <stem>_L0 (RGB + A = env) .. <stem>_L22 (RGB)     */
+  SHB_SAVE_LUMINANCE_PACKED = 2   /* <stem>_packed_0..2: L0 RGB + env; Rec. 709 luma of
+                                     L1m1..L2m2; luma of L2m1..L22 (RGBA each)           */
+} shb_save_mode;
+
+/* Writes the SH lightmap (width x height texels of 27 floats) and the
+ * environment visibility (nullable: written as 0) as OpenEXR, half storage,
+ * ZIP compression, the files and channel names of the reference.  Device
+ * pointers when device_ptrs, else host.  Empty dimensions are
+ * SHB_ERR_INVALID_ARG (the reference logs and returns false). */
+SHB_API shb_status shb_save_sh_lightmap(shb_context* ctx, const float* sh, const float* env,
+                                        int32_t width, int32_t height, int32_t device_ptrs,
+                                        const char* path, int32_t mode);
 
 /* ---- FindOcclusion (src/occlusion.cpp:9-107), batched ----------------- */
 

@@ -123,6 +123,8 @@ class Options(C.Structure):
 assert C.sizeof(SurfacePoint) == 64
 assert C.sizeof(Hit) == 48
 
+SAVE_COMBINED, SAVE_SPLIT_CHANNELS, SAVE_LUMINANCE_PACKED = 0, 1, 2
+
 vp = C.c_void_p
 # name -> (restype, argtypes); every symbol declared in include/shb.h
 SIGNATURES = {
@@ -153,6 +155,7 @@ SIGNATURES = {
     "shb_dilate_noalloc": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_int32]),
     "shb_bake_batch": (C.c_int, [vp, vp, C.c_int32, C.POINTER(BatchOptions), C.POINTER(BakeStats)]),
     "shb_scene_set_params": (C.c_int, [vp, vp, vp, vp]),
+    "shb_save_sh_lightmap": (C.c_int, [vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_char_p, C.c_int32]),
     "shb_backward": (C.c_int, [vp, vp, C.POINTER(RasterConfig), C.POINTER(BakeConfig), vp, C.c_int32, vp, vp,
                                C.POINTER(BakeStats)]),
 }

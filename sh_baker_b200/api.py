@@ -398,6 +398,33 @@ def bake_lightmap(scene, width: int, height: int, samples: int = 128, bounces: i
     return LightmapResult(sh, env, mask, st)
 
 
+class SaveMode:
+    """src/saver.h:21-25."""
+    kCombined = A.SAVE_COMBINED
+    kSplitChannels = A.SAVE_SPLIT_CHANNELS
+    kLuminancePacked = A.SAVE_LUMINANCE_PACKED
+
+
+def SaveSHLightMap(sh_texture: np.ndarray, environment_visibility_texture: Optional[np.ndarray], path,
+                   mode: int = SaveMode.kCombined, ctx: Optional[Context] = None) -> bool:
+    """src/saver.h:45-48: sh_texture (H, W, 9, 3) float32, env (H, W) or
+    None.  Returns False where the reference does (empty texture, write
+    failure), with the reason in shb_last_error."""
+    ctx = ctx or default_context()
+    sh = np.ascontiguousarray(sh_texture, np.float32)
+    if sh.ndim != 4 or sh.shape[2:] != (9, 3):
+        raise ValueError("sh_texture must be (H, W, 9, 3)")
+    H, W = sh.shape[:2]
+    env = None
+    if environment_visibility_texture is not None:
+        env = np.zeros((H, W), np.float32)
+        e = np.ascontiguousarray(environment_visibility_texture, np.float32).reshape(-1)[:H * W]
+        env.reshape(-1)[:e.size] = e  # missing texels are 0, as in the reference
+    st = ctx.lib.shb_save_sh_lightmap(ctx.h, sh.ctypes.data, None if env is None else env.ctypes.data, W, H, 0,
+                                      str(path).encode(), int(mode))
+    return st == 0
+
+
 def FindOcclusion(scene, rays: np.ndarray, ctx: Optional[Context] = None):
     """Batched src/occlusion.cpp:9-107.  rays: (N, 8) float32 rows of
     origin(3), direction(3), tnear, tfar.  Returns a structured hit array."""

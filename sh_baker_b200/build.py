@@ -26,6 +26,7 @@ SOURCES = {
     "traverse.cu": ["-fmad=true"],
     "bvh_build.cu": ["-fmad=true"],
     "batch.cu": ["-fmad=false"],
+    "exr.cu": ["-fmad=false"],
 }
 HEADERS = ["shb_internal.h", "shb_math.cuh", "wavefront.h"]
 
@@ -56,7 +57,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
     if force or _newer(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-Xlinker", "--no-undefined"]
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lz", "-Xlinker", "--no-undefined"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

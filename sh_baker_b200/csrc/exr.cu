@@ -1,0 +1,320 @@
+// exr.cu - SaveSHLightMap (src/saver.cpp:108-401): the SH lightmap written
+// as OpenEXR scanline files, half storage, ZIP compression, in the three
+// layouts of the reference (combined 28 channels, 9 split RGB(A) files, 3
+// luminance-packed RGBA files).
+//
+// The device does the per-sample work: channel selection, Rec. 709 luminance
+// of L1/L2 (src/saver.cpp:313,354-360), float -> half, the EXR scanline
+// layout of each 16-line chunk, and ZIP's byte reorder + delta predictor
+// (the OpenEXR ZIP pre-pass).  The host deflates each chunk with zlib on all
+// cores and writes header, offset table and chunks.
+//
+// File layout and choices follow what the reference's writer emits
+// (tinyexr's SaveEXRImageToFile as called in src/saver.cpp): attributes
+// channels, compression, dataWindow, displayWindow, lineOrder,
+// pixelAspectRatio, screenWindowCenter, screenWindowWidth in that order; the
+// channel list in the order the saver names them (not sorted); HALF
+// storage; ZIP_COMPRESSION with 16 lines per chunk; a chunk whose deflate
+// output is not smaller than its raw bytes is stored raw.
+#include <zlib.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "shb_internal.h"
+
+namespace shb {
+namespace {
+
+constexpr int kLinesPerChunk = 16;  // ZIP_COMPRESSION
+
+// Output channel recipes: kind 0 = SH coefficient channel `src` (0..26),
+// kind 1 = Rec. 709 luminance of SH coefficient `src` (0..8), kind 2 = env.
+struct ChanSpec {
+  int kind;
+  int src;
+};
+constexpr int kMaxChannels = 28;
+struct ChanTable {
+  ChanSpec c[kMaxChannels];
+  int n;
+};
+
+// float -> half with the rounding of the reference's writer (tinyexr's
+// float_to_half_full, the public-domain conversion by F. Giesen after the
+// ISPC reference): truncate the mantissa and add one unit when the first
+// dropped bit is set (round half away from zero in magnitude), float
+// denormals flush to zero, overflow gives infinity, NaN gives a quiet NaN.
+__device__ __forceinline__ uint16_t half_bits(float f) {
+  const uint32_t u = __float_as_uint(f);
+  const uint32_t sign = (u >> 16) & 0x8000u;
+  const int exp = (int)((u >> 23) & 0xFFu);
+  const uint32_t man = u & 0x7FFFFFu;
+  uint32_t h = 0;
+  if (exp == 0) {
+    h = 0;
+  } else if (exp == 255) {
+    h = (31u << 10) | (man ? 0x200u : 0u);
+  } else {
+    const int e = exp - 127 + 15;
+    if (e >= 31) {
+      h = 31u << 10;
+    } else if (e <= 0) {
+      if (14 - e <= 24) {
+        const uint32_t m = man | 0x800000u;
+        h = m >> (14 - e);
+        if ((m >> (13 - e)) & 1u) h += 1u;
+      }
+    } else {
+      h = ((uint32_t)e << 10) | (man >> 13);
+      if (man & 0x1000u) h += 1u;
+    }
+  }
+  return (uint16_t)((h & 0x7FFFu) | sign);
+}
+
+// One half sample per thread, written in the raw chunk layout:
+// chunk k holds lines [16k, 16k + lines), each line holds every channel's
+// `width` samples in table order (little-endian).
+__global__ void k_exr_raw(const float* __restrict__ sh, const float* __restrict__ env, int W, int H, ChanTable t,
+                          uint16_t* __restrict__ raw) {
+  const int64_t total = (int64_t)W * H * t.n;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    // i enumerates (y, c, x) in file order: chunks are contiguous lines
+    const int64_t line = i / ((int64_t)W * t.n);
+    const int rem = (int)(i - line * (int64_t)W * t.n);
+    const int c = rem / W;
+    const int x = rem - c * W;
+    const int64_t p = line * W + x;
+    const ChanSpec s = t.c[c];
+    float v;
+    if (s.kind == 0) {
+      v = sh[p * 27 + s.src];
+    } else if (s.kind == 1) {
+      // Eigen dot: x0*y0 + (x1*y1 + x2*y2), Rec. 709 weights
+      const float* q = sh + p * 27 + 3 * s.src;
+      v = __fadd_rn(__fmul_rn(q[0], 0.2126f), __fadd_rn(__fmul_rn(q[1], 0.7152f), __fmul_rn(q[2], 0.0722f)));
+      if (isnan(v)) {
+        // The host (x86 SSE) result: a NaN operand propagates quieted with
+        // its sign, the first in evaluation order (x0, then x1, then x2);
+        // a NaN made from inf - inf is the negative default NaN.  The GPU's
+        // own NaN is the positive canonical one.
+        uint32_t bits = 0xFFC00000u;
+        if (isnan(q[0])) bits = __float_as_uint(q[0]) | 0x400000u;
+        else if (isnan(q[1])) bits = __float_as_uint(q[1]) | 0x400000u;
+        else if (isnan(q[2])) bits = __float_as_uint(q[2]) | 0x400000u;
+        v = __uint_as_float(bits);
+      }
+    } else {
+      v = env ? env[p] : 0.0f;
+    }
+    raw[i] = half_bits(v);
+  }
+}
+
+// ZIP pre-pass per chunk (OpenEXR ZIP compressor): bytes are reordered as
+// [even-indexed bytes, odd-indexed bytes], then each byte after the first
+// becomes (t[i] - t[i-1] + 128) mod 256.  One output byte per thread.
+__global__ void k_exr_predict(const uint8_t* __restrict__ raw, int64_t line_bytes, int H, int64_t total,
+                              uint8_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t chunk_bytes = line_bytes * kLinesPerChunk;
+    const int64_t k = i / chunk_bytes;
+    const int64_t base = k * chunk_bytes;
+    const int lines = min(kLinesPerChunk, H - (int)(k * kLinesPerChunk));
+    const int64_t n = line_bytes * lines;
+    const int64_t j = i - base;
+    const int64_t half = (n + 1) / 2;
+    auto t = [&](int64_t q) -> int { return q < half ? raw[base + 2 * q] : raw[base + 2 * (q - half) + 1]; };
+    out[i] = j == 0 ? (uint8_t)t(0) : (uint8_t)((t(j) - t(j - 1) + 128 + 256) & 0xFF);
+  }
+}
+
+void put_attr(std::vector<uint8_t>& o, const char* name, const char* type, const void* data, int len) {
+  o.insert(o.end(), name, name + std::strlen(name) + 1);
+  o.insert(o.end(), type, type + std::strlen(type) + 1);
+  const uint8_t* l = reinterpret_cast<const uint8_t*>(&len);
+  o.insert(o.end(), l, l + 4);
+  const uint8_t* d = static_cast<const uint8_t*>(data);
+  o.insert(o.end(), d, d + len);
+}
+
+std::vector<uint8_t> exr_header(const std::vector<std::string>& names, int W, int H) {
+  std::vector<uint8_t> o = {0x76, 0x2f, 0x31, 0x01, 2, 0, 0, 0};
+  std::vector<uint8_t> ch;
+  for (const std::string& n : names) {
+    ch.insert(ch.end(), n.begin(), n.end());
+    ch.push_back(0);
+    const int32_t v[4] = {1 /* HALF */, 0 /* pLinear + reserved */, 1, 1};
+    const uint8_t* b = reinterpret_cast<const uint8_t*>(v);
+    ch.insert(ch.end(), b, b + 16);
+  }
+  ch.push_back(0);
+  put_attr(o, "channels", "chlist", ch.data(), (int)ch.size());
+  const uint8_t zip = 3;
+  put_attr(o, "compression", "compression", &zip, 1);
+  const int32_t win[4] = {0, 0, W - 1, H - 1};
+  put_attr(o, "dataWindow", "box2i", win, 16);
+  put_attr(o, "displayWindow", "box2i", win, 16);
+  const uint8_t order = 0;
+  put_attr(o, "lineOrder", "lineOrder", &order, 1);
+  const float one = 1.0f, center[2] = {0.f, 0.f};
+  put_attr(o, "pixelAspectRatio", "float", &one, 4);
+  put_attr(o, "screenWindowCenter", "v2f", center, 8);
+  put_attr(o, "screenWindowWidth", "float", &one, 4);
+  o.push_back(0);
+  return o;
+}
+
+// One file: channels of `t` named `names`.
+shb_status write_exr(shb_context* c, const float* d_sh, const float* d_env, int W, int H, const ChanTable& t,
+                     const std::vector<std::string>& names, const std::string& path) {
+  cudaStream_t st = c->stream;
+  const int64_t line_bytes = (int64_t)W * t.n * 2;
+  const int64_t total = line_bytes * H;
+  SHB_TRY(c->scratch[26].reserve((size_t)total * 2));
+  uint8_t* d_raw = c->scratch[26].as<uint8_t>();
+  uint8_t* d_pred = d_raw + total;
+  const int64_t samples = (int64_t)W * H * t.n;
+  const int grid = (int)std::min<int64_t>((samples + 255) / 256, 148 * 16);
+  k_exr_raw<<<grid, 256, 0, st>>>(d_sh, d_env, W, H, t, reinterpret_cast<uint16_t*>(d_raw));
+  const int grid2 = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  k_exr_predict<<<grid2, 256, 0, st>>>(d_raw, line_bytes, H, total, d_pred);
+  count_launch(c, 2);
+  SHB_CUDA(cudaGetLastError());
+  std::vector<uint8_t> raw((size_t)total), pred((size_t)total);
+  SHB_CUDA(cudaMemcpyAsync(raw.data(), d_raw, (size_t)total, cudaMemcpyDeviceToHost, st));
+  SHB_CUDA(cudaMemcpyAsync(pred.data(), d_pred, (size_t)total, cudaMemcpyDeviceToHost, st));
+  SHB_CUDA(cudaStreamSynchronize(st));
+
+  const int chunks = (H + kLinesPerChunk - 1) / kLinesPerChunk;
+  std::vector<std::vector<uint8_t>> data((size_t)chunks);
+  std::atomic<int> next{0}, failed{0};
+  auto worker = [&]() {
+    for (int k; (k = next.fetch_add(1)) < chunks;) {
+      const int lines = std::min(kLinesPerChunk, H - k * kLinesPerChunk);
+      const size_t n = (size_t)line_bytes * lines, off = (size_t)k * line_bytes * kLinesPerChunk;
+      uLongf cap = compressBound((uLong)n);
+      std::vector<uint8_t> z(cap);
+      if (compress2(z.data(), &cap, pred.data() + off, (uLong)n, Z_DEFAULT_COMPRESSION) != Z_OK) {
+        failed = 1;
+        continue;
+      }
+      if (cap >= n) z.assign(raw.begin() + off, raw.begin() + off + n);  // stored raw
+      else z.resize(cap);
+      data[k] = std::move(z);
+    }
+  };
+  const int nt = std::max(1, std::min<int>(chunks, (int)std::thread::hardware_concurrency()));
+  std::vector<std::thread> th;
+  for (int i = 0; i < nt; ++i) th.emplace_back(worker);
+  for (auto& x : th) x.join();
+  if (failed) {
+    set_error("zlib compression failed");
+    return SHB_ERR_INTERNAL;
+  }
+  std::vector<uint8_t> head = exr_header(names, W, H);
+  std::vector<uint64_t> offsets((size_t)chunks);
+  uint64_t pos = head.size() + 8ull * chunks;
+  for (int k = 0; k < chunks; ++k) {
+    offsets[k] = pos;
+    pos += 8 + data[k].size();
+  }
+  FILE* f = std::fopen(path.c_str(), "wb");
+  if (!f) {
+    set_error("cannot open " + path + " for writing");
+    return SHB_ERR_INVALID_ARG;
+  }
+  bool ok = std::fwrite(head.data(), 1, head.size(), f) == head.size();
+  ok = ok && std::fwrite(offsets.data(), 8, offsets.size(), f) == offsets.size();
+  for (int k = 0; ok && k < chunks; ++k) {
+    const int32_t y = k * kLinesPerChunk, sz = (int32_t)data[k].size();
+    ok = std::fwrite(&y, 4, 1, f) == 1 && std::fwrite(&sz, 4, 1, f) == 1 &&
+         std::fwrite(data[k].data(), 1, data[k].size(), f) == data[k].size();
+  }
+  ok = (std::fclose(f) == 0) && ok;
+  if (!ok) {
+    set_error("write failed: " + path);
+    return SHB_ERR_INVALID_ARG;
+  }
+  return SHB_OK;
+}
+
+const char* kCoeffNames[9] = {"L0", "L1m1", "L10", "L11", "L2m2", "L2m1", "L20", "L21", "L22"};
+
+// path -> (parent/stem, extension) as std::filesystem::path would split it
+void split_path(const std::string& path, std::string& base, std::string& ext) {
+  const size_t slash = path.find_last_of('/');
+  const size_t dot = path.find_last_of('.');
+  const size_t name0 = slash == std::string::npos ? 0 : slash + 1;
+  // a leading dot of the file name does not start an extension
+  if (dot != std::string::npos && dot > name0 && path.size() - dot > 0) {
+    base = path.substr(0, dot);
+    ext = path.substr(dot);
+  } else {
+    base = path;
+    ext.clear();
+  }
+}
+
+}  // namespace
+
+shb_status save_sh_lightmap_device(shb_context* c, const float* d_sh, const float* d_env, int W, int H,
+                                   const std::string& path, int mode) {
+  if (mode == SHB_SAVE_COMBINED) {
+    ChanTable t{};
+    std::vector<std::string> names;
+    const char* rgb[3] = {".R", ".G", ".B"};
+    for (int i = 0; i < 9; ++i)
+      for (int k = 0; k < 3; ++k) {
+        t.c[t.n++] = ChanSpec{0, 3 * i + k};
+        names.push_back(std::string(kCoeffNames[i]) + rgb[k]);
+      }
+    t.c[t.n++] = ChanSpec{2, 0};
+    names.push_back("EnvVisibility");
+    return write_exr(c, d_sh, d_env, W, H, t, names, path);
+  }
+  std::string base, ext;
+  split_path(path, base, ext);
+  if (mode == SHB_SAVE_SPLIT_CHANNELS) {
+    for (int i = 0; i < 9; ++i) {
+      ChanTable t{};
+      std::vector<std::string> names = {"R", "G", "B"};
+      for (int k = 0; k < 3; ++k) t.c[t.n++] = ChanSpec{0, 3 * i + k};
+      if (i == 0) {
+        t.c[t.n++] = ChanSpec{2, 0};
+        names.push_back("A");
+      }
+      SHB_TRY(write_exr(c, d_sh, d_env, W, H, t, names, base + "_" + kCoeffNames[i] + ext));
+    }
+    return SHB_OK;
+  }
+  if (mode == SHB_SAVE_LUMINANCE_PACKED) {
+    const std::vector<std::string> names = {"R", "G", "B", "A"};
+    ChanTable t0{}, t1{}, t2{};
+    t0.c[0] = ChanSpec{0, 0};
+    t0.c[1] = ChanSpec{0, 1};
+    t0.c[2] = ChanSpec{0, 2};
+    t0.c[3] = ChanSpec{2, 0};
+    t0.n = 4;
+    for (int k = 0; k < 4; ++k) {
+      t1.c[k] = ChanSpec{1, 1 + k};
+      t2.c[k] = ChanSpec{1, 5 + k};
+    }
+    t1.n = t2.n = 4;
+    SHB_TRY(write_exr(c, d_sh, d_env, W, H, t0, names, base + "_packed_0" + ext));
+    SHB_TRY(write_exr(c, d_sh, d_env, W, H, t1, names, base + "_packed_1" + ext));
+    return write_exr(c, d_sh, d_env, W, H, t2, names, base + "_packed_2" + ext);
+  }
+  set_error("unknown save mode");
+  return SHB_ERR_INVALID_ARG;
+}
+
+}  // namespace shb

@@ -601,6 +601,29 @@ shb_status shb_bake(shb_scene* s, const shb_gbuffer* g, const shb_raster_config*
   return SHB_OK;
 }
 
+shb_status shb_save_sh_lightmap(shb_context* ctx, const float* sh, const float* env, int32_t width, int32_t height,
+                                int32_t device_ptrs, const char* path, int32_t mode) {
+  if (!ctx || !sh || !path || !*path) return bad("NULL argument");
+  if (width <= 0 || height <= 0) return bad("Invalid SHTexture dimensions or empty pixels.");
+  if (mode < SHB_SAVE_COMBINED || mode > SHB_SAVE_LUMINANCE_PACKED) return bad("unknown save mode");
+  SHB_CUDA(cudaSetDevice(ctx->device));
+  const size_t n = (size_t)width * height;
+  const float* dsh = sh;
+  const float* denv = env;
+  if (!device_ptrs) {
+    SHB_TRY(ctx->scratch[27].reserve(sizeof(float) * 28 * n));
+    float* d = ctx->scratch[27].as<float>();
+    SHB_CUDA(cudaMemcpyAsync(d, sh, sizeof(float) * 27 * n, cudaMemcpyHostToDevice, ctx->stream));
+    dsh = d;
+    denv = nullptr;
+    if (env) {
+      SHB_CUDA(cudaMemcpyAsync(d + 27 * n, env, sizeof(float) * n, cudaMemcpyHostToDevice, ctx->stream));
+      denv = d + 27 * n;
+    }
+  }
+  return save_sh_lightmap_device(ctx, dsh, denv, width, height, std::string(path), mode);
+}
+
 shb_status shb_scene_set_params(shb_scene* s, const float* albedo_rgb, const uint8_t* use_override,
                                 const float* light_intensity) {
   if (!s) return bad("NULL scene");

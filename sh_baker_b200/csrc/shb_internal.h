@@ -135,7 +135,7 @@ struct shb_context {
   cudaStream_t stream = nullptr;
   uint64_t launches = 0;
   // scratch reused across calls
-  shb::DevBuf scratch[26];
+  shb::DevBuf scratch[28];
   shb::DevBuf counters;
   void* host_pinned = nullptr;
   size_t host_pinned_bytes = 0;
@@ -211,6 +211,9 @@ struct BatchParams {
 shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs, const BatchParams& prm,
                              shb_bake_stats* stats);
 shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n, shb_hit* d_hits);
+// SaveSHLightMap (exr.cu): device SH (27 f32) and env (f32, nullable) texels.
+shb_status save_sh_lightmap_device(shb_context* c, const float* d_sh, const float* d_env, int W, int H,
+                                   const std::string& path, int mode);
 // Path-replay adjoint of bake_device: grad[3 * mat_count + light_count] (device).
 shb_status backward_device(shb_scene* s, const shb_surface_point* d_pts, int W, int H, const shb_bake_config* cfg,
                            const float* d_dsh, double* d_grad, shb_bake_stats* stats);

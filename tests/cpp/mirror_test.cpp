@@ -5,6 +5,7 @@
 // Exit status 0 when every check passes.
 #include <cmath>
 #include <cstdio>
+#include <filesystem>
 
 #include "sh_baker/sh_baker.h"
 
@@ -169,6 +170,28 @@ void BackwardLinearInIntensity() {
   EXPECT(g.d_albedo.size() == 3);
 }
 
+// SaveSHLightMap: a 2x2 texture in each mode writes the reference's files.
+void SaveModes() {
+  SHTexture sh;
+  sh.width = sh.height = 2;
+  sh.pixels.resize(4);
+  for (auto& p : sh.pixels)
+    for (auto& c : p.coeffs) c = Vector3f(0.5f, 0.25f, 2.0f);
+  Texture32F env;
+  env.width = env.height = 2;
+  env.pixel_data = {1.0f, 0.5f, 0.0f, 0.25f};
+  const std::string dir = std::filesystem::temp_directory_path() / "shb_mirror_exr";
+  std::filesystem::create_directories(dir);
+  EXPECT(SaveSHLightMap(sh, env, dir + "/lightmap.exr"));
+  EXPECT(SaveSHLightMap(sh, env, dir + "/lightmap.exr", SaveMode::kLuminancePacked));
+  EXPECT(SaveSHLightMap(sh, env, dir + "/lightmap.exr", SaveMode::kSplitChannels));
+  for (const char* f : {"lightmap.exr", "lightmap_packed_0.exr", "lightmap_packed_2.exr", "lightmap_L0.exr",
+                        "lightmap_L22.exr"})
+    EXPECT(std::filesystem::file_size(dir + "/" + f) > 100);
+  EXPECT(!SaveSHLightMap(SHTexture{}, env, dir + "/empty.exr"));
+  std::filesystem::remove_all(dir);
+}
+
 int main() {
   try {
     RasterizeQuad();
@@ -176,6 +199,7 @@ int main() {
     Dilation();
     BakeSimpleQuad();
     BackwardLinearInIntensity();
+    SaveModes();
   } catch (const std::exception& e) {
     std::printf("exception: %s\n", e.what());
     return 2;
