@@ -13,6 +13,7 @@
  *                         (src/baker.h:35-36)        -> shb_downsample (channels = 1)
  *   Dilate<T>             (src/dilation.h:14-16)     -> shb_dilate (kind = SH9 / F32 / U8)
  *   SaveSHLightMap        (src/saver.h:45-48)        -> shb_save_sh_lightmap
+ *   LoadScene             (src/loader.h)             -> shb_load_gltf
  *
  * Plain C types only: host pointers are owned by the caller, device objects
  * are owned by the opaque handles.  Every entry point returns a shb_status;
@@ -400,6 +401,29 @@ typedef enum shb_save_mode {
 SHB_API shb_status shb_save_sh_lightmap(shb_context* ctx, const float* sh, const float* env,
                                         int32_t width, int32_t height, int32_t device_ptrs,
                                         const char* path, int32_t mode);
+
+/* ---- LoadScene (src/loader.h, src/loader.cpp:144-844) ------------------ */
+
+/* A scene read from a .gltf / .glb file and owned by the handle; its
+ * shb_scene_desc (valid until shb_host_scene_destroy) feeds
+ * shb_scene_upload.  Missing material / POSITION / NORMAL / TEXCOORD_0 on a
+ * primitive, an unreadable file or an unsupported texture (not PNG) are
+ * SHB_ERR_INVALID_ARG (the reference returns nullopt).  Emissive primitives
+ * become area lights; TEXCOORD_1 becomes the lightmap UVs. */
+typedef struct shb_host_scene shb_host_scene;
+SHB_API shb_status shb_load_gltf(const char* path, shb_host_scene** out);
+SHB_API const shb_scene_desc* shb_host_scene_desc(const shb_host_scene* scene);
+SHB_API shb_status shb_host_scene_destroy(shb_host_scene* scene);
+/* A loaded material's name and the absolute path of its albedo image file
+ * (NULL when the albedo is not an external file); valid with the handle. */
+SHB_API shb_status shb_host_scene_material_info(const shb_host_scene* scene, int32_t material,
+                                                const char** name, const char** albedo_file);
+
+/* SaveScene (src/saver.h:50-53, src/saver.cpp:423-781): writes `path`
+ * (.gltf) and <stem>.bin beside it; albedo image files are copied next to
+ * it.  material_names / albedo_files: one entry per material or NULL. */
+SHB_API shb_status shb_save_gltf(const shb_scene_desc* scene, const char* const* material_names,
+                                 const char* const* albedo_files, const char* path);
 
 /* ---- FindOcclusion (src/occlusion.cpp:9-107), batched ----------------- */
 

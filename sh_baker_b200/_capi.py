@@ -155,6 +155,11 @@ SIGNATURES = {
     "shb_dilate_noalloc": (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, vp, vp, C.c_int32]),
     "shb_bake_batch": (C.c_int, [vp, vp, C.c_int32, C.POINTER(BatchOptions), C.POINTER(BakeStats)]),
     "shb_scene_set_params": (C.c_int, [vp, vp, vp, vp]),
+    "shb_load_gltf": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
+    "shb_host_scene_desc": (C.POINTER(SceneDesc), [vp]),
+    "shb_host_scene_destroy": (C.c_int, [vp]),
+    "shb_host_scene_material_info": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p)]),
+    "shb_save_gltf": (C.c_int, [C.POINTER(SceneDesc), vp, vp, C.c_char_p]),
     "shb_save_sh_lightmap": (C.c_int, [vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_char_p, C.c_int32]),
     "shb_backward": (C.c_int, [vp, vp, C.POINTER(RasterConfig), C.POINTER(BakeConfig), vp, C.c_int32, vp, vp,
                                C.POINTER(BakeStats)]),

@@ -398,6 +398,43 @@ def bake_lightmap(scene, width: int, height: int, samples: int = 128, bounces: i
     return LightmapResult(sh, env, mask, st)
 
 
+def LoadScene(path, error: Optional[list] = None) -> Optional[Scene]:
+    """src/loader.h LoadScene: a .gltf / .glb file read by shb_load_gltf
+    (host only, no GPU).  None on failure, like the reference's nullopt; the
+    reason is appended to `error` when given."""
+    from .scene import unpack_scene
+    lib = A.load()
+    h = C.c_void_p()
+    st = lib.shb_load_gltf(str(path).encode(), C.byref(h))
+    if st != 0:
+        if error is not None:
+            error.append(lib.shb_last_error().decode())
+        return None
+    try:
+        return unpack_scene(lib.shb_host_scene_desc(h).contents)
+    finally:
+        lib.shb_host_scene_destroy(h)
+
+
+def SaveScene(scene: Scene, path, material_names=None, albedo_files=None) -> bool:
+    """src/saver.h:50-53 SaveScene: glTF + <stem>.bin (host only).  False
+    on failure, like the reference."""
+    lib = A.load()
+    desc, keep = pack_scene(scene)
+    n = len(scene.materials)
+
+    def strs(v):
+        if v is None:
+            return None
+        arr = (C.c_char_p * max(1, n))()
+        for i in range(n):
+            arr[i] = v[i].encode() if v[i] else None
+        keep.append(arr)
+        return C.cast(arr, C.c_void_p)
+
+    return lib.shb_save_gltf(C.byref(desc), strs(material_names), strs(albedo_files), str(path).encode()) == 0
+
+
 class SaveMode:
     """src/saver.h:21-25."""
     kCombined = A.SAVE_COMBINED

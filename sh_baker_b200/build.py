@@ -27,6 +27,7 @@ SOURCES = {
     "bvh_build.cu": ["-fmad=true"],
     "batch.cu": ["-fmad=false"],
     "exr.cu": ["-fmad=false"],
+    "gltf.cpp": [],
 }
 HEADERS = ["shb_internal.h", "shb_math.cuh", "wavefront.h"]
 

@@ -46,7 +46,7 @@ void srgb_upload(const float table[256]);
 // Rotation part of an affine map (Eigen Transform::rotation(): polar
 // decomposition M = U S V^T, R = U diag(x,1,1) V^T, x = sign det(U V^T)),
 // by cyclic Jacobi on M^T M in double precision.
-static void polar_rotation(const float Lf[9], float Rout[9]) {
+void polar_rotation(const float Lf[9], float Rout[9]) {
   bool ident = true;
   for (int i = 0; i < 9; ++i) ident = ident && (Lf[i] == ((i % 4 == 0) ? 1.f : 0.f));
   if (ident) {

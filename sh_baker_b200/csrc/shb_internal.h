@@ -218,6 +218,10 @@ shb_status save_sh_lightmap_device(shb_context* c, const float* d_sh, const floa
 shb_status backward_device(shb_scene* s, const shb_surface_point* d_pts, int W, int H, const shb_bake_config* cfg,
                            const float* d_dsh, double* d_grad, shb_bake_stats* stats);
 
+// Rotation of the polar decomposition of a row-major 3x3 (Eigen's
+// Transform::rotation()), shb_capi.cu.
+void polar_rotation(const float L[9], float R[9]);
+
 // sRGB -> linear table (computed on the host with powf, colorspace.h:10-14)
 void srgb_table(float out[256]);
 

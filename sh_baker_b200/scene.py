@@ -144,3 +144,38 @@ def surface_points_empty(n: int) -> np.ndarray:
     sp = np.zeros(n, dtype=SURFACE_POINT_DTYPE)
     sp["material_id"] = -1
     return sp
+
+
+def unpack_scene(desc: A.SceneDesc) -> Scene:
+    """Copies a shb_scene_desc (for example one returned by shb_load_gltf)
+    into a Scene."""
+    def arr(ptr, n, cols, dt=np.float32):
+        if not ptr or n == 0:
+            return None
+        return np.ctypeslib.as_array(ptr, shape=(n * cols,)).astype(dt).reshape(n, cols)
+
+    sc = Scene()
+    for i in range(desc.geometry_count):
+        d = desc.geometries[i]
+        nv = d.vertex_count
+        idx = (np.ctypeslib.as_array(d.indices, shape=(d.index_count,)).astype(np.uint32)
+               if d.indices and d.index_count else np.zeros(0, np.uint32))
+        sc.geometries.append(Geometry(vertices=arr(d.vertices, nv, 3), indices=idx, normals=arr(d.normals, nv, 3),
+                                      texture_uvs=arr(d.texture_uvs, nv, 2), lightmap_uvs=arr(d.lightmap_uvs, nv, 2),
+                                      tangents=arr(d.tangents, nv, 4), material_id=int(d.material_id),
+                                      transform=np.array(list(d.transform), np.float32).reshape(3, 4)))
+    for i in range(desc.material_count):
+        d = desc.materials[i]
+        n = d.albedo_width * d.albedo_height * d.albedo_channels
+        px = (np.ctypeslib.as_array(d.albedo_pixels, shape=(n,)).astype(np.uint8)
+              if d.albedo_pixels and n else np.zeros(0, np.uint8))
+        sc.materials.append(Material(albedo=Texture(d.albedo_width, d.albedo_height, d.albedo_channels, px),
+                                     emission_intensity=float(d.emission_intensity)))
+    for i in range(desc.light_count):
+        d = desc.lights[i]
+        sc.lights.append(Light(type=int(d.type), position=tuple(d.position), direction=tuple(d.direction),
+                               color=tuple(d.color), intensity=float(d.intensity),
+                               cos_inner_cone=float(d.cos_inner_cone), cos_outer_cone=float(d.cos_outer_cone),
+                               area=float(d.area), material_index=int(d.material_index),
+                               geometry_index=int(d.geometry_index)))
+    return sc

@@ -1,0 +1,224 @@
+"""LoadScene (shb_load_gltf, src/loader.cpp:144-844) on glTF files written
+by tests/gltf_fixture.py; host code only, no GPU."""
+import math
+
+import numpy as np
+import pytest
+
+from sh_baker_b200 import api
+from sh_baker_b200.scene import AREA, DIRECTIONAL, POINT, SPOT
+from tests.gltf_fixture import GltfBuilder, png_bytes, quad
+
+
+def quat_matrix(q):
+    x, y, z, w = q
+    return np.array([[1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)],
+                     [2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)],
+                     [2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)]])
+
+
+def affine(R, t):
+    m = np.eye(4)
+    m[:3, :3] = R
+    m[:3, 3] = t
+    return m
+
+
+def linear_to_srgb(x):
+    x = np.float32(x)
+    if x <= np.float32(0.0031308):
+        return int(np.rint(x * np.float32(12.92) * np.float32(255.0)))
+    return int(np.rint((np.float32(1.055) * np.float32(x) ** np.float32(1 / 2.4) - np.float32(0.055)) *
+                       np.float32(255.0)))
+
+
+def build_scene():
+    b = GltfBuilder()
+    pos, nrm, uv, idx = quad(2.0)
+    m_factor = b.material(factor=[0.5, 0.2, 0.3, 0.7], name="factor")
+    tex = np.array([[[255, 0, 0, 255], [0, 255, 0, 128], [0, 0, 255, 0]],
+                    [[10, 20, 30, 40], [50, 60, 70, 80], [90, 100, 110, 120]]], np.uint8)
+    m_tex = b.material(texture_png=png_bytes(tex), name="tex")
+    m_emit = b.material(factor=[1, 1, 1, 1], emissive_strength=3.0, name="emit")
+    # a degenerate triangle (repeated index) that the loader drops
+    idx_d = np.concatenate([idx, [1, 1, 2]]).astype(np.uint32)
+    p0 = b.primitive(pos, nrm, uv, uv * 0.5, idx=idx_d, material=m_factor, pad=4)
+    p1 = b.primitive(pos, nrm, uv, idx=idx.astype(np.uint16), material=m_tex, idx_type=5123)
+    p2 = b.primitive(pos * 0.5, nrm, uv, uv, idx=idx.astype(np.uint8), material=m_emit, idx_type=5121)
+    mesh0 = b.mesh([p0, p1])
+    mesh1 = b.mesh([p2])
+    q = [0.0, math.sin(math.pi / 8), 0.0, math.cos(math.pi / 8)]  # 45 deg about Y
+    child_m = affine(quat_matrix([math.sin(math.pi / 4), 0, 0, math.cos(math.pi / 4)]), [0, 0, 5])
+    child = b.node(root=False, mesh=mesh1, matrix=list(child_m.T.reshape(-1)))
+    parent = b.node(mesh=mesh0, translation=[1, 2, 3], rotation=q, scale=[2, 2, 2], children=[child])
+    lp = b.light(type="point", color=[1, 0.5, 0.25], intensity=20.0)
+    ls = b.light(type="spot", intensity=7.0, spot={"innerConeAngle": 0.3, "outerConeAngle": 0.6})
+    ld = b.light(type="directional", intensity=2.5)
+    b.node(translation=[0, 4, 0], extensions={"KHR_lights_punctual": {"light": lp}})
+    b.node(translation=[1, 1, 1], rotation=q, extensions={"KHR_lights_punctual": {"light": ls}})
+    b.node(rotation=[math.sin(math.pi / 4), 0, 0, math.cos(math.pi / 4)],
+           extensions={"KHR_lights_punctual": {"light": ld}})
+    expect = {"parent": affine(quat_matrix(q) * 2.0, [1, 2, 3]), "child_local": child_m, "q": q, "tex": tex,
+              "pos": pos, "nrm": nrm, "uv": uv, "idx": idx}
+    return b, expect
+
+
+@pytest.mark.parametrize("container", ["data", "bin", "glb"])
+def test_load_scene(tmp_path, container):
+    b, ex = build_scene()
+    path = b.write(tmp_path / ("scene.glb" if container == "glb" else "scene.gltf"), container)
+    sc = api.LoadScene(path)
+    assert sc is not None
+    assert len(sc.geometries) == 3 and len(sc.materials) == 3
+    g0, g1, g2 = sc.geometries
+    # transforms: parent TRS, child = parent * child matrix
+    np.testing.assert_allclose(g0.transform, ex["parent"][:3], atol=1e-6)
+    np.testing.assert_allclose(g2.transform, (ex["parent"] @ ex["child_local"])[:3], atol=1e-5)
+    # attributes, strided accessors, u8/u16/u32 indices, degenerate triangle dropped
+    np.testing.assert_array_equal(g0.vertices, ex["pos"])
+    np.testing.assert_array_equal(g0.normals, ex["nrm"])
+    np.testing.assert_array_equal(g0.lightmap_uvs, ex["uv"] * 0.5)
+    np.testing.assert_array_equal(g0.indices, ex["idx"])
+    np.testing.assert_array_equal(g1.indices, ex["idx"])
+    assert g1.lightmap_uvs is None
+    np.testing.assert_array_equal(g2.indices, ex["idx"])
+    # materials: baseColorFactor through LinearToSRGB, PNG texture, emission
+    m0, m1, m2 = sc.materials
+    assert (m0.albedo.width, m0.albedo.height, m0.albedo.channels) == (1, 1, 4)
+    assert list(m0.albedo.pixel_data) == [linear_to_srgb(0.5), linear_to_srgb(0.2), linear_to_srgb(0.3),
+                                          int(np.rint(0.7 * 255))]
+    assert (m1.albedo.width, m1.albedo.height, m1.albedo.channels) == (3, 2, 4)
+    np.testing.assert_array_equal(m1.albedo.pixel_data, ex["tex"].reshape(-1))
+    assert m2.emission_intensity == 3.0 and m0.emission_intensity == 0.0
+    # lights: area light for the emissive primitive (added while traversing),
+    # then point, spot, directional in node order
+    kinds = [L.type for L in sc.lights]
+    assert kinds == [AREA, POINT, SPOT, DIRECTIONAL]
+    area, point, spot, sun = sc.lights
+    assert area.material_index == 2 and area.geometry_index == 2 and area.intensity == 3.0
+    assert area.area == pytest.approx(1.0)  # object-space area of the 1x1 quad
+    np.testing.assert_allclose(point.position, [0, 4, 0])
+    np.testing.assert_allclose(point.color, [1, 0.5, 0.25])
+    assert point.intensity == 20.0
+    np.testing.assert_allclose(spot.position, [1, 1, 1])
+    d = quat_matrix(ex["q"]) @ np.array([0, 0, -1.0])
+    np.testing.assert_allclose(spot.direction, d / np.linalg.norm(d), atol=1e-6)
+    assert spot.cos_inner_cone == pytest.approx(math.cos(0.3)) and spot.cos_outer_cone == pytest.approx(math.cos(0.6))
+    np.testing.assert_allclose(sun.direction, [0, 1, 0], atol=1e-6)
+
+
+def test_generated_tangents(tmp_path):
+    b = GltfBuilder()
+    pos, nrm, uv, idx = quad()
+    b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=b.material(factor=[1, 1, 1, 1]))]))
+    # second primitive: v flipped -> left-handed frame
+    g = api.LoadScene(b.write(tmp_path / "t.gltf")).geometries[0]
+    np.testing.assert_allclose(g.tangents, np.tile([[1, 0, 0, 1]], (4, 1)), atol=1e-6)
+    b2 = GltfBuilder()
+    b2.node(mesh=b2.mesh([b2.primitive(pos, nrm, uv * [1, -1], idx=idx, material=b2.material(factor=[1, 1, 1, 1]))]))
+    g2 = api.LoadScene(b2.write(tmp_path / "t2.gltf")).geometries[0]
+    np.testing.assert_allclose(g2.tangents, np.tile([[1, 0, 0, -1]], (4, 1)), atol=1e-6)
+    # a TANGENT attribute is kept as given
+    t = np.tile(np.array([[0, 1, 0, -1]], np.float32), (4, 1))
+    b3 = GltfBuilder()
+    b3.node(mesh=b3.mesh([b3.primitive(pos, nrm, uv, tan=t, idx=idx, material=b3.material(factor=[1, 1, 1, 1]))]))
+    np.testing.assert_array_equal(api.LoadScene(b3.write(tmp_path / "t3.gltf")).geometries[0].tangents, t)
+
+
+def test_png_colour_types(tmp_path):
+    gray = np.array([[[0], [128]], [[255], [7]]], np.uint8)
+    pal = np.array([[0, 1], [2, 1]], np.uint8)
+    palette = np.array([[10, 20, 30], [40, 50, 60], [70, 80, 90]], np.uint8)
+    b = GltfBuilder()
+    pos, nrm, uv, idx = quad()
+    m_g = b.material(texture_png=png_bytes(gray))
+    m_p = b.material(texture_png=png_bytes(pal, palette=palette, trns=[255, 128]))
+    b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=m_g),
+                        b.primitive(pos, nrm, uv, idx=idx, material=m_p)]))
+    sc = api.LoadScene(b.write(tmp_path / "p.gltf"))
+    mg, mp = sc.materials
+    assert mg.albedo.channels == 3
+    np.testing.assert_array_equal(mg.albedo.pixel_data.reshape(2, 2, 3), np.repeat(gray, 3, axis=2))
+    assert mp.albedo.channels == 4
+    exp = np.concatenate([palette[pal], np.array([255, 128, 255])[pal][..., None]], axis=2)
+    np.testing.assert_array_equal(mp.albedo.pixel_data.reshape(2, 2, 4), exp)
+
+
+def test_defaults_and_errors(tmp_path):
+    pos, nrm, uv, idx = quad()
+    # no materials: a white default (a primitive must still name material 0)
+    b = GltfBuilder()
+    b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=0)]))
+    sc = api.LoadScene(b.write(tmp_path / "d.gltf"))
+    assert len(sc.materials) == 1 and list(sc.materials[0].albedo.pixel_data) == [255, 255, 255, 255]
+    # no indices: no triangles
+    b = GltfBuilder()
+    b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, material=b.material(factor=[1, 1, 1, 1]))]))
+    assert len(api.LoadScene(b.write(tmp_path / "n.gltf")).geometries[0].indices) == 0
+    # missing NORMAL / material / TEXCOORD_0, unreadable file, JPEG texture
+    for kw, what in [({"nrm": None}, "NORMAL"), ({"material": None}, "material"), ({"uv0": None}, "TEXCOORD_0")]:
+        b = GltfBuilder()
+        args = dict(pos=pos, nrm=nrm, uv0=uv, idx=idx, material=0)
+        args.update(kw)
+        if args["material"] is not None:
+            b.material(factor=[1, 1, 1, 1])
+        b.node(mesh=b.mesh([b.primitive(**args)]))
+        err = []
+        assert api.LoadScene(b.write(tmp_path / "e.gltf"), err) is None
+        assert what in err[0]
+    err = []
+    assert api.LoadScene(tmp_path / "missing.gltf", err) is None and "cannot read" in err[0]
+    b = GltfBuilder()
+    b.material(texture_png=b"\xff\xd8\xff\xe0 not a png")
+    b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=0)]))
+    err = []
+    assert api.LoadScene(b.write(tmp_path / "j.gltf"), err) is None and "PNG" in err[0]
+
+
+def test_save_scene_round_trip(tmp_path):
+    """SaveScene then LoadScene gives back geometry, transforms, lightmap
+    UVs, 1x1 albedos (through SRGBToLinear / LinearToSRGB) and the punctual
+    lights; like the reference, emission strength is not written, so area
+    lights do not come back."""
+    b, ex = build_scene()
+    sc = api.LoadScene(b.write(tmp_path / "in.gltf"))
+    out = tmp_path / "out" / "scene.gltf"
+    out.parent.mkdir()
+    assert api.SaveScene(sc, out)
+    assert (out.parent / "scene.bin").exists()
+    back = api.LoadScene(out)
+    assert back is not None and len(back.geometries) == 3
+    for a, c in zip(sc.geometries, back.geometries):
+        np.testing.assert_array_equal(a.vertices, c.vertices)
+        np.testing.assert_array_equal(a.indices, c.indices)
+        np.testing.assert_array_equal(a.tangents, c.tangents)
+        np.testing.assert_allclose(a.transform, c.transform, rtol=0, atol=1e-6)
+        if a.lightmap_uvs is None:
+            assert c.lightmap_uvs is None
+        else:
+            np.testing.assert_array_equal(a.lightmap_uvs, c.lightmap_uvs)
+    np.testing.assert_array_equal(sc.materials[0].albedo.pixel_data, back.materials[0].albedo.pixel_data)
+    punctual = [L for L in sc.lights if L.type != AREA]
+    assert [L.type for L in back.lights] == [L.type for L in punctual]
+    for a, c in zip(punctual, back.lights):
+        np.testing.assert_allclose(a.position, c.position, atol=1e-6)
+        np.testing.assert_allclose(a.color, c.color, atol=1e-7)
+        assert a.intensity == c.intensity
+        if a.type != POINT:
+            np.testing.assert_allclose(a.direction, c.direction, atol=1e-5)
+        if a.type == SPOT:
+            assert c.cos_outer_cone == pytest.approx(a.cos_outer_cone, abs=1e-6)
+
+
+def test_srgb_bytes_round_trip_through_factor(tmp_path):
+    """A 1x1 albedo byte survives SaveScene's SRGBToLinear and the loader's
+    LinearToSRGB for all 256 values."""
+    from sh_baker_b200.scene import Geometry, Material, Scene, Texture
+    pos, nrm, uv, idx = quad()
+    mats = [Material(albedo=Texture(1, 1, 4, np.array([v, 255 - v, (v * 7) % 256, v], np.uint8)))
+            for v in range(256)]
+    sc = Scene([Geometry(pos, idx, nrm, uv, uv, None, 0)], mats, [])
+    assert api.SaveScene(sc, tmp_path / "s.gltf")
+    back = api.LoadScene(tmp_path / "s.gltf")
+    for a, c in zip(mats, back.materials):
+        np.testing.assert_array_equal(a.albedo.pixel_data, c.albedo.pixel_data)
