@@ -62,7 +62,24 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
+    build_cli(verbose, force)
     return LIB
+
+
+CLI_SRC = PKG / "cli" / "sh_baker.cpp"
+CLI = PKG / "bin" / "sh_baker"
+
+
+def build_cli(verbose: bool = False, force: bool = False) -> Path:
+    """The sh_baker command line (the reference's flags) linked to libshb.so."""
+    CLI.parent.mkdir(exist_ok=True)
+    if force or _newer(CLI, [CLI_SRC, LIB, PKG.parent / "include" / "shb.h", Path(__file__)]):
+        cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", str(PKG.parent / "include"), str(CLI_SRC), "-L", str(PKG),
+               "-lshb", "-lz", "-Wl,-rpath,$ORIGIN/..", "-o", str(CLI)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        subprocess.run(cmd, check=True)
+    return CLI
 
 
 if __name__ == "__main__":
