@@ -515,7 +515,8 @@ def main():
             "traffic": traffic, "kernel": dom, "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
             "bytes_per_ray": bpr, "rays_per_launch": k_rays / max(k_launch, 1),
             "launch_ms": k_ms / max(k_launch, 1),
-            "kernel_ms": {"closest_hit": ext_ms / args.steps, "any_hit": sh_ms / args.steps},
+            "kernel_ms": {"closest_hit": ext_ms / args.steps, "any_hit": sh_ms / args.steps,
+                          "shade": sum(s.shade_kernel_ms for s in stats) / args.steps},
             "rays_per_s": (ext_rays + sh_rays) / (ms / 1e3)}
 
     # end to end through the public API from pinned host memory

@@ -184,7 +184,7 @@ typedef struct shb_bake_stats {
   double trace_ms;
   double extend_kernel_ms; /* sum of closest-hit kernel durations         */
   double shadow_kernel_ms;
-  double shade_kernel_ms;
+  double shade_kernel_ms;   /* generate + shade + resolve kernel durations   */
   uint64_t extend_launches;
   uint64_t shadow_launches;
 } shb_bake_stats;

@@ -20,11 +20,23 @@
 
 namespace shb {
 
-__constant__ float c_srgb[256];
+// sRGB -> linear table in global memory (L1-cached reads): lanes of a warp
+// read different entries, which constant memory would serialise.
+__device__ float g_srgb[256];
 
 namespace {
 
 constexpr int kThreads = 256;
+// Launch bounds of the shading kernels: SHB_SHADE_BLOCKS_PER_SM > 0 asks
+// the compiler to fit that many resident blocks per SM (fewer registers).
+#ifndef SHB_SHADE_BLOCKS_PER_SM
+#define SHB_SHADE_BLOCKS_PER_SM 0
+#endif
+#if SHB_SHADE_BLOCKS_PER_SM > 0
+#define SHB_SHADE_BOUNDS __launch_bounds__(kThreads, SHB_SHADE_BLOCKS_PER_SM)
+#else
+#define SHB_SHADE_BOUNDS __launch_bounds__(kThreads)
+#endif
 // Alpha branches per path kept apart for deterministic accumulation: the
 // wave is shrunk by 2^min(bounces, kMaxBranchLog).  Branch slots beyond that
 // (more than six transmissive bounces) fall back to atomic accumulation.
@@ -67,7 +79,7 @@ __device__ __forceinline__ f3 get_albedo(const SceneView& sc, const DMat& m, f2 
   if (m.use_override) return {m.override_rgb[0], m.override_rgb[1], m.override_rgb[2]};
   if (m.c == 0) return {0.8f, 0.8f, 0.8f};
   const uint8_t* px = sc.pixels + m.pix_offset + tex_index(m, uv);
-  return {c_srgb[px[0]], c_srgb[px[1]], c_srgb[px[2]]};
+  return {__ldg(&g_srgb[px[0]]), __ldg(&g_srgb[px[1]]), __ldg(&g_srgb[px[2]])};
 }
 // src/material.cpp:57-67
 __device__ __forceinline__ float get_alpha(const SceneView& sc, const DMat& m, f2 uv) {
@@ -87,6 +99,20 @@ __device__ __forceinline__ float max_coeff_std(f3 a) {
   return a.x < m ? m : a.x;
 }
 
+// Area-light triangle records (built once per scene by build_area_tris):
+// float4 {v0, pdf}, {v1, uv0.x}, {v2, uv0.y}, {uv1, uv2} with object-space
+// vertices and pdf = max(1e-6, 1 / (n * area)) computed by the expressions
+// of SampleAreaLight, so a sample reads one 64-byte record instead of the
+// index, vertex and uv gathers.  area_info[area light] = (first record,
+// triangle count | has-texture-uv << 31).
+constexpr uint32_t kAreaHasUv = 0x80000000u;
+
+__device__ __forceinline__ float area_pdf(f3 v0, f3 v1, f3 v2, uint32_t n) {
+  float area = sqrtf(sqnorm(cross(v0 - v1, v0 - v2))) / 2.f;
+  float x = 1.f / (float)n * 1.f / area;
+  return 1e-6f < x ? x : 1e-6f;
+}
+
 // src/light.cpp:16-78; uniforms ubase (triangle), ubase+1, ubase+2.
 __device__ void sample_area(const SceneView& sc, const DLight& L, Event& ev, int ubase, f3& point, f3& rad,
                             float& pdf) {
@@ -94,12 +120,12 @@ __device__ void sample_area(const SceneView& sc, const DLight& L, Event& ev, int
   rad = {0.f, 0.f, 0.f};
   pdf = 0.f;
   if (L.geom < 0 || L.mat < 0) return;
-  DGeom g = sc.geoms[L.geom];
-  uint32_t n = g.tri_count;
+  const uint2 info = sc.area_info[L.area_ord];
+  const uint32_t n = info.y & ~kAreaHasUv;
   if (n == 0) return;
   uint32_t tri = ev.tri(ubase, n);
-  uint32_t p = g.prim_base + tri;
-  uint32_t i0 = sc.tri_vidx[3 * p], i1 = sc.tri_vidx[3 * p + 1], i2 = sc.tri_vidx[3 * p + 2];
+  const float4* r = sc.area_tris + 4 * ((size_t)info.x + tri);
+  const float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
   float u1 = ev.u(ubase + 1);
   float u2 = ev.u(ubase + 2);
   if (u1 + u2 > 1.0f) {
@@ -107,14 +133,32 @@ __device__ void sample_area(const SceneView& sc, const DLight& L, Event& ev, int
     u2 = 1.0f - u2;
   }
   float w = 1.0f - u1 - u2;
-  f3 v0 = ld3(sc.obj_v, i0), v1 = ld3(sc.obj_v, i1), v2 = ld3(sc.obj_v, i2);
+  f3 v0 = {a.x, a.y, a.z}, v1 = {b.x, b.y, b.z}, v2 = {c.x, c.y, c.z};
   point = w * v0 + u1 * v1 + u2 * v2;
   f2 uv = {0.f, 0.f};
-  if (g.flags & GEOM_HAS_TEXUV) uv = w * ld2(sc.tex_uv, i0) + u1 * ld2(sc.tex_uv, i1) + u2 * ld2(sc.tex_uv, i2);
+  if (info.y & kAreaHasUv) uv = w * f2{b.w, c.w} + u1 * f2{d.x, d.y} + u2 * f2{d.z, d.w};
   rad = get_emission(sc, load_mat(sc, L.mat), uv);
-  float area = sqrtf(sqnorm(cross(v0 - v1, v0 - v2))) / 2.f;
-  float x = 1.f / (float)n * 1.f / area;
-  pdf = 1e-6f < x ? x : 1e-6f;
+  pdf = a.w;
+}
+
+// entries: (global triangle, triangle count of its light, has uv, 0)
+__global__ void k_area_tris(SceneView sc, const uint4* __restrict__ entries, int count, float4* __restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const uint4 e = entries[i];
+    const uint32_t p = e.x;
+    const uint32_t i0 = sc.tri_vidx[3 * p], i1 = sc.tri_vidx[3 * p + 1], i2 = sc.tri_vidx[3 * p + 2];
+    const f3 v0 = ld3(sc.obj_v, i0), v1 = ld3(sc.obj_v, i1), v2 = ld3(sc.obj_v, i2);
+    f2 t0 = {0.f, 0.f}, t1 = t0, t2 = t0;
+    if (e.z) {
+      t0 = ld2(sc.tex_uv, i0);
+      t1 = ld2(sc.tex_uv, i1);
+      t2 = ld2(sc.tex_uv, i2);
+    }
+    out[4 * (size_t)i] = make_float4(v0.x, v0.y, v0.z, area_pdf(v0, v1, v2, e.y));
+    out[4 * (size_t)i + 1] = make_float4(v1.x, v1.y, v1.z, t0.x);
+    out[4 * (size_t)i + 2] = make_float4(v2.x, v2.y, v2.z, t0.y);
+    out[4 * (size_t)i + 3] = make_float4(t1.x, t1.y, t2.x, t2.y);
+  }
 }
 
 struct LightEval {
@@ -440,7 +484,7 @@ __device__ __forceinline__ int find_tile(const WaveArgs& a, int64_t x) {
 
 // ------------------------------------------------------------- generate --
 template <bool BWD>
-__global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
+__global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const int64_t warp_id = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
@@ -547,7 +591,7 @@ __global__ void __launch_bounds__(kThreads) k_generate(WaveArgs a) {
 // = D X + beta dX for a collected term X, and the child tangent of a bounce
 // with factor f = alpha rho h is D f + [m] beta alpha h.
 template <bool BWD>
-__global__ void __launch_bounds__(kThreads) k_shade(WaveArgs a, int cur, int depth) {
+__global__ void SHB_SHADE_BOUNDS k_shade(WaveArgs a, int cur, int depth) {
   extern __shared__ float sgrad[];
   if (BWD) grad_zero(sgrad, a.n_params);
   const int n = min(a.cnt[cur], a.ext_cap);
@@ -958,7 +1002,37 @@ inline int grid_for(int64_t n) {
 
 }  // namespace
 
-void srgb_upload(const float table[256]) { cudaMemcpyToSymbol(c_srgb, table, sizeof(float) * 256); }
+void srgb_upload(const float table[256]) { cudaMemcpyToSymbol(g_srgb, table, sizeof(float) * 256); }
+
+// Area-light triangle records of a scene (see sample_area).
+shb_status build_area_tris(shb_scene* s) {
+  std::vector<uint2> info(std::max<uint32_t>(s->area_light_count, 1), make_uint2(0u, 0u));
+  std::vector<uint4> entries;
+  for (const DLight& L : s->h_lights) {
+    if (L.type != SHB_LIGHT_AREA || L.area_ord < 0) continue;
+    if (L.geom < 0 || L.mat < 0 || (size_t)L.geom >= s->h_geoms.size()) continue;
+    const DGeom& g = s->h_geoms[(size_t)L.geom];
+    const uint32_t has_uv = (g.flags & GEOM_HAS_TEXUV) ? 1u : 0u;
+    info[(size_t)L.area_ord] = make_uint2((uint32_t)entries.size(), g.tri_count | (has_uv ? kAreaHasUv : 0u));
+    for (uint32_t t = 0; t < g.tri_count; ++t) entries.push_back(make_uint4(g.prim_base + t, g.tri_count, has_uv, 0u));
+  }
+  cudaStream_t st = s->ctx->stream;
+  SHB_TRY(s->area_info.reserve(sizeof(uint2) * info.size()));
+  SHB_CUDA(cudaMemcpyAsync(s->area_info.ptr, info.data(), sizeof(uint2) * info.size(), cudaMemcpyHostToDevice, st));
+  SHB_TRY(s->area_tris.reserve(sizeof(float4) * 4 * std::max<size_t>(entries.size(), 1)));
+  if (!entries.empty()) {
+    DevBuf tmp;
+    SHB_TRY(tmp.reserve(sizeof(uint4) * entries.size()));
+    SHB_CUDA(cudaMemcpyAsync(tmp.ptr, entries.data(), sizeof(uint4) * entries.size(), cudaMemcpyHostToDevice, st));
+    const int n = (int)entries.size();
+    k_area_tris<<<std::min((n + 255) / 256, 148 * 8), 256, 0, st>>>(s->view(), tmp.as<uint4>(), n,
+                                                                      s->area_tris.as<float4>());
+    count_launch(s->ctx, 1);
+    SHB_CUDA(cudaGetLastError());
+    SHB_CUDA(cudaStreamSynchronize(st));  // tmp is freed on return
+  }
+  return SHB_OK;
+}
 
 shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n, shb_hit* d_hits) {
   shb_context* c = s->ctx;
@@ -1229,8 +1303,10 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
     a.P = w.P;
     a.n_tex = w.n_tex;
     cudaMemsetAsync(cnt, 0, sizeof(int) * (CNT_FETCH_SHADOW + 1), st);
+    Pair pg = stamp(2);
     if (bwd) k_generate<true><<<grid_for(w.P), kThreads, 0, st>>>(a);
     else k_generate<false><<<grid_for(w.P), kThreads, 0, st>>>(a);
+    close_stamp(pg);
     launches++;
     for (int k = 0; k <= w.max_bounces; ++k) {
       int cur = k & 1, nxt = cur ^ 1;
@@ -1240,8 +1316,10 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       launch_extend(st, tgrid, d_items, nb, a.info, a.ext[cur], cnt + cur, a.ext_cap, a.hits, cnt + CNT_FETCH_EXT,
                     cnt + CNT_ERROR, c64);
       close_stamp(pe);
+      Pair pd = stamp(2);
       if (bwd) k_shade<true><<<sgrid, kThreads, gsmem, st>>>(a, cur, k);
       else k_shade<false><<<sgrid, kThreads, 0, st>>>(a, cur, k);
+      close_stamp(pd);
       Pair ps = stamp(1);
       launch_shadow(st, tgrid, d_items, nb, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, a.pend,
                     cnt + CNT_FETCH_SHADOW, cnt + CNT_ERROR, c64);
@@ -1260,7 +1338,9 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       sh_launches++;
     }
     if (!bwd) {
+      Pair pr = stamp(2);
       k_resolve<<<grid_for(w.n_tex * 32), kThreads, 0, st>>>(a);
+      close_stamp(pr);
       launches++;
     }
   }
@@ -1285,7 +1365,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   SHB_CUDA(cudaMemcpyAsync(&h64, c64, sizeof(Counters64), cudaMemcpyDeviceToHost, st));
   if (c->profiling) cudaEventRecord(t_end, st);
   SHB_CUDA(cudaStreamSynchronize(st));
-  double ext_ms = 0.0, sh_ms = 0.0;
+  double ext_ms = 0.0, sh_ms = 0.0, shade_ms = 0.0;
   float total_ms = 0.f;
   if (c->profiling) {
     cudaEventElapsedTime(&total_ms, t_begin, t_end);
@@ -1295,7 +1375,8 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       float ms = 0.f;
       cudaEventElapsedTime(&ms, pr.a, pr.b);
       if (pr.kind == 0) ext_ms += ms;
-      else sh_ms += ms;
+      else if (pr.kind == 1) sh_ms += ms;
+      else shade_ms += ms;
       cudaEventDestroy(pr.a);
       cudaEventDestroy(pr.b);
     }
@@ -1315,6 +1396,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
     stats->trace_ms = total_ms;
     stats->extend_kernel_ms = ext_ms;
     stats->shadow_kernel_ms = sh_ms;
+    stats->shade_kernel_ms = shade_ms;
     stats->extend_launches = ext_launches;
     stats->shadow_launches = sh_launches;
   }

@@ -156,6 +156,8 @@ SceneView shb_scene::view() const {
   v.mats = mats.as<DMat>();
   v.pixels = pixels.as<uint8_t>();
   v.lights = lights.as<DLight>();
+  v.area_tris = area_tris.as<float4>();
+  v.area_info = area_info.as<uint2>();
   v.geom_count = geom_count;
   v.mat_count = mat_count;
   v.light_count = light_count;
@@ -413,6 +415,7 @@ shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene
   if (rc == SHB_OK) chk(s->world_t.reserve(sizeof(float) * 4 * (vbase ? vbase : 1)));
   if (rc == SHB_OK) chk(transform_vertices(s));
   if (rc == SHB_OK) chk(build_bvh(s));
+  if (rc == SHB_OK) chk(build_area_tris(s));
   if (rc == SHB_OK) {
     cudaError_t e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) rc = cuda_fail(e, "scene upload");

@@ -120,6 +120,8 @@ struct SceneView {
   const DMat* mats;
   const uint8_t* pixels;
   const DLight* lights;
+  const float4* area_tris;  // 4 per area-light triangle (shade.cu sample_area)
+  const uint2* area_info;   // per area light: first record, count | uv flag
   uint32_t geom_count, mat_count, light_count, area_light_count;
   uint32_t prim_count, vertex_count;
   int32_t has_alpha;     // any material with 4-channel albedo
@@ -146,6 +148,7 @@ struct shb_scene {
   // uploaded per-vertex arrays
   shb::DevBuf obj_v, obj_n, tex_uv, lm_uv, obj_t, world_v, world_n, world_t;
   shb::DevBuf tri_vidx, tri_geom, geoms, mats, pixels, lights, rot, lin, vgeom;
+  shb::DevBuf area_tris, area_info;
   uint32_t vertex_count = 0, prim_count = 0, geom_count = 0, mat_count = 0, light_count = 0;
   uint32_t area_light_count = 0;
   int32_t has_alpha = 0;
@@ -176,6 +179,7 @@ inline void count_launch(shb_context* c, uint64_t n = 1) { c->launches += n; }
 // kernels implemented in the .cu files
 shb_status transform_vertices(shb_scene* s);
 shb_status build_bvh(shb_scene* s);
+shb_status build_area_tris(shb_scene* s);
 shb_status rasterize_device(shb_scene* s, int W, int H, shb_surface_point* d_out);
 shb_status validity_mask_device(shb_context* c, const shb_surface_point* pts, int64_t n, uint8_t* out);
 shb_status downsample_mask_device(shb_context* c, const uint8_t* in, int w, int h, int s, uint8_t* out);

@@ -101,8 +101,10 @@ __device__ __forceinline__ bool tri_test(const TravRay& r, float4 a, float4 b, f
   return true;
 }
 
+// Byte k of w as a float (exact): one byte permute builds the bit pattern
+// 0x4B0000bb = 2^23 + bb, from which 2^23 is subtracted.
 __device__ __forceinline__ float byte_f(uint32_t w, int k) {
-  return __uint_as_float(0x4B000000u | ((w >> (8 * k)) & 0xFFu)) - 8388608.0f;
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | (uint32_t)k)) - 8388608.0f;
 }
 
 // Traversal state of one ray.  Groups are (base, bits): a node group has
