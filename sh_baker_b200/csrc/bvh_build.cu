@@ -16,8 +16,22 @@ namespace shb {
 
 namespace {
 
-constexpr int kBins = 16;
-constexpr int kMaxLeaf = 3;    // triangles per leaf child of a wide node
+// Binned SAH: bins per axis, largest leaf, and the cost of a node visit
+// relative to a triangle test in the leaf decision.
+#ifndef SHB_BVH_BINS
+#define SHB_BVH_BINS 32
+#endif
+#ifndef SHB_BVH_MAX_LEAF
+#define SHB_BVH_MAX_LEAF 3
+#endif
+#ifndef SHB_BVH_NODE_COST
+#define SHB_BVH_NODE_COST 1.0f
+#endif
+constexpr int kBins = SHB_BVH_BINS;
+constexpr int kMaxLeaf = SHB_BVH_MAX_LEAF;  // triangles per leaf child of a wide node
+// A wide node's triangle group is a 24-bit mask (bit 31 marks node groups in
+// the traversal), so its 8 leaf children hold at most 24 triangles.
+static_assert(kMaxLeaf >= 1 && kMaxLeaf * 8 <= 24, "leaf triangles must fit the 24-bit triangle group");
 constexpr int kMaxDepth = 40;  // deeper nodes use median splits
 constexpr int kThreads = 256;
 
@@ -257,7 +271,7 @@ __global__ void k_split(int n_act, int depth, const int* __restrict__ act, BNode
       bool leaf = false;
       if (count <= kMaxLeaf) {
         float A = half_area(nd.lo, nd.hi);
-        float split_cost = best_axis >= 0 && A > 0.f ? 1.0f + best / A : INFINITY;
+        float split_cost = best_axis >= 0 && A > 0.f ? SHB_BVH_NODE_COST + best / A : INFINITY;
         leaf = (float)count <= split_cost;
       }
       if (!leaf) {

@@ -6,8 +6,10 @@
 // once; a lane whose ray finishes takes the next queue entry (one atomic per
 // warp for all lanes that refill), so lanes do not wait for the slowest ray
 // of a batch.  Within a ray, children are visited in the ray-octant order of
-// their slots; triangle groups are postponed on the stack while too few
-// lanes of the warp want to test triangles (Ylitie, Karras, Laine 2017).
+// their slots.  Triangle groups can be postponed on the stack while too few
+// lanes of the warp want to test triangles (Ylitie, Karras, Laine 2017);
+// measured here that only slows both kernels down (the any-hit kernel most,
+// it ends on the first triangle it hits), so SHB_POSTPONE defaults to off.
 // The watertight triangle test (Woop, Benthin, Wald 2013) uses explicit
 // round-to-nearest intrinsics so it rounds exactly like the CPU restatement
 // even though this file is compiled with FMA contraction for the box tests.
@@ -19,7 +21,20 @@ namespace {
 
 constexpr int kStack = 64;
 constexpr int kTravThreads = 128;
-constexpr int kPostpone = 6;        // fewer lanes than this on triangles: postpone them
+// Resident blocks per SM the traversal kernels are register-limited to
+// (0: the compiler's choice).
+#ifndef SHB_TRAV_MIN_BLOCKS
+#define SHB_TRAV_MIN_BLOCKS 0
+#endif
+#if SHB_TRAV_MIN_BLOCKS > 0
+#define SHB_TRAV_BOUNDS __launch_bounds__(kTravThreads, SHB_TRAV_MIN_BLOCKS)
+#else
+#define SHB_TRAV_BOUNDS __launch_bounds__(kTravThreads)
+#endif
+#ifndef SHB_POSTPONE
+#define SHB_POSTPONE 0
+#endif
+constexpr int kPostpone = SHB_POSTPONE;  // fewer lanes than this on triangles: postpone them
 constexpr uint32_t kNodeGroup = 0x80000000u;
 constexpr uint32_t kMaxIters = 1u << 22;
 
@@ -288,7 +303,7 @@ __device__ __forceinline__ void consume(const Q& q, int n, int* fetch, int* err,
   }
 }
 
-__global__ void __launch_bounds__(kTravThreads) k_extend(const BakeItem* __restrict__ bakes, int n_bakes,
+__global__ void SHB_TRAV_BOUNDS k_extend(const BakeItem* __restrict__ bakes, int n_bakes,
                                                         const PathInfo* __restrict__ info, ExtQueue q,
                                                         const int* __restrict__ n_ptr, int cap,
                                                         float4* __restrict__ hits, int* fetch, int* err,
@@ -305,7 +320,7 @@ __global__ void __launch_bounds__(kTravThreads) k_extend(const BakeItem* __restr
   });
 }
 
-__global__ void __launch_bounds__(kTravThreads) k_shadow(const BakeItem* __restrict__ bakes, int n_bakes, ShadowQueue q,
+__global__ void SHB_TRAV_BOUNDS k_shadow(const BakeItem* __restrict__ bakes, int n_bakes, ShadowQueue q,
                                                         const int* __restrict__ n_ptr, int cap,
                                                         float4* __restrict__ path_L, float4* __restrict__ nee_li,
                                                         float4* __restrict__ pend, int* fetch, int* err,
