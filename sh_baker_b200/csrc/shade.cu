@@ -20,9 +20,9 @@
 
 namespace shb {
 
-// sRGB -> linear table in global memory (L1-cached reads): lanes of a warp
-// read different entries, which constant memory would serialise.
-__device__ float g_srgb[256];
+// sRGB -> linear table (constant memory; measured faster on the atrium
+// than an L1-cached global table).
+__constant__ float g_srgb[256];
 
 namespace {
 
@@ -79,7 +79,7 @@ __device__ __forceinline__ f3 get_albedo(const SceneView& sc, const DMat& m, f2 
   if (m.use_override) return {m.override_rgb[0], m.override_rgb[1], m.override_rgb[2]};
   if (m.c == 0) return {0.8f, 0.8f, 0.8f};
   const uint8_t* px = sc.pixels + m.pix_offset + tex_index(m, uv);
-  return {__ldg(&g_srgb[px[0]]), __ldg(&g_srgb[px[1]]), __ldg(&g_srgb[px[2]])};
+  return {g_srgb[px[0]], g_srgb[px[1]], g_srgb[px[2]]};
 }
 // src/material.cpp:57-67
 __device__ __forceinline__ float get_alpha(const SceneView& sc, const DMat& m, f2 uv) {
