@@ -402,6 +402,36 @@ SHB_API shb_status shb_save_sh_lightmap(shb_context* ctx, const float* sh, const
                                         int32_t width, int32_t height, int32_t device_ptrs,
                                         const char* path, int32_t mode);
 
+/* ---- SH previews (src/sh_cvt_main.cpp, glsl/viz.frag:42-99 as math) ---- */
+
+typedef enum shb_preview_mode {
+  SHB_PREVIEW_L0 = 0,        /* L0 coefficient as RGB (the EXR -> PNG tool)        */
+  SHB_PREVIEW_SH = 1,        /* max(0, SH9 radiance towards the direction)          */
+  SHB_PREVIEW_SH_PACKED = 2  /* the same from L0 + Rec. 709 luminance of L1/L2,
+                                re-coloured with L0's chroma (luminance-packed) */
+} shb_preview_mode;
+
+/* width x height texels of 27 floats -> width x height x 3 bytes of
+ * clamp(v) * 255 + 0.5 (optionally after Reinhard v / (1 + v)).  The
+ * direction is normals[3 * texel] when normals != NULL (same memory kind
+ * as sh), else direction[0..2].  sh / normals are device pointers when
+ * device_ptrs, else host; rgb_out is always host memory. */
+SHB_API shb_status shb_sh_preview(shb_context* ctx, const float* sh, int32_t width, int32_t height,
+                                  const float* normals, const float direction[3], int32_t mode,
+                                  int32_t reinhard, int32_t device_ptrs, uint8_t* rgb_out);
+
+/* The named channels of a single-part scanline OpenEXR file (NONE, ZIPS or
+ * ZIP compression; HALF, FLOAT or UINT samples) as float planes, count x
+ * width x height (host); with out == NULL only width and height are
+ * filled.  A missing channel is SHB_ERR_INVALID_ARG.  (The reference reads
+ * EXR through tinyexr, src/sh_cvt_main.cpp:27-59.) */
+SHB_API shb_status shb_exr_load_channels(const char* path, const char* const* names, int32_t count,
+                                         int32_t* width, int32_t* height, float* out);
+
+/* SaveTexture (src/saver.cpp:783-795): an 8-bit PNG of 1 to 4 channels. */
+SHB_API shb_status shb_write_png(const char* path, int32_t width, int32_t height, int32_t channels,
+                                 const uint8_t* pixels);
+
 /* ---- LoadScene (src/loader.h, src/loader.cpp:144-844) ------------------ */
 
 /* A scene read from a .gltf / .glb file and owned by the handle; its

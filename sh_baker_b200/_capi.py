@@ -124,6 +124,7 @@ assert C.sizeof(SurfacePoint) == 64
 assert C.sizeof(Hit) == 48
 
 SAVE_COMBINED, SAVE_SPLIT_CHANNELS, SAVE_LUMINANCE_PACKED = 0, 1, 2
+PREVIEW_L0, PREVIEW_SH, PREVIEW_SH_PACKED = 0, 1, 2
 
 vp = C.c_void_p
 # name -> (restype, argtypes); every symbol declared in include/shb.h
@@ -160,6 +161,10 @@ SIGNATURES = {
     "shb_host_scene_destroy": (C.c_int, [vp]),
     "shb_host_scene_material_info": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p)]),
     "shb_save_gltf": (C.c_int, [C.POINTER(SceneDesc), vp, vp, C.c_char_p]),
+    "shb_sh_preview": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp, vp, C.c_int32, C.c_int32, C.c_int32, vp]),
+    "shb_exr_load_channels": (C.c_int, [C.c_char_p, vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                        vp]),
+    "shb_write_png": (C.c_int, [C.c_char_p, C.c_int32, C.c_int32, C.c_int32, vp]),
     "shb_save_sh_lightmap": (C.c_int, [vp, vp, vp, C.c_int32, C.c_int32, C.c_int32, C.c_char_p, C.c_int32]),
     "shb_backward": (C.c_int, [vp, vp, C.POINTER(RasterConfig), C.POINTER(BakeConfig), vp, C.c_int32, vp, vp,
                                C.POINTER(BakeStats)]),

@@ -28,6 +28,7 @@ SOURCES = {
     "batch.cu": ["-fmad=false"],
     "exr.cu": ["-fmad=false"],
     "gltf.cpp": [],
+    "preview.cu": ["-fmad=false"],
 }
 HEADERS = ["shb_internal.h", "shb_math.cuh", "wavefront.h"]
 
@@ -66,19 +67,22 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     return LIB
 
 
-CLI_SRC = PKG / "cli" / "sh_baker.cpp"
 CLI = PKG / "bin" / "sh_baker"
+CVT = PKG / "bin" / "sh_cvt"
 
 
 def build_cli(verbose: bool = False, force: bool = False) -> Path:
-    """The sh_baker command line (the reference's flags) linked to libshb.so."""
+    """The command lines (the reference's sh_baker and sh_cvt, same flags)
+    linked to libshb.so."""
     CLI.parent.mkdir(exist_ok=True)
-    if force or _newer(CLI, [CLI_SRC, LIB, PKG.parent / "include" / "shb.h", Path(__file__)]):
-        cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", str(PKG.parent / "include"), str(CLI_SRC), "-L", str(PKG),
-               "-lshb", "-lz", "-Wl,-rpath,$ORIGIN/..", "-o", str(CLI)]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+    for exe in (CLI, CVT):
+        src = PKG / "cli" / (exe.name + ".cpp")
+        if force or _newer(exe, [src, LIB, PKG.parent / "include" / "shb.h", Path(__file__)]):
+            cmd = ["g++", "-std=c++17", "-O2", "-Wall", "-I", str(PKG.parent / "include"), str(src), "-L", str(PKG),
+                   "-lshb", "-Wl,-rpath,$ORIGIN/..", "-o", str(exe)]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
     return CLI
 
 

@@ -9,7 +9,6 @@
 // this build, so the lightmap UVs are taken from the input (TEXCOORD_1, as
 // SaveScene writes them); a scene without them is an error.
 #include <sys/stat.h>
-#include <zlib.h>
 
 #include <chrono>
 #include <cstdio>
@@ -130,43 +129,6 @@ bool mkdirs(const std::string& dir) {
   return true;
 }
 
-// SaveTexture (src/saver.cpp:783-795) as an 8-bit RGB PNG.
-bool write_png(const std::string& path, int w, int h, const std::vector<uint8_t>& rgb) {
-  std::vector<uint8_t> raw;
-  raw.reserve((size_t)h * (3 * (size_t)w + 1));
-  for (int y = 0; y < h; ++y) {
-    raw.push_back(0);
-    raw.insert(raw.end(), rgb.begin() + (size_t)y * 3 * w, rgb.begin() + (size_t)(y + 1) * 3 * w);
-  }
-  uLongf zl = compressBound((uLong)raw.size());
-  std::vector<uint8_t> z(zl);
-  if (compress2(z.data(), &zl, raw.data(), (uLong)raw.size(), Z_DEFAULT_COMPRESSION) != Z_OK) return false;
-  z.resize(zl);
-  FILE* f = std::fopen(path.c_str(), "wb");
-  if (!f) return false;
-  auto be = [](uint32_t v) {
-    return std::vector<uint8_t>{(uint8_t)(v >> 24), (uint8_t)(v >> 16), (uint8_t)(v >> 8), (uint8_t)v};
-  };
-  auto chunk = [&](const char* t, const std::vector<uint8_t>& d) {
-    std::vector<uint8_t> td(t, t + 4);
-    td.insert(td.end(), d.begin(), d.end());
-    auto l = be((uint32_t)d.size()), c = be((uint32_t)crc32(0, td.data(), (uInt)td.size()));
-    std::fwrite(l.data(), 1, 4, f);
-    std::fwrite(td.data(), 1, td.size(), f);
-    std::fwrite(c.data(), 1, 4, f);
-  };
-  static const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
-  std::fwrite(sig, 1, 8, f);
-  std::vector<uint8_t> ihdr = be((uint32_t)w);
-  auto hh = be((uint32_t)h);
-  ihdr.insert(ihdr.end(), hh.begin(), hh.end());
-  ihdr.insert(ihdr.end(), {8, 2, 0, 0, 0});
-  chunk("IHDR", ihdr);
-  chunk("IDAT", z);
-  chunk("IEND", {});
-  return std::fclose(f) == 0;
-}
-
 // CreateMaterialMap (src/rasterizer.cpp:243-287): a colour per material id
 // from an integer hash, lifted when all channels are dark.
 std::vector<uint8_t> material_map(const std::vector<shb_surface_point>& pts) {
@@ -233,7 +195,8 @@ int main(int argc, char** argv) {
     const std::string dir = F.output.empty() ? "." : F.output;
     mkdirs(dir);
     const std::string map_path = dir + "/material_map.png";
-    if (write_png(map_path, sw, sh, material_map(pts))) log("Material map saved to: " + map_path);
+    const std::vector<uint8_t> mm = material_map(pts);
+    if (shb_write_png(map_path.c_str(), sw, sh, 3, mm.data()) == SHB_OK) log("Material map saved to: " + map_path);
     else std::fprintf(stderr, "E Failed to save material map to: %s\n", map_path.c_str());
   }
 

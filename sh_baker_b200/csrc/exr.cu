@@ -264,7 +264,230 @@ void split_path(const std::string& path, std::string& base, std::string& ext) {
   }
 }
 
+// ------------------------------------------------------------- reader -----
+
+float half_to_float(uint16_t h) {
+  const uint32_t sign = (uint32_t)(h & 0x8000u) << 16;
+  uint32_t exp = (h >> 10) & 0x1Fu, man = h & 0x3FFu, bits;
+  if (exp == 0) {
+    if (man == 0) {
+      bits = sign;
+    } else {  // subnormal: renormalise
+      int e = -1;
+      do {
+        ++e;
+        man <<= 1;
+      } while (!(man & 0x400u));
+      bits = sign | ((uint32_t)(127 - 15 - e) << 23) | ((man & 0x3FFu) << 13);
+    }
+  } else if (exp == 31) {
+    bits = sign | 0x7F800000u | (man << 13);
+  } else {
+    bits = sign | ((exp + 112u) << 23) | (man << 13);
+  }
+  float f;
+  std::memcpy(&f, &bits, 4);
+  return f;
+}
+
+struct ExrFile {
+  int W = 0, H = 0, comp = 0;
+  std::vector<std::string> names;
+  std::vector<int> types;
+  std::vector<uint8_t> bytes;
+  size_t chunk_table = 0;
+};
+
+bool read_exr_header(const std::string& path, ExrFile& e, std::string& err) {
+  FILE* f = std::fopen(path.c_str(), "rb");
+  if (!f) {
+    err = "cannot read " + path;
+    return false;
+  }
+  std::fseek(f, 0, SEEK_END);
+  long n = std::ftell(f);
+  std::fseek(f, 0, SEEK_SET);
+  e.bytes.resize(n > 0 ? (size_t)n : 0);
+  size_t got = e.bytes.empty() ? 0 : std::fread(e.bytes.data(), 1, e.bytes.size(), f);
+  std::fclose(f);
+  const std::vector<uint8_t>& b = e.bytes;
+  if (got != b.size() || b.size() < 8 || b[0] != 0x76 || b[1] != 0x2f || b[2] != 0x31 || b[3] != 0x01) {
+    err = "not an OpenEXR file: " + path;
+    return false;
+  }
+  if (b[4] != 2 || (b[5] & 0x1E)) {
+    err = "only single-part scanline OpenEXR files are read";
+    return false;
+  }
+  size_t i = 8;
+  auto cstr = [&](std::string& out) {
+    size_t j = i;
+    while (j < b.size() && b[j]) ++j;
+    if (j >= b.size()) return false;
+    out.assign(reinterpret_cast<const char*>(&b[i]), j - i);
+    i = j + 1;
+    return true;
+  };
+  bool have_ch = false, have_dw = false;
+  int x0 = 0, y0 = 0, x1 = -1, y1 = -1;
+  while (i < b.size() && b[i]) {
+    std::string name, type;
+    int32_t size = 0;
+    if (!cstr(name) || !cstr(type) || i + 4 > b.size()) break;
+    std::memcpy(&size, &b[i], 4);
+    i += 4;
+    if (size < 0 || i + (size_t)size > b.size()) break;
+    const uint8_t* v = &b[i];
+    if (name == "channels") {
+      size_t k = 0;
+      while (k < (size_t)size && v[k]) {
+        size_t z = k;
+        while (z < (size_t)size && v[z]) ++z;
+        if (z + 17 > (size_t)size) break;
+        e.names.emplace_back(reinterpret_cast<const char*>(v + k), z - k);
+        int32_t t;
+        std::memcpy(&t, v + z + 1, 4);
+        e.types.push_back(t);
+        k = z + 17;
+      }
+      have_ch = true;
+    } else if (name == "compression" && size >= 1) {
+      e.comp = v[0];
+    } else if (name == "dataWindow" && size >= 16) {
+      int32_t w[4];
+      std::memcpy(w, v, 16);
+      x0 = w[0];
+      y0 = w[1];
+      x1 = w[2];
+      y1 = w[3];
+      have_dw = true;
+    }
+    i += (size_t)size;
+  }
+  if (!have_ch || !have_dw || i >= b.size() || x1 < x0 || y1 < y0) {
+    err = "bad OpenEXR header: " + path;
+    return false;
+  }
+  e.W = x1 - x0 + 1;
+  e.H = y1 - y0 + 1;
+  e.chunk_table = i + 1;
+  if (e.comp != 0 && e.comp != 2 && e.comp != 3) {
+    err = "unsupported OpenEXR compression (NONE, ZIPS and ZIP are read)";
+    return false;
+  }
+  for (int t : e.types)
+    if (t < 0 || t > 2) {
+      err = "bad OpenEXR channel type";
+      return false;
+    }
+  return true;
+}
+
+bool read_exr_channels(ExrFile& e, const std::vector<int>& want, float* out, std::string& err) {
+  const std::vector<uint8_t>& b = e.bytes;
+  const int lpc = e.comp == 3 ? 16 : 1;
+  const int chunks = (e.H + lpc - 1) / lpc;
+  size_t line_bytes = 0;
+  std::vector<size_t> off;
+  for (int t : e.types) {
+    off.push_back(line_bytes);
+    line_bytes += (size_t)e.W * (t == 1 ? 2 : 4);
+  }
+  if (e.chunk_table + 8ull * chunks > b.size()) {
+    err = "truncated OpenEXR offset table";
+    return false;
+  }
+  std::vector<uint8_t> raw, tmp;
+  for (int k = 0; k < chunks; ++k) {
+    uint64_t pos;
+    std::memcpy(&pos, &b[e.chunk_table + 8ull * k], 8);
+    if (pos + 8 > b.size()) {
+      err = "bad OpenEXR chunk offset";
+      return false;
+    }
+    int32_t y, size;
+    std::memcpy(&y, &b[pos], 4);
+    std::memcpy(&size, &b[pos + 4], 4);
+    const int ly = k * lpc;
+    const int lines = std::min(lpc, e.H - ly);
+    const size_t n = line_bytes * lines;
+    if (size < 0 || pos + 8 + (uint64_t)size > b.size()) {
+      err = "bad OpenEXR chunk size";
+      return false;
+    }
+    const uint8_t* d = &b[pos + 8];
+    raw.resize(n);
+    if (e.comp == 0 || (size_t)size == n) {
+      if ((size_t)size != n) {
+        err = "bad OpenEXR chunk size";
+        return false;
+      }
+      std::memcpy(raw.data(), d, n);
+    } else {
+      tmp.resize(n);
+      uLongf got = (uLongf)n;
+      if (uncompress(tmp.data(), &got, d, (uLong)size) != Z_OK || got != n) {
+        err = "OpenEXR chunk does not inflate";
+        return false;
+      }
+      // undo the delta predictor, then re-interleave the two byte halves
+      for (size_t q = 1; q < n; ++q) tmp[q] = (uint8_t)(tmp[q - 1] + tmp[q] - 128);
+      const size_t half = (n + 1) / 2;
+      for (size_t q = 0; q < n; ++q) raw[q] = (q & 1) ? tmp[half + q / 2] : tmp[q / 2];
+    }
+    for (int l = 0; l < lines; ++l)
+      for (size_t c = 0; c < want.size(); ++c) {
+        const int ch = want[c];
+        const uint8_t* src = raw.data() + (size_t)l * line_bytes + off[(size_t)ch];
+        float* dst = out + c * (size_t)e.W * e.H + (size_t)(ly + l) * e.W;
+        for (int x = 0; x < e.W; ++x) {
+          if (e.types[(size_t)ch] == 1) {
+            uint16_t h;
+            std::memcpy(&h, src + 2 * (size_t)x, 2);
+            dst[x] = half_to_float(h);
+          } else if (e.types[(size_t)ch] == 2) {
+            std::memcpy(&dst[x], src + 4 * (size_t)x, 4);
+          } else {
+            uint32_t u;
+            std::memcpy(&u, src + 4 * (size_t)x, 4);
+            dst[x] = (float)u;
+          }
+        }
+      }
+  }
+  return true;
+}
+
 }  // namespace
+
+// Named channels of an OpenEXR file as float planes (n x width x height);
+// with out == NULL only the dimensions are returned.
+shb_status exr_load_channels(const char* path, const char* const* names, int n, int* width, int* height, float* out) {
+  ExrFile e;
+  std::string err;
+  if (!read_exr_header(path, e, err)) {
+    set_error(err);
+    return SHB_ERR_INVALID_ARG;
+  }
+  std::vector<int> want;
+  for (int k = 0; k < n; ++k) {
+    int found = -1;
+    for (size_t c = 0; c < e.names.size(); ++c)
+      if (e.names[c] == names[k]) found = (int)c;
+    if (found < 0) {
+      set_error(std::string("no channel ") + names[k] + " in " + path);
+      return SHB_ERR_INVALID_ARG;
+    }
+    want.push_back(found);
+  }
+  if (width) *width = e.W;
+  if (height) *height = e.H;
+  if (out && !read_exr_channels(e, want, out, err)) {
+    set_error(err);
+    return SHB_ERR_INVALID_ARG;
+  }
+  return SHB_OK;
+}
 
 shb_status save_sh_lightmap_device(shb_context* c, const float* d_sh, const float* d_env, int W, int H,
                                    const std::string& path, int mode) {

@@ -627,6 +627,50 @@ shb_status shb_save_sh_lightmap(shb_context* ctx, const float* sh, const float* 
   return save_sh_lightmap_device(ctx, dsh, denv, width, height, std::string(path), mode);
 }
 
+shb_status shb_sh_preview(shb_context* ctx, const float* sh, int32_t width, int32_t height, const float* normals,
+                          const float direction[3], int32_t mode, int32_t reinhard, int32_t device_ptrs,
+                          uint8_t* rgb_out) {
+  if (!ctx || !sh || !rgb_out) return bad("NULL argument");
+  if (width <= 0 || height <= 0) return bad("empty image");
+  if (mode < SHB_PREVIEW_L0 || mode > SHB_PREVIEW_SH_PACKED) return bad("unknown preview mode");
+  if (mode != SHB_PREVIEW_L0 && !normals && !direction) return bad("a direction or normals is needed");
+  SHB_CUDA(cudaSetDevice(ctx->device));
+  const size_t n = (size_t)width * height;
+  const size_t in_floats = 27 * n + (normals ? 3 * n : 0);
+  SHB_TRY(ctx->scratch[27].reserve(sizeof(float) * in_floats + 3 * n));
+  float* d_in = ctx->scratch[27].as<float>();
+  uint8_t* d_out = reinterpret_cast<uint8_t*>(d_in + in_floats);
+  const float* dsh = sh;
+  const float* dn = normals;
+  if (!device_ptrs) {
+    SHB_CUDA(cudaMemcpyAsync(d_in, sh, sizeof(float) * 27 * n, cudaMemcpyHostToDevice, ctx->stream));
+    dsh = d_in;
+    if (normals) {
+      SHB_CUDA(cudaMemcpyAsync(d_in + 27 * n, normals, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, ctx->stream));
+      dn = d_in + 27 * n;
+    }
+  }
+  const float zero[3] = {0.f, 0.f, 1.f};
+  SHB_TRY(sh_preview_device(ctx, dsh, (int64_t)n, dn, direction ? direction : zero, mode, reinhard, d_out));
+  SHB_CUDA(cudaMemcpyAsync(rgb_out, d_out, 3 * n, cudaMemcpyDeviceToHost, ctx->stream));
+  SHB_CUDA(cudaStreamSynchronize(ctx->stream));
+  return SHB_OK;
+}
+
+shb_status shb_exr_load_channels(const char* path, const char* const* names, int32_t count, int32_t* width,
+                                 int32_t* height, float* out) {
+  if (!path || (count > 0 && !names)) return bad("NULL argument");
+  for (int32_t k = 0; k < count; ++k)
+    if (!names[k]) return bad("NULL channel name");
+  return exr_load_channels(path, names, count, width, height, out);
+}
+
+shb_status shb_write_png(const char* path, int32_t width, int32_t height, int32_t channels, const uint8_t* pixels) {
+  if (!path || !pixels || width <= 0 || height <= 0 || channels < 1 || channels > 4) return bad("bad PNG arguments");
+  if (!write_png(path, width, height, channels, pixels)) return bad(std::string("cannot write ") + path);
+  return SHB_OK;
+}
+
 shb_status shb_scene_set_params(shb_scene* s, const float* albedo_rgb, const uint8_t* use_override,
                                 const float* light_intensity) {
   if (!s) return bad("NULL scene");

@@ -218,6 +218,11 @@ shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n,
 // SaveSHLightMap (exr.cu): device SH (27 f32) and env (f32, nullable) texels.
 shb_status save_sh_lightmap_device(shb_context* c, const float* d_sh, const float* d_env, int W, int H,
                                    const std::string& path, int mode);
+shb_status exr_load_channels(const char* path, const char* const* names, int n, int* width, int* height, float* out);
+// SH previews (preview.cu): d_out = n x 3 bytes (device).
+shb_status sh_preview_device(shb_context* c, const float* d_sh, int64_t n, const float* d_normals, const float dir[3],
+                             int mode, int reinhard, uint8_t* d_out);
+bool write_png(const std::string& path, int w, int h, int channels, const uint8_t* px);
 // Path-replay adjoint of bake_device: grad[3 * mat_count + light_count] (device).
 shb_status backward_device(shb_scene* s, const shb_surface_point* d_pts, int W, int H, const shb_bake_config* cfg,
                            const float* d_dsh, double* d_grad, shb_bake_stats* stats);
