@@ -289,7 +289,8 @@ def run_batched(args):
             "sequential": {"value": seq, "ms_per_step": s_ms / args.steps},
             "speedup_vs_sequential": s_ms / b_ms, "autotuned": {"wave_paths": int(tuned[1]),
                                                                 "tile_texels": int(tuned[2]),
-                                                                "grid_scale": int(tuned[3])},
+                                                                "grid_scale": int(tuned[3]),
+                                                                "share_paths": int(tuned[4])},
             "gpu_launches": int(launches), "clocks": clk}
     print(json.dumps(line), flush=True)
     ctx.close()

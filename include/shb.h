@@ -285,11 +285,15 @@ typedef struct shb_batch_item {
 
 typedef struct shb_batch_options {
   int32_t use_graph;    /* 1: capture the waves in one CUDA graph            */
-  int32_t autotune;     /* 1: pick wave/tile/grid per shape class, cached   */
+  int32_t autotune;     /* 1: pick wave/share/tile/grid per shape class,
+                           cached                                          */
   int32_t wave_paths;   /* paths per wave (0: default or tuned)             */
   int32_t tile_texels;  /* texels per work tile (0: default or tuned)       */
   int32_t grid_scale;   /* traversal grid multiplier (0: default or tuned)  */
-  int32_t reserved[3];
+  int32_t share_paths;  /* bakes of fewer paths share waves with others;
+                           larger ones get waves of their own (0: default
+                           or tuned, which is half a wave; -1: no sharing) */
+  int32_t reserved[2];
   const char* tune_cache; /* tuning file; NULL: $SHB_TUNE_CACHE or
                              $HOME/.cache/sh_baker_b200/autotune.txt        */
 } shb_batch_options;

@@ -1,13 +1,16 @@
 // batch.cu - shb_bake_batch: many bakes in one persistent launch, and the
 // autotuner that picks its launch structure per shape class.
 //
-// The tuned parameters are the queue depth (paths per wave), the work-tile
-// size (texels per tile) and the traversal grid (a multiple of SMs x
-// resident blocks).  A shape class is (bake count, total paths, max bounces,
-// mean triangles, max lights), each bucketed by powers of two.  Tuning runs
-// every candidate on a prefix of the batch, times it with CUDA events, keeps
-// the fastest per path, and appends "<gpu>|<class> wave tile grid ms" to the
-// tuning file so later batches of the same class skip the search.
+// The tuned parameters are the queue depth (paths per wave), the size below
+// which bakes share waves (larger bakes get waves of their own), the
+// work-tile size (texels per tile) and the traversal grid (a multiple of
+// SMs x resident blocks).  A shape class is (bake count, total paths, max
+// bounces, mean triangles, max lights), each bucketed by powers of two.
+// Tuning is a coordinate descent over those four parameters, each candidate
+// timed with CUDA events on the whole batch (sample counts thinned evenly
+// when the batch holds more than 2^30 paths); the fastest per path is
+// appended as "<gpu>|v2|<class> wave tile grid share ms" to the tuning file so
+// later batches of the same class skip the search.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
@@ -68,14 +71,15 @@ bool lookup(const std::string& file, const std::string& key, BatchParams* out) {
   while (std::getline(in, line)) {
     std::istringstream is(line);
     std::string k;
-    long long wave = 0, tile = 0;
+    long long wave = 0, tile = 0, share = 0;
     int grid = 0;
     double ms = 0;
-    if (!(is >> k >> wave >> tile >> grid >> ms)) continue;
-    if (k == key && wave > 0 && tile > 0 && grid > 0) {
+    if (!(is >> k >> wave >> tile >> grid >> share >> ms)) continue;
+    if (k == key && wave > 0 && tile > 0 && grid > 0 && share >= 0) {
       out->wave_paths = wave;
       out->tile_texels = tile;
       out->grid_scale = grid;
+      out->share_paths = share;
       found = true;  // the last entry wins
     }
   }
@@ -98,47 +102,65 @@ shb_status time_batch(shb_context* c, const std::vector<BakeSpec>& specs, const 
   return st;
 }
 
-// Tries every candidate on a prefix of the batch of about 2^24 paths.
+// Coordinate descent from the defaults: queue depth, then the sharing
+// threshold, then the tile size, then the traversal grid, keeping the best
+// of each sweep.  The probe is the whole batch, with every bake's sample
+// count scaled by the same factor when the batch holds more than 2^30 paths.
 shb_status tune(shb_context* c, const std::vector<BakeSpec>& specs, BatchParams* best, double* best_cost) {
-  std::vector<BakeSpec> probe;
+  std::vector<BakeSpec> probe = specs;
   double paths = 0;
-  for (const BakeSpec& s : specs) {
-    probe.push_back(s);
-    paths += (double)s.W * s.H * s.cfg.samples;
-    if (paths >= double(1 << 24)) break;
-  }
-  if (paths > double(1 << 25)) {  // one huge bake: probe it at fewer samples
-    double f = double(1 << 24) / paths;
+  for (const BakeSpec& s : probe) paths += (double)s.W * s.H * s.cfg.samples;
+  if (paths > double(1 << 30)) {
+    const double f = double(1 << 30) / paths;
     paths = 0;
     for (BakeSpec& s : probe) {
       s.cfg.samples = std::max(1, (int)(s.cfg.samples * f));
       paths += (double)s.W * s.H * s.cfg.samples;
     }
   }
-  const int64_t waves[] = {int64_t(1) << 21, int64_t(1) << 22, int64_t(1) << 23, int64_t(1) << 24};
-  const int64_t tiles[] = {int64_t(1) << 10, int64_t(1) << 13, int64_t(1) << 30};
-  const int grids[] = {1, 2};
+  BatchParams cur;
+  cur.tile_texels = int64_t(1) << 13;
+  double ms = 0;
+  {  // the first run pays allocation of the largest wave buffers
+    BatchParams w = cur;
+    w.wave_paths = int64_t(1) << 24;
+    SHB_TRY(time_batch(c, probe, w, &ms));
+  }
   *best_cost = 1e300;
-  bool warmed = false;
-  for (int64_t w : waves)
-    for (int64_t t : tiles)
-      for (int g : grids) {
-        BatchParams p;
-        p.wave_paths = w;
-        p.tile_texels = t;
-        p.grid_scale = g;
-        double ms = 0;
-        if (!warmed) {  // first run pays allocation of the wave buffers
-          SHB_TRY(time_batch(c, probe, p, &ms));
-          warmed = true;
-        }
-        SHB_TRY(time_batch(c, probe, p, &ms));
-        double cost = ms / std::max(paths, 1.0) * 1e6;  // ms per million paths
-        if (cost < *best_cost) {
-          *best_cost = cost;
-          *best = p;
-        }
-      }
+  auto trial = [&](const BatchParams& p) -> shb_status {
+    SHB_TRY(time_batch(c, probe, p, &ms));
+    const double cost = ms / std::max(paths, 1.0) * 1e6;  // ms per million paths
+    if (cost < *best_cost) {
+      *best_cost = cost;
+      *best = p;
+    }
+    return SHB_OK;
+  };
+  SHB_TRY(trial(cur));
+  for (int64_t w : {int64_t(1) << 22, int64_t(1) << 24}) {
+    BatchParams p = cur;
+    p.wave_paths = w;
+    SHB_TRY(trial(p));
+  }
+  cur = *best;
+  for (int64_t sh : {int64_t(0), cur.wave_paths / 8, int64_t(1) << 40}) {
+    BatchParams p = cur;
+    p.share_paths = sh;
+    SHB_TRY(trial(p));
+  }
+  cur = *best;
+  {
+    BatchParams p = cur;
+    p.tile_texels = int64_t(1) << 30;
+    SHB_TRY(trial(p));
+  }
+  cur = *best;
+  {
+    BatchParams p = cur;
+    p.grid_scale = 2;
+    SHB_TRY(trial(p));
+  }
+  if (best->share_paths < 0) best->share_paths = best->wave_paths / 2;
   return SHB_OK;
 }
 
@@ -194,7 +216,7 @@ extern "C" shb_status shb_bake_batch(shb_context* ctx, const shb_batch_item* ite
   prm.tile_texels = int64_t(1) << 13;
   if (options && options->autotune) {
     const std::string file = tune_path(options->tune_cache);
-    const std::string key = device_name(ctx->device) + "|" + shape_class(specs);
+    const std::string key = device_name(ctx->device) + "|v2|" + shape_class(specs);
     if (!lookup(file, key, &prm)) {
       double cost = 0;
       BatchParams best;
@@ -202,13 +224,17 @@ extern "C" shb_status shb_bake_batch(shb_context* ctx, const shb_batch_item* ite
       prm.wave_paths = best.wave_paths;
       prm.tile_texels = best.tile_texels;
       prm.grid_scale = best.grid_scale;
+      prm.share_paths = best.share_paths;
       std::ofstream out(file, std::ios::app);
-      out << key << " " << prm.wave_paths << " " << prm.tile_texels << " " << prm.grid_scale << " " << cost << "\n";
+      out << key << " " << prm.wave_paths << " " << prm.tile_texels << " " << prm.grid_scale << " "
+          << prm.share_paths << " " << cost << "\n";
     }
   }
   if (options && options->wave_paths > 0) prm.wave_paths = options->wave_paths;
   if (options && options->tile_texels > 0) prm.tile_texels = options->tile_texels;
   if (options && options->grid_scale > 0) prm.grid_scale = options->grid_scale;
+  if (options && options->share_paths > 0) prm.share_paths = options->share_paths;
+  if (options && options->share_paths < 0) prm.share_paths = 0;
   uint64_t l0 = ctx->launches;
   SHB_TRY(bake_batch_device(ctx, specs, prm, stats));
   if (stats) stats->kernel_launches = ctx->launches - l0;

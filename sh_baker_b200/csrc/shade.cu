@@ -1064,26 +1064,30 @@ struct Wave {
   int tile_begin, n_tiles;
   int64_t P, n_tex;
   int max_bounces;
+  int bake;  // the one bake whose tiles fill the wave, else -1
 };
 
 // Splits every bake's valid texels into tiles of whole texels (all their
-// samples) and packs consecutive tiles into waves of at most `wave_paths`
-// paths.
+// samples) and packs tiles into waves of at most `wave_paths` paths.  A bake
+// of at least `share_paths` paths gets waves of its own, split evenly (no
+// short last wave), so that traversal runs with that bake's BVH bound for
+// the whole launch; smaller bakes share waves in their order.
 void plan_waves(const std::vector<BakeSpec>& specs, const std::vector<int>& n_valid, int64_t wave_paths,
-                int64_t tile_texels, std::vector<Tile>& tiles, std::vector<Wave>& waves) {
+                int64_t tile_texels, int64_t share_paths, std::vector<Tile>& tiles, std::vector<Wave>& waves) {
   tiles.clear();
   waves.clear();
-  Wave cur{0, 0, 0, 0, 0};
-  for (size_t b = 0; b < specs.size(); ++b) {
+  Wave cur{0, 0, 0, 0, 0, -1};
+  auto flush = [&] {
+    if (cur.n_tiles > 0) waves.push_back(cur);
+    cur = Wave{(int)tiles.size(), 0, 0, 0, 0, -1};
+  };
+  auto add = [&](size_t b, int64_t cap) {
     const int64_t spp = specs[b].cfg.samples;
-    int64_t per_tile = std::max<int64_t>(1, std::min<int64_t>(tile_texels, wave_paths / spp));
+    const int64_t per_tile = std::max<int64_t>(1, std::min<int64_t>(tile_texels, cap / spp));
     for (int64_t t0 = 0; t0 < n_valid[b]; t0 += per_tile) {
-      int64_t nt = std::min<int64_t>(per_tile, n_valid[b] - t0);
-      int64_t paths = nt * spp;
-      if (cur.n_tiles > 0 && cur.P + paths > wave_paths) {
-        waves.push_back(cur);
-        cur = Wave{(int)tiles.size(), 0, 0, 0, 0};
-      }
+      const int64_t nt = std::min<int64_t>(per_tile, n_valid[b] - t0);
+      const int64_t paths = nt * spp;
+      if (cur.n_tiles > 0 && cur.P + paths > cap) flush();
       Tile t;
       t.bake = (uint32_t)b;
       t.t0 = (uint32_t)t0;
@@ -1092,13 +1096,25 @@ void plan_waves(const std::vector<BakeSpec>& specs, const std::vector<int>& n_va
       t.path_off = cur.P;
       t.tex_off = cur.n_tex;
       tiles.push_back(t);
+      cur.bake = (cur.n_tiles == 0 || cur.bake == (int)b) ? (int)b : -1;
       cur.n_tiles++;
       cur.P += paths;
       cur.n_tex += nt;
       cur.max_bounces = std::max(cur.max_bounces, specs[b].cfg.bounces);
     }
+  };
+  for (size_t b = 0; b < specs.size(); ++b) {
+    const int64_t spp = specs[b].cfg.samples, paths = n_valid[b] * spp;
+    if (paths == 0 || paths < share_paths) continue;
+    flush();
+    const int64_t n_w = (paths + wave_paths - 1) / wave_paths;
+    const int64_t tex = (n_valid[b] + n_w - 1) / n_w;
+    add(b, std::min(wave_paths, tex * spp));
+    flush();
   }
-  if (cur.n_tiles > 0) waves.push_back(cur);
+  for (size_t b = 0; b < specs.size(); ++b)
+    if ((int64_t)n_valid[b] * specs[b].cfg.samples < share_paths) add(b, wave_paths);
+  flush();
 }
 
 }  // namespace
@@ -1197,7 +1213,8 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   const int slots = (int)mult;
   std::vector<Tile> tiles;
   std::vector<Wave> waves;
-  plan_waves(specs, n_valid, wave_paths, prm.tile_texels, tiles, waves);
+  const int64_t share = prm.share_paths < 0 ? wave_paths / 2 : prm.share_paths;
+  plan_waves(specs, n_valid, wave_paths, prm.tile_texels, share, tiles, waves);
   int64_t Pmax = 0;
   for (const Wave& w : waves) Pmax = std::max(Pmax, w.P);
   const int64_t ext_cap = std::max<int64_t>(Pmax * mult, 1);
@@ -1302,6 +1319,9 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
     a.n_tiles = w.n_tiles;
     a.P = w.P;
     a.n_tex = w.n_tex;
+    // traversal of a one-bake wave skips the per-ray bake lookup
+    const BakeItem* bk = w.bake >= 0 ? d_items + w.bake : d_items;
+    const int nbk = w.bake >= 0 ? 1 : nb;
     cudaMemsetAsync(cnt, 0, sizeof(int) * (CNT_FETCH_SHADOW + 1), st);
     Pair pg = stamp(2);
     if (bwd) k_generate<true><<<grid_for(w.P), kThreads, 0, st>>>(a);
@@ -1313,7 +1333,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       cudaMemsetAsync(cnt + nxt, 0, sizeof(int), st);
       cudaMemsetAsync(cnt + CNT_FETCH_EXT, 0, sizeof(int) * 2, st);
       Pair pe = stamp(0);
-      launch_extend(st, tgrid, d_items, nb, a.info, a.ext[cur], cnt + cur, a.ext_cap, a.hits, cnt + CNT_FETCH_EXT,
+      launch_extend(st, tgrid, bk, nbk, a.info, a.ext[cur], cnt + cur, a.ext_cap, a.hits, cnt + CNT_FETCH_EXT,
                     cnt + CNT_ERROR, c64);
       close_stamp(pe);
       Pair pd = stamp(2);
@@ -1321,7 +1341,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       else k_shade<false><<<sgrid, kThreads, 0, st>>>(a, cur, k);
       close_stamp(pd);
       Pair ps = stamp(1);
-      launch_shadow(st, tgrid, d_items, nb, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, a.pend,
+      launch_shadow(st, tgrid, bk, nbk, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, a.pend,
                     cnt + CNT_FETCH_SHADOW, cnt + CNT_ERROR, c64);
       close_stamp(ps);
       if (bwd) {

@@ -204,6 +204,7 @@ struct BatchParams {
   int64_t wave_paths = int64_t(1) << 23;  // paths in flight per wave (queue depth)
   int64_t tile_texels = int64_t(1) << 30; // texels per work tile
   int grid_scale = 1;                     // traversal grid = grid_scale x SMs x occupancy
+  int64_t share_paths = -1;               // bakes of fewer paths share waves (-1: wave_paths / 2)
   bool use_graph = false;                 // capture the waves in one CUDA graph
   // Path-replay adjoint instead of the forward bake (one bake): gradients of
   // sum(dsh * SH) accumulate into grad[3 * mat_count + light_count] (device,

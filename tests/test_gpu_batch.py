@@ -47,12 +47,16 @@ def plain(bakes):
     return outs
 
 
-@pytest.mark.parametrize("use_graph,tile", [(False, 0), (True, 0), (True, 7), (False, 100)])
-def test_batch_equals_plain(gpu_ctx, use_graph, tile):
+@pytest.mark.parametrize("use_graph,tile,share", [(False, 0, 0), (True, 0, 0), (True, 7, 0), (False, 100, 0),
+                                                  (False, 0, -1), (True, 7, 2**31 - 1), (True, 0, 3000)])
+def test_batch_equals_plain(gpu_ctx, use_graph, tile, share):
+    """share: 0 = bakes under half a wave share waves; -1 = every bake has
+    waves of its own (one-bake traversal); 2^31-1 = all bakes share."""
     bakes = make_batch(gpu_ctx)
     ref = plain(bakes)
-    outs, st = api.bake_batch(gpu_ctx, bakes, use_graph=use_graph, tile_texels=tile, wave_paths=1 << 14)
-    assert st.error_flags == 0 and st.waves >= 2
+    outs, st = api.bake_batch(gpu_ctx, bakes, use_graph=use_graph, tile_texels=tile, wave_paths=1 << 14,
+                              share_paths=share)
+    assert st.error_flags == 0 and st.waves >= (len(bakes) if share == -1 else 2)
     for (sh, env), (rsh, renv) in zip(outs, ref):
         assert sh.cpu().numpy().tobytes() == rsh.tobytes()
         assert env.cpu().numpy().tobytes() == renv.tobytes()
@@ -65,8 +69,8 @@ def test_autotune_persists_per_shape_class(gpu_ctx, tmp_path):
     outs, _ = api.bake_batch(gpu_ctx, bakes, autotune=True, tune_cache=str(cache))
     lines = cache.read_text().splitlines()
     assert len(lines) == 1
-    key, wave, tile, grid, cost = lines[0].split()
-    assert int(wave) > 0 and int(tile) > 0 and int(grid) >= 1 and float(cost) > 0
+    key, wave, tile, grid, share, cost = lines[0].split()
+    assert int(wave) > 0 and int(tile) > 0 and int(grid) >= 1 and int(share) >= 0 and float(cost) > 0
     outs2, _ = api.bake_batch(gpu_ctx, bakes, autotune=True, tune_cache=str(cache))
     assert cache.read_text().splitlines() == lines  # second batch reads the entry
     for (sh, env), (sh2, env2), (rsh, renv) in zip(outs, outs2, ref):
