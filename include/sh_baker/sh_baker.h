@@ -11,6 +11,7 @@
 //   DownsampleEnvironmentVisibilityTexture                  (src/baker.h:25-36)
 //   Dilate<T> for SHCoeffs, float, uint8_t                  (src/dilation.h:14-16)
 //   SaveMode, SaveSHLightMap                                (src/saver.h:21-48)
+//   CreateAtlasGeometries, atlas_internal::CalculateGeometryScales (src/atlas.h:10-53)
 // Where the reference CHECK-fails these throw sh_baker::Error.  With Eigen
 // available the vector types are Eigen's; otherwise small POD stand-ins with
 // the same memory layout and accessors are used.
@@ -209,8 +210,17 @@ struct SceneHandle {
   ~SceneHandle() { shb_scene_destroy(s); }
 };
 
-inline void upload(const Scene& scene, SceneHandle* out) {
-  std::vector<shb_geometry_desc> g(scene.geometries.size());
+// A shb_scene_desc pointing into `scene` and the arrays below.
+struct Desc {
+  std::vector<shb_geometry_desc> g;
+  std::vector<shb_material_desc> m;
+  std::vector<shb_light_desc> l;
+  shb_scene_desc d{};
+};
+
+inline void describe(const Scene& scene, Desc* out) {
+  std::vector<shb_geometry_desc>& g = out->g;
+  g.assign(scene.geometries.size(), shb_geometry_desc{});
   for (size_t i = 0; i < g.size(); ++i) {
     const Geometry& G = scene.geometries[i];
     shb_geometry_desc& d = g[i];
@@ -226,7 +236,8 @@ inline void upload(const Scene& scene, SceneHandle* out) {
     d.material_id = G.material_id;
     affine_rows(G.transform, d.transform);
   }
-  std::vector<shb_material_desc> m(scene.materials.size());
+  std::vector<shb_material_desc>& m = out->m;
+  m.assign(scene.materials.size(), shb_material_desc{});
   for (size_t i = 0; i < m.size(); ++i) {
     const Material& M = scene.materials[i];
     m[i].albedo_pixels = M.albedo.pixel_data.empty() ? nullptr : M.albedo.pixel_data.data();
@@ -235,7 +246,8 @@ inline void upload(const Scene& scene, SceneHandle* out) {
     m[i].albedo_channels = M.albedo.channels;
     m[i].emission_intensity = M.emission_intensity;
   }
-  std::vector<shb_light_desc> l(scene.lights.size());
+  std::vector<shb_light_desc>& l = out->l;
+  l.assign(scene.lights.size(), shb_light_desc{});
   for (size_t i = 0; i < l.size(); ++i) {
     const Light& L = scene.lights[i];
     shb_light_desc& d = l[i];
@@ -253,11 +265,85 @@ inline void upload(const Scene& scene, SceneHandle* out) {
     if (d.geometry_index < 0 && L.geometry) d.geometry_index = (int32_t)(L.geometry - scene.geometries.data());
     d.material_index = L.material ? (int32_t)(L.material - scene.materials.data()) : -1;
   }
-  shb_scene_desc desc{g.data(), (uint32_t)g.size(), m.data(), (uint32_t)m.size(), l.data(), (uint32_t)l.size()};
-  check(shb_scene_upload(context(), &desc, &out->s));
+  out->d = shb_scene_desc{g.data(), (uint32_t)g.size(), m.data(), (uint32_t)m.size(), l.data(), (uint32_t)l.size()};
+}
+
+inline void upload(const Scene& scene, SceneHandle* out) {
+  Desc D;
+  describe(scene, &D);
+  check(shb_scene_upload(context(), &D.d, &out->s));
 }
 
 }  // namespace detail
+
+// ---- src/atlas.h:10-53 -----------------------------------------------------
+
+namespace atlas_internal {
+
+// Per geometry: density * sqrt(albedo w*h) * sqrt(UV tile count), clamped
+// to 5x the median (shb_atlas_geometry_scales).
+inline std::vector<float> CalculateGeometryScales(const std::vector<Geometry>& geometries,
+                                                  const std::vector<Material>& materials, float density_multiplier) {
+  std::vector<shb_geometry_desc> g(geometries.size(), shb_geometry_desc{});
+  for (size_t i = 0; i < g.size(); ++i) {
+    g[i].texture_uvs = geometries[i].texture_uvs.empty()
+                           ? nullptr
+                           : reinterpret_cast<const float*>(geometries[i].texture_uvs.data());
+    g[i].vertex_count = (uint32_t)geometries[i].texture_uvs.size();
+    g[i].material_id = geometries[i].material_id;
+  }
+  std::vector<shb_material_desc> m(materials.size(), shb_material_desc{});
+  for (size_t i = 0; i < m.size(); ++i) {
+    m[i].albedo_width = materials[i].albedo.width;
+    m[i].albedo_height = materials[i].albedo.height;
+  }
+  shb_scene_desc d{g.data(), (uint32_t)g.size(), m.data(), (uint32_t)m.size(), nullptr, 0};
+  std::vector<float> out(geometries.size());
+  check(shb_atlas_geometry_scales(&d, density_multiplier, out.data()));
+  return out;
+}
+
+}  // namespace atlas_internal
+
+struct AtlasResult {
+  std::vector<Geometry> geometries;
+  int width;
+  int height;
+};
+
+// New geometries with non-overlapping lightmap UVs (shb_create_atlas);
+// nullopt when the charts do not fit one page, like the reference.
+inline std::optional<AtlasResult> CreateAtlasGeometries(const Scene& scene, unsigned target_resolution,
+                                                        unsigned padding, float density_multiplier = 1.0f) {
+  detail::Desc D;
+  detail::describe(scene, &D);
+  shb_host_scene* hs = nullptr;
+  int32_t w = 0, h = 0;
+  if (shb_create_atlas(&D.d, target_resolution, padding, density_multiplier, &hs, &w, &h) != SHB_OK)
+    return std::nullopt;
+  const shb_scene_desc* out = shb_host_scene_desc(hs);
+  AtlasResult r;
+  r.width = w;
+  r.height = h;
+  for (uint32_t i = 0; i < out->geometry_count; ++i) {
+    const shb_geometry_desc& d = out->geometries[i];
+    Geometry G;
+    G.material_id = d.material_id;
+    G.transform = scene.geometries[i].transform;
+    for (uint32_t v = 0; v < d.vertex_count; ++v) {
+      G.vertices.push_back(Vector3f(d.vertices[3 * v], d.vertices[3 * v + 1], d.vertices[3 * v + 2]));
+      G.normals.push_back(Vector3f(d.normals[3 * v], d.normals[3 * v + 1], d.normals[3 * v + 2]));
+      G.texture_uvs.push_back(Vector2f(d.texture_uvs[2 * v], d.texture_uvs[2 * v + 1]));
+      G.lightmap_uvs.push_back(Vector2f(d.lightmap_uvs[2 * v], d.lightmap_uvs[2 * v + 1]));
+      G.tangents.push_back(
+          Vector4f(d.tangents[4 * v], d.tangents[4 * v + 1], d.tangents[4 * v + 2], d.tangents[4 * v + 3]));
+    }
+    G.indices.assign(d.indices, d.indices + d.index_count);
+    r.geometries.push_back(std::move(G));
+  }
+  shb_host_scene_destroy(hs);
+  return r;
+}
 
 // ---- src/rasterizer.h:27-39 ------------------------------------------------
 

@@ -459,6 +459,31 @@ SHB_API shb_status shb_host_scene_material_info(const shb_host_scene* scene, int
 SHB_API shb_status shb_save_gltf(const shb_scene_desc* scene, const char* const* material_names,
                                  const char* const* albedo_files, const char* path);
 
+/* ---- CreateAtlasGeometries (src/atlas.h:28-53, src/atlas.cpp:95-250) --- */
+
+/* atlas_internal::CalculateGeometryScales (src/atlas.h:22-24,
+ * src/atlas.cpp:21-93): per geometry density * sqrt(albedo w*h) *
+ * sqrt(texture-UV tile count), clamped to 5x the median.  scales_out holds
+ * geometry_count floats.  A geometry without texture UVs or with a
+ * material_id out of range is SHB_ERR_INVALID_ARG (the reference CHECKs). */
+SHB_API shb_status shb_atlas_geometry_scales(const shb_scene_desc* scene, float density_multiplier,
+                                             float* scales_out);
+
+/* New lightmap UVs for every geometry, non-overlapping, in one page of
+ * target_resolution^2 texels with at least `padding` empty texels between
+ * charts.  Vertices on chart seams are split; each output vertex keeps the
+ * position, normal, tangent and texture UV of its source vertex; faces keep
+ * their order.  The result (geometries, copied materials and lights) is a
+ * host scene owned by *out; width and height receive the page size.
+ * Charts that cannot fit the page, an empty scene, or geometries without
+ * texture UVs, normals or tangents are SHB_ERR_INVALID_ARG (the reference
+ * returns nullopt or CHECKs).  xatlas is not used: the charts are built by
+ * this library, so UVs differ from the reference's while keeping its
+ * contract. */
+SHB_API shb_status shb_create_atlas(const shb_scene_desc* scene, uint32_t target_resolution, uint32_t padding,
+                                    float density_multiplier, shb_host_scene** out, int32_t* width,
+                                    int32_t* height);
+
 /* ---- FindOcclusion (src/occlusion.cpp:9-107), batched ----------------- */
 
 SHB_API shb_status shb_find_occlusion(shb_scene* scene, const shb_ray* rays,

@@ -162,6 +162,9 @@ SIGNATURES = {
     "shb_host_scene_destroy": (C.c_int, [vp]),
     "shb_host_scene_material_info": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p)]),
     "shb_save_gltf": (C.c_int, [C.POINTER(SceneDesc), vp, vp, C.c_char_p]),
+    "shb_atlas_geometry_scales": (C.c_int, [C.POINTER(SceneDesc), C.c_float, vp]),
+    "shb_create_atlas": (C.c_int, [C.POINTER(SceneDesc), C.c_uint32, C.c_uint32, C.c_float, C.POINTER(vp),
+                                   C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "shb_sh_preview": (C.c_int, [vp, vp, C.c_int32, C.c_int32, vp, vp, C.c_int32, C.c_int32, C.c_int32, vp]),
     "shb_exr_load_channels": (C.c_int, [C.c_char_p, vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                         vp]),

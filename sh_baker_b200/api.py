@@ -5,7 +5,8 @@ RasterizeScene (src/rasterizer.h:27-28), CreateValidityMask /
 DownsampleValidityMask (src/rasterizer.h:31-39), BakeSHLightMap
 (src/baker.h:25-28), DownsampleSHTexture /
 DownsampleEnvironmentVisibilityTexture (src/baker.h:31-36), Dilate
-(src/dilation.h:14-16) and FindOcclusion (src/occlusion.h:27).  Where the
+(src/dilation.h:14-16), FindOcclusion (src/occlusion.h:27) and
+CreateAtlasGeometries / CalculateGeometryScales (src/atlas.h).  Where the
 reference aborts (CHECK) these raise ShbError.  All compute runs in
 libshb.so on the GPU.
 """
@@ -417,6 +418,65 @@ def LoadScene(path, error: Optional[list] = None) -> Optional[Scene]:
         return unpack_scene(lib.shb_host_scene_desc(h).contents)
     finally:
         lib.shb_host_scene_destroy(h)
+
+
+@dataclass
+class AtlasResult:
+    """src/atlas.h:26-35: atlas geometries and the page size."""
+    geometries: list
+    width: int
+    height: int
+
+
+def CalculateGeometryScales(geometries, materials, density_multiplier: float) -> np.ndarray:
+    """atlas_internal::CalculateGeometryScales (src/atlas.cpp:21-93) through
+    shb_atlas_geometry_scales.  Only texture_uvs, material_id and the
+    materials' albedo sizes are read, so geometries may carry nothing else
+    (as in the reference's tests).  Raises ShbError where the reference
+    CHECKs (no texture UVs, material out of range)."""
+    from .scene import _f32, _ptr
+    lib = A.load()
+    keep = []
+    geos = (A.GeometryDesc * max(1, len(geometries)))()
+    for i, g in enumerate(geometries):
+        uv = _f32(g.texture_uvs, 2)
+        keep.append(uv)
+        geos[i].texture_uvs = _ptr(uv, C.c_float)
+        geos[i].vertex_count = 0 if uv is None else len(uv)
+        geos[i].material_id = int(g.material_id)
+    mats = (A.MaterialDesc * max(1, len(materials)))()
+    for i, m in enumerate(materials):
+        mats[i].albedo_width = m.albedo.width
+        mats[i].albedo_height = m.albedo.height
+    desc = A.SceneDesc(geos, len(geometries), mats, len(materials), None, 0)
+    out = np.zeros(max(1, len(geometries)), np.float32)
+    A.check(lib.shb_atlas_geometry_scales(C.byref(desc), float(density_multiplier), out.ctypes.data))
+    return out[:len(geometries)]
+
+
+def CreateAtlasGeometries(scene: Scene, target_resolution: int, padding: int, density_multiplier: float = 1.0,
+                          error: Optional[list] = None) -> Optional[AtlasResult]:
+    """src/atlas.h:49-51 CreateAtlasGeometries through shb_create_atlas (host
+    only): new geometries with non-overlapping lightmap UVs in one page of
+    target_resolution^2 texels, `padding` texels apart.  None when it fails
+    (no geometries, charts that do not fit), like the reference's nullopt;
+    the reason is appended to `error` when given."""
+    from .scene import unpack_scene
+    lib = A.load()
+    desc, keep = pack_scene(scene)
+    h = C.c_void_p()
+    w, hh = C.c_int32(), C.c_int32()
+    st = lib.shb_create_atlas(C.byref(desc), int(target_resolution), int(padding), float(density_multiplier),
+                              C.byref(h), C.byref(w), C.byref(hh))
+    if st != 0:
+        if error is not None:
+            error.append(lib.shb_last_error().decode())
+        return None
+    try:
+        geos = unpack_scene(lib.shb_host_scene_desc(h).contents).geometries
+    finally:
+        lib.shb_host_scene_destroy(h)
+    return AtlasResult(geos, w.value, hh.value)
 
 
 def SaveScene(scene: Scene, path, material_names=None, albedo_files=None) -> bool:

@@ -28,6 +28,7 @@ SOURCES = {
     "batch.cu": ["-fmad=false"],
     "exr.cu": ["-fmad=false"],
     "gltf.cpp": [],
+    "atlas.cpp": [],
     "preview.cu": ["-fmad=false"],
 }
 HEADERS = ["shb_internal.h", "shb_math.cuh", "wavefront.h"]

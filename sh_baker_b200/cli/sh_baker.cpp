@@ -4,10 +4,12 @@
 // --output.  Same flags and defaults as the reference; --seed selects the
 // random stream (the reference always uses the fixed stream 12345 + texel).
 //
-// The reference regenerates lightmap UVs with xatlas (src/main.cpp:71-91)
-// before rasterising.  xatlas is a third-party library that is not part of
-// this build, so the lightmap UVs are taken from the input (TEXCOORD_1, as
-// SaveScene writes them); a scene without them is an error.
+// Like the reference (src/main.cpp:71-91), the lightmap UVs are generated
+// for every scene before rasterising: shb_create_atlas with --width as the
+// page size, --dilation as the padding and --density_multiplier (the
+// reference uses xatlas; the charts here are built by libshb, so UVs differ
+// while following the same contract).  --keep_lightmap_uvs, not a reference
+// flag, bakes with the input's TEXCOORD_1 instead.
 #include <sys/stat.h>
 
 #include <chrono>
@@ -25,7 +27,7 @@ namespace {
 struct Flags {
   std::string input, output;
   int width = 2048, height = 2048, samples = 128, bounces = 3, dilation = 16, supersample_scale = 1;
-  bool split_channels = false, luminance_only = false, debug_output = false;
+  bool split_channels = false, luminance_only = false, debug_output = false, keep_lightmap_uvs = false;
   double density_multiplier = 1.0;
   long long seed = 12345;
 };
@@ -44,7 +46,8 @@ bool parse(int argc, char** argv, Flags& f) {
                                       {"samples", &f.samples},   {"bounces", &f.bounces},
                                       {"dilation", &f.dilation}, {"supersample_scale", &f.supersample_scale}};
   std::map<std::string, bool*> bools = {
-      {"split_channels", &f.split_channels}, {"luminance_only", &f.luminance_only}, {"debug_output", &f.debug_output}};
+      {"split_channels", &f.split_channels}, {"luminance_only", &f.luminance_only}, {"debug_output", &f.debug_output},
+      {"keep_lightmap_uvs", &f.keep_lightmap_uvs}};
   for (int i = 1; i < argc; ++i) {
     std::string a = argv[i];
     if (a.size() < 2 || a[0] != '-') {
@@ -173,11 +176,20 @@ int main(int argc, char** argv) {
   log("Scene loaded successfully.  Geometries: " + std::to_string(desc->geometry_count) +
       "  Materials: " + std::to_string(desc->material_count) + "  Lights: " + std::to_string(desc->light_count));
   if (desc->geometry_count == 0) return fail("No geometries found in scene.");
-  for (uint32_t g = 0; g < desc->geometry_count; ++g)
-    if (!desc->geometries[g].lightmap_uvs)
-      return fail("geometry " + std::to_string(g) +
-                  " has no lightmap UVs (TEXCOORD_1); generating them needs xatlas, which this build does not have");
-  if (F.density_multiplier != 1.0) log("--density_multiplier only scales xatlas charts; ignored");
+  shb_host_scene* atlas = nullptr;
+  if (F.keep_lightmap_uvs) {
+    for (uint32_t g = 0; g < desc->geometry_count; ++g)
+      if (!desc->geometries[g].lightmap_uvs)
+        return fail("geometry " + std::to_string(g) + " has no lightmap UVs (TEXCOORD_1) to keep");
+  } else {
+    log("Generating Lightmap UVs...");
+    int32_t aw = 0, ah = 0;
+    if (shb_create_atlas(desc, (uint32_t)F.width, (uint32_t)F.dilation, (float)F.density_multiplier, &atlas, &aw,
+                         &ah) != SHB_OK)
+      return fail(std::string("Atlas generation failed (possibly could not fit charts): ") + shb_last_error());
+    desc = shb_host_scene_desc(atlas);
+    log("Atlas generation complete.  Resolution: " + std::to_string(aw) + "x" + std::to_string(ah));
+  }
 
   shb_options o{};
   const char* dev = std::getenv("SHB_DEVICE");
@@ -230,6 +242,7 @@ int main(int argc, char** argv) {
   }
   shb_scene_destroy(scene);
   shb_context_destroy(ctx);
+  shb_host_scene_destroy(atlas);
   shb_host_scene_destroy(hs);
   return 0;
 }

@@ -38,29 +38,8 @@
 #include <string>
 #include <vector>
 
+#include "host_scene.h"
 #include "shb_internal.h"
-
-struct shb_host_scene {
-  struct Geo {
-    std::vector<float> v, n, uv0, uv1, t;
-    std::vector<uint32_t> idx;
-    int material = -1;
-    float transform[12];
-  };
-  struct Mat {
-    std::vector<uint8_t> px;
-    uint32_t w = 0, h = 0, c = 0;
-    float emission = 0.f;
-    std::string name;
-    std::string albedo_file;  // absolute path of an external albedo image
-  };
-  std::vector<Geo> geos;
-  std::vector<Mat> mats;
-  std::vector<shb_light_desc> lights;
-  std::vector<shb_geometry_desc> gd;
-  std::vector<shb_material_desc> md;
-  shb_scene_desc desc{};
-};
 
 namespace shb {
 namespace {
@@ -1221,31 +1200,7 @@ shb_status shb_load_gltf(const char* path, shb_host_scene** out) {
     shb::set_error("LoadScene: " + L.err);
     return SHB_ERR_INVALID_ARG;
   }
-  for (auto& g : s->geos) {
-    shb_geometry_desc d{};
-    d.vertices = g.v.data();
-    d.normals = g.n.empty() ? nullptr : g.n.data();
-    d.texture_uvs = g.uv0.empty() ? nullptr : g.uv0.data();
-    d.lightmap_uvs = g.uv1.empty() ? nullptr : g.uv1.data();
-    d.tangents = g.t.empty() ? nullptr : g.t.data();
-    d.vertex_count = (uint32_t)(g.v.size() / 3);
-    d.indices = g.idx.data();
-    d.index_count = (uint32_t)g.idx.size();
-    d.material_id = g.material;
-    std::memcpy(d.transform, g.transform, sizeof(d.transform));
-    s->gd.push_back(d);
-  }
-  for (auto& mt : s->mats) {
-    shb_material_desc d{};
-    d.albedo_pixels = mt.px.empty() ? nullptr : mt.px.data();
-    d.albedo_width = mt.w;
-    d.albedo_height = mt.h;
-    d.albedo_channels = mt.c;
-    d.emission_intensity = mt.emission;
-    s->md.push_back(d);
-  }
-  s->desc = shb_scene_desc{s->gd.data(), (uint32_t)s->gd.size(), s->md.data(), (uint32_t)s->md.size(),
-                           s->lights.data(), (uint32_t)s->lights.size()};
+  s->finish();
   *out = s.release();
   return SHB_OK;
 }

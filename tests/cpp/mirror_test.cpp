@@ -1,11 +1,13 @@
 // The reference's own unit tests, restated against the C++ mirror
 // (include/sh_baker/sh_baker.h) so they run on the CUDA library:
 //   src/rasterizer_test.cpp:7-126, src/dilation_test.cpp:11-58,
-//   src/baker_test.cpp:10-88.
-// Exit status 0 when every check passes.
+//   src/baker_test.cpp:10-88, src/atlas_test.cpp:9-170.
+// Exit status 0 when every check passes; with --host only the host-side
+// tests (atlas) run, no GPU needed.
 #include <cmath>
 #include <cstdio>
 #include <filesystem>
+#include <string>
 
 #include "sh_baker/sh_baker.h"
 
@@ -192,8 +194,63 @@ void SaveModes() {
   std::filesystem::remove_all(dir);
 }
 
-int main() {
+// src/atlas_test.cpp:9-65 (SimpleQuad) and :67-170 (geometry scales).
+static void Atlas() {
+  Geometry g;
+  g.vertices = {Vector3f(-1, -1, 0), Vector3f(1, -1, 0), Vector3f(-1, 1, 0), Vector3f(1, 1, 0)};
+  g.normals = {Vector3f(0, 0, 1), Vector3f(0, 0, 1), Vector3f(0, 0, 1), Vector3f(0, 0, 1)};
+  g.tangents = {Vector4f(1, 0, 0, 1), Vector4f(1, 0, 0, 1), Vector4f(1, 0, 0, 1), Vector4f(1, 0, 0, 1)};
+  g.texture_uvs = {Vector2f(0, 0), Vector2f(1, 0), Vector2f(0, 1), Vector2f(1, 1)};
+  g.indices = {0, 1, 2, 2, 1, 3};
+  g.material_id = 0;
+  Scene scene;
+  scene.geometries = {g};
+  Material mat;
+  mat.albedo.width = 256;
+  mat.albedo.height = 256;
+  scene.materials.push_back(mat);
+  std::optional<AtlasResult> r = CreateAtlasGeometries(scene, 256, 2);
+  EXPECT(r.has_value());
+  if (r) {
+    EXPECT(r->width >= 0 && r->height >= 0);
+    EXPECT(r->geometries.size() == 1);
+    const Geometry& o = r->geometries[0];
+    EXPECT(o.lightmap_uvs.size() == o.vertices.size());
+    for (const auto& uv : o.lightmap_uvs) EXPECT(uv.x() >= 0.f && uv.x() <= 1.f && uv.y() >= 0.f && uv.y() <= 1.f);
+    EXPECT(o.indices.size() == g.indices.size());
+    EXPECT(o.vertices.size() >= g.vertices.size());
+  }
+  auto one = [](std::vector<Vector2f> uvs, uint32_t w, float density) {
+    std::vector<Geometry> gs(1);
+    gs[0].material_id = 0;
+    gs[0].texture_uvs = uvs;
+    std::vector<Material> ms(1);
+    ms[0].albedo.width = ms[0].albedo.height = w;
+    return atlas_internal::CalculateGeometryScales(gs, ms, density);
+  };
+  EXPECT(std::fabs(one({Vector2f(0, 0), Vector2f(1, 0), Vector2f(0, 1)}, 100, 1.f)[0] - 100.f) <= 1e-4f);
+  EXPECT(std::fabs(one({Vector2f(0, 0), Vector2f(2, 0), Vector2f(0, 2)}, 10, 1.f)[0] - 20.f) <= 1e-4f);
+  EXPECT(std::fabs(one({Vector2f(0, 0), Vector2f(1, 1)}, 100, 2.f)[0] - 200.f) <= 1e-4f);
+  std::vector<Geometry> gs(3);
+  std::vector<Material> ms(3);
+  for (int i = 0; i < 3; ++i) {
+    gs[i].material_id = i;
+    gs[i].texture_uvs = {Vector2f(0, 0), Vector2f(1, 1)};
+    ms[i].albedo.width = ms[i].albedo.height = i == 2 ? 1000 : 10;
+  }
+  std::vector<float> s = atlas_internal::CalculateGeometryScales(gs, ms, 1.f);
+  EXPECT(s.size() == 3 && std::fabs(s[0] - 10.f) <= 1e-4f && std::fabs(s[1] - 10.f) <= 1e-4f &&
+         std::fabs(s[2] - 50.f) <= 1e-4f);
+}
+
+int main(int argc, char** argv) {
+  const bool host_only = argc > 1 && std::string(argv[1]) == "--host";
   try {
+    Atlas();
+    if (host_only) {
+      std::printf("%s (%d failures)\n", failures ? "FAILED" : "OK", failures);
+      return failures ? 1 : 0;
+    }
     RasterizeQuad();
     Masks();
     Dilation();

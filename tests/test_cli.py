@@ -35,38 +35,74 @@ def test_usage_and_flag_errors(tmp_path):
     assert r.returncode == 1 and "does not exist" in r.stderr
 
 
-def test_scene_without_lightmap_uvs_is_an_error(tmp_path):
+def no_lightmap_uvs_gltf(path):
     sc = scenes.procedural_room(seed=3, n_boxes=4, res=32)
     for g in sc.geometries:
         g.lightmap_uvs = None
-    assert api.SaveScene(sc, tmp_path / "s.gltf")
-    r = run("--input", tmp_path / "s.gltf", "--output", tmp_path / "out")
+    assert api.SaveScene(sc, path)
+    return path
+
+
+def test_keep_lightmap_uvs_needs_them(tmp_path):
+    src = no_lightmap_uvs_gltf(tmp_path / "s.gltf")
+    r = run("--input", src, "--output", tmp_path / "out", "--keep_lightmap_uvs")
     assert r.returncode == 1 and "TEXCOORD_1" in r.stderr
+
+
+def test_atlas_that_cannot_fit_fails(tmp_path):
+    """The atlas runs before any GPU work; 200+ charts cannot fit a 16x16
+    page with 8 texels of padding (src/main.cpp:76-83)."""
+    src = room_gltf(tmp_path / "in.gltf")
+    r = run("--input", src, "--output", tmp_path / "out", "--width", 16, "--height", 16, "--dilation", 8)
+    assert r.returncode == 1 and "Atlas generation failed" in r.stderr
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("flags,files", [([], ["lightmap.exr"]),
                                          (["--luminance_only"], [f"lightmap_packed_{k}.exr" for k in range(3)]),
-                                         (["--split_channels=true"], ["lightmap_L0.exr", "lightmap_L22.exr"])])
+                                         (["--split_channels=true"], ["lightmap_L0.exr", "lightmap_L22.exr"]),
+                                         (["--keep_lightmap_uvs", "--density_multiplier=2"], ["lightmap.exr"])])
 def test_bake_matches_library_pipeline(tmp_path, flags, files):
-    """The CLI's files decode to what LoadScene + the bake pipeline +
-    SaveSHLightMap give for the same scene, config and seed."""
+    """The CLI's files decode to what LoadScene + CreateAtlasGeometries +
+    the bake pipeline + SaveSHLightMap give for the same scene, config and
+    seed; scene.gltf carries the atlas UVs as TEXCOORD_1."""
     src = room_gltf(tmp_path / "in.gltf")
     out = tmp_path / "out"
     r = run("--input", src, "--output", out, "--width", 64, "--height", 64, "--samples", 8, "--bounces", 2,
             "--dilation", 2, "--supersample_scale", 2, "--seed", 7, "--debug_output", *flags)
     assert r.returncode == 0, r.stderr
     assert (out / "scene.gltf").exists() and (out / "scene.bin").exists() and (out / "material_map.png").exists()
-    assert api.LoadScene(out / "scene.gltf") is not None
     sc = api.LoadScene(src)
+    if "--keep_lightmap_uvs" not in flags:
+        atlas = api.CreateAtlasGeometries(sc, 64, 2, 1.0)
+        sc.geometries = atlas.geometries
+    saved = api.LoadScene(out / "scene.gltf")
+    assert saved is not None
+    for a, b in zip(saved.geometries, sc.geometries):
+        np.testing.assert_array_equal(a.lightmap_uvs, b.lightmap_uvs)
     res = api.bake_lightmap(sc, 64, 64, samples=8, bounces=2, supersample_scale=2, dilation=2, seed=7)
     ref = tmp_path / "ref"
     ref.mkdir()
     mode = (api.SaveMode.kLuminancePacked if "--luminance_only" in flags else
-            api.SaveMode.kSplitChannels if flags else api.SaveMode.kCombined)
+            api.SaveMode.kSplitChannels if "--split_channels=true" in flags else api.SaveMode.kCombined)
     assert api.SaveSHLightMap(res.sh, res.env, ref / "lightmap.exr", mode)
     for f in files:
         a, b = exr_read.read(out / f), exr_read.read(ref / f)
         assert a.channels == b.channels
         for name, _ in a.channels:
             np.testing.assert_array_equal(a.raw[name], b.raw[name])
+
+
+@pytest.mark.gpu
+def test_scene_without_lightmap_uvs_bakes(tmp_path):
+    """Like the reference, the CLI makes its own lightmap UVs: a scene with
+    no TEXCOORD_1 bakes and gets them in scene.gltf."""
+    src = no_lightmap_uvs_gltf(tmp_path / "s.gltf")
+    out = tmp_path / "out"
+    r = run("--input", src, "--output", out, "--width", 64, "--height", 64, "--samples", 4, "--bounces", 1,
+            "--dilation", 2)
+    assert r.returncode == 0, r.stderr
+    ex = exr_read.read(out / "lightmap.exr")
+    assert ex.half("L0.R").max() > 0
+    saved = api.LoadScene(out / "scene.gltf")
+    assert all(g.lightmap_uvs is not None for g in saved.geometries)

@@ -20,9 +20,11 @@ def compile_mirror(out: Path) -> Path:
     return out
 
 
-def test_mirror_compiles(tmp_path):
+def test_mirror_compiles_and_runs_host_tests(tmp_path):
+    """Compiles; the host-side tests (atlas) run without a GPU."""
     exe = compile_mirror(tmp_path / "mirror_test")
-    assert exe.exists()
+    r = subprocess.run([str(exe), "--host"], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and "OK (0 failures)" in r.stdout, r.stdout + r.stderr
 
 
 @pytest.mark.gpu
