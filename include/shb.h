@@ -382,7 +382,9 @@ typedef struct shb_pipeline_config {
  * DownsampleValidityMask -> (dilation > 0) Dilate(SH) then Dilate(env) with
  * the mask the first Dilate already updated, all on the device.  Host
  * outputs at width x height: sh (27 floats per texel), env_visibility,
- * mask (nullable). */
+ * mask (nullable).  The supersampled G-buffer and the intermediate
+ * textures stay allocated in the context for the next call (released by
+ * shb_context_destroy). */
 SHB_API shb_status shb_bake_pipeline(shb_scene* scene, const shb_pipeline_config* cfg,
                                      float* sh_out, float* env_out, uint8_t* mask_out,
                                      shb_bake_stats* stats);

@@ -230,6 +230,7 @@ shb_status shb_context_destroy(shb_context* ctx) {
   cudaStreamSynchronize(ctx->stream);
   for (auto& b : ctx->scratch) b.release();
   ctx->counters.release();
+  delete ctx->pipe_gbuf;
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
   return SHB_OK;
@@ -452,31 +453,38 @@ shb_status shb_scene_bvh_info(const shb_scene* s, uint32_t* wide_nodes, uint32_t
   return SHB_OK;
 }
 
-shb_status shb_rasterize(shb_scene* s, const shb_raster_config* cfg, shb_surface_point* host_out,
-                         shb_gbuffer** out_gbuffer) {
-  if (!s || !cfg) return bad("NULL argument");
-  if (out_gbuffer) *out_gbuffer = nullptr;
+namespace {
+
+// Rasterises into g (its storage grows as needed), optionally downloading
+// the points to host_out, and waits for the stream.
+shb_status rasterize_into(shb_scene* s, const shb_raster_config* cfg, shb_gbuffer* g, shb_surface_point* host_out) {
   if (!s->raster_ready) return bad(s->raster_error);
   if (cfg->width <= 0 || cfg->height <= 0 || cfg->supersample_scale <= 0)
     return bad("raster width, height and supersample_scale must be positive");
   int64_t W = (int64_t)cfg->width * cfg->supersample_scale, H = (int64_t)cfg->height * cfg->supersample_scale;
   if (W > 65535 || H > 65535 || W * H > (1ll << 31) - 1) return bad("raster size too large");
   SHB_CUDA(cudaSetDevice(s->ctx->device));
-  auto* g = new shb_gbuffer();
   g->ctx = s->ctx;
   g->width = (int)W;
   g->height = (int)H;
-  shb_status rc = g->points.reserve(sizeof(shb_surface_point) * (size_t)(W * H));
-  if (rc == SHB_OK) rc = rasterize_device(s, (int)W, (int)H, g->points.as<shb_surface_point>());
-  if (rc == SHB_OK && host_out) {
-    cudaError_t e = cudaMemcpyAsync(host_out, g->points.ptr, sizeof(shb_surface_point) * (size_t)(W * H),
-                                    cudaMemcpyDeviceToHost, s->ctx->stream);
-    if (e != cudaSuccess) rc = cuda_fail(e, "G-buffer download");
-  }
-  if (rc == SHB_OK) {
-    cudaError_t e = cudaStreamSynchronize(s->ctx->stream);
-    if (e != cudaSuccess) rc = cuda_fail(e, "rasterize");
-  }
+  SHB_TRY(g->points.reserve(sizeof(shb_surface_point) * (size_t)(W * H)));
+  SHB_TRY(rasterize_device(s, (int)W, (int)H, g->points.as<shb_surface_point>()));
+  if (host_out)
+    SHB_CUDA(cudaMemcpyAsync(host_out, g->points.ptr, sizeof(shb_surface_point) * (size_t)(W * H),
+                             cudaMemcpyDeviceToHost, s->ctx->stream));
+  cudaError_t e = cudaStreamSynchronize(s->ctx->stream);
+  if (e != cudaSuccess) return cuda_fail(e, "rasterize");
+  return SHB_OK;
+}
+
+}  // namespace
+
+shb_status shb_rasterize(shb_scene* s, const shb_raster_config* cfg, shb_surface_point* host_out,
+                         shb_gbuffer** out_gbuffer) {
+  if (!s || !cfg) return bad("NULL argument");
+  if (out_gbuffer) *out_gbuffer = nullptr;
+  auto* g = new shb_gbuffer();
+  shb_status rc = rasterize_into(s, cfg, g, host_out);
   if (rc != SHB_OK || !out_gbuffer) {
     delete g;
     return rc;
@@ -799,12 +807,9 @@ shb_status shb_bake_pipeline(shb_scene* s, const shb_pipeline_config* cfg, float
   SHB_CUDA(cudaSetDevice(c->device));
   const int ss = cfg->supersample_scale;
   shb_raster_config rc{cfg->width, cfg->height, ss};
-  shb_gbuffer* g = nullptr;
-  SHB_TRY(shb_rasterize(s, &rc, nullptr, &g));
-  struct Guard {
-    shb_gbuffer* g;
-    ~Guard() { shb_gbuffer_destroy(g); }
-  } guard{g};
+  if (!c->pipe_gbuf) c->pipe_gbuf = new shb_gbuffer();
+  shb_gbuffer* g = c->pipe_gbuf;
+  SHB_TRY(rasterize_into(s, &rc, g, nullptr));
   const size_t W = (size_t)cfg->width * ss, H = (size_t)cfg->height * ss;
   const size_t n_hi = W * H, n_lo = (size_t)cfg->width * cfg->height;
   // device buffers: hi-res SH + env, hi-res mask, lo-res SH + env + mask

@@ -139,6 +139,9 @@ struct shb_context {
   // scratch reused across calls
   shb::DevBuf scratch[28];
   shb::DevBuf counters;
+  // G-buffer of shb_bake_pipeline, kept between calls: allocating and
+  // freeing hundreds of MB per call stalls the host for up to a second
+  struct shb_gbuffer* pipe_gbuf = nullptr;
   void* host_pinned = nullptr;
   size_t host_pinned_bytes = 0;
 };
