@@ -626,10 +626,10 @@ shb_status build_bvh(shb_scene* s) {
     count_launch(c);
     SHB_CUDA(cudaGetLastError());
     if (n_split > 0) {
-      std::swap(idx.ptr, idx2.ptr);
-      std::swap(pslot.ptr, pslot2.ptr);
+      idx.swap(idx2);
+      pslot.swap(pslot2);
     }
-    std::swap(act.ptr, act2.ptr);
+    act.swap(act2);
     node_count += 2 * n_split;
     n_act = 2 * n_split;
     depth++;
@@ -677,7 +677,7 @@ shb_status build_bvh(shb_scene* s) {
     tri_count += totals[1];
     wide_count += totals[0];
     n_level = totals[0];
-    std::swap(lev.ptr, lev2.ptr);
+    lev.swap(lev2);
     wdepth++;
   }
   s->bvh_node_count = (uint32_t)wide_count;

@@ -19,17 +19,100 @@ shb_status cuda_fail(cudaError_t e, const char* what) {
   return e == cudaErrorMemoryAllocation ? SHB_ERR_OOM : SHB_ERR_CUDA;
 }
 
+// ------------------------------------------------------- block cache ----
+
+namespace {
+
+struct CachedBlock {
+  int dev;
+  void* ptr;
+  size_t bytes;
+};
+
+std::mutex g_cache_mu;
+std::vector<CachedBlock> g_cache;
+int g_contexts = 0;  // live contexts; the cache is emptied with the last
+constexpr size_t kCacheBytesPerDevice = size_t(8) << 30;
+
+// Returns every cached block of `dev` (all devices: -1) with cudaFree.
+void cache_flush(int dev) {
+  std::vector<CachedBlock> keep, drop;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (const CachedBlock& b : g_cache) (dev < 0 || b.dev == dev ? drop : keep).push_back(b);
+    g_cache.swap(keep);
+  }
+  int cur = 0;
+  cudaGetDevice(&cur);
+  for (const CachedBlock& b : drop) {
+    cudaSetDevice(b.dev);
+    cudaFree(b.ptr);
+  }
+  cudaSetDevice(cur);
+}
+
+// Takes the smallest cached block of `dev` that holds n bytes and is at
+// most twice that (plus 1 MiB), so a small request does not pin a large block.
+bool cache_take(int dev, size_t n, void** ptr, size_t* bytes) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  size_t best = g_cache.size();
+  for (size_t i = 0; i < g_cache.size(); ++i) {
+    const CachedBlock& b = g_cache[i];
+    if (b.dev != dev || b.bytes < n || b.bytes > 2 * n + (size_t(1) << 20)) continue;
+    if (best == g_cache.size() || b.bytes < g_cache[best].bytes) best = i;
+  }
+  if (best == g_cache.size()) return false;
+  *ptr = g_cache[best].ptr;
+  *bytes = g_cache[best].bytes;
+  g_cache.erase(g_cache.begin() + (ptrdiff_t)best);
+  return true;
+}
+
+}  // namespace
+
+void block_release(int dev, void* ptr, size_t bytes) {
+  int cur = 0;
+  cudaGetDevice(&cur);
+  if (dev >= 0 && dev != cur) cudaSetDevice(dev);
+  cudaDeviceSynchronize();  // as cudaFree: no queued work still uses the block
+  bool cached = false;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    size_t held = 0;
+    for (const CachedBlock& b : g_cache)
+      if (b.dev == dev) held += b.bytes;
+    if (g_contexts > 0 && dev >= 0 && held + bytes <= kCacheBytesPerDevice) {
+      g_cache.push_back(CachedBlock{dev, ptr, bytes});
+      cached = true;
+    }
+  }
+  if (!cached) cudaFree(ptr);
+  if (dev >= 0 && dev != cur) cudaSetDevice(cur);
+}
+
 shb_status DevBuf::reserve(size_t n) {
   if (n <= bytes && ptr) return SHB_OK;
   release();
   if (n == 0) n = 16;
+  int d = 0;
+  SHB_CUDA(cudaGetDevice(&d));
+  if (cache_take(d, n, &ptr, &bytes)) {
+    dev = d;
+    return SHB_OK;
+  }
   cudaError_t e = cudaMalloc(&ptr, n);
+  if (e == cudaErrorMemoryAllocation) {  // give the cached blocks back and retry
+    cudaGetLastError();
+    cache_flush(d);
+    e = cudaMalloc(&ptr, n);
+  }
   if (e != cudaSuccess) {
     ptr = nullptr;
     bytes = 0;
     return cuda_fail(e, "cudaMalloc");
   }
   bytes = n;
+  dev = d;
   return SHB_OK;
 }
 
@@ -220,6 +303,10 @@ shb_status shb_context_create(const shb_options* options, shb_context** out) {
     delete c;
     return cuda_fail(e, "sRGB table upload");
   }
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    ++g_contexts;
+  }
   *out = c;
   return SHB_OK;
 }
@@ -233,6 +320,12 @@ shb_status shb_context_destroy(shb_context* ctx) {
   delete ctx->pipe_gbuf;
   if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
   delete ctx;
+  bool last = false;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    last = --g_contexts == 0;
+  }
+  if (last) cache_flush(-1);
   return SHB_OK;
 }
 

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/shb.h"
@@ -33,19 +34,32 @@ shb_status cuda_fail(cudaError_t e, const char* what);
 // --------------------------------------------------------- device buffer --
 
 // Owning device allocation (cudaMalloc), grown on demand, never shrunk.
+// Device blocks given back by DevBuf::release are kept per device for reuse
+// (shb_capi.cu) instead of being returned with cudaFree, which on shared
+// machines has stalled the calling thread for up to a second.  A release
+// first waits for the device, as cudaFree does, so a cached block is never
+// still read or written by queued work when it is handed out again.
+void block_release(int dev, void* ptr, size_t bytes);
+
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
+  int dev = -1;
   DevBuf() = default;
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
   ~DevBuf() { release(); }
   void release() {
-    if (ptr) cudaFree(ptr);
+    if (ptr) block_release(dev, ptr, bytes);
     ptr = nullptr;
     bytes = 0;
   }
   shb_status reserve(size_t n);  // keeps no contents
+  void swap(DevBuf& o) {  // exchanges the blocks with their sizes
+    std::swap(ptr, o.ptr);
+    std::swap(bytes, o.bytes);
+    std::swap(dev, o.dev);
+  }
   template <class T>
   T* as() const { return reinterpret_cast<T*>(ptr); }
 };
