@@ -41,6 +41,9 @@ constexpr int kThreads = 256;
 // wave is shrunk by 2^min(bounces, kMaxBranchLog).  Branch slots beyond that
 // (more than six transmissive bounces) fall back to atomic accumulation.
 constexpr int kMaxBranchLog = 6;
+// Lights from which the forward bake runs next-event estimation as a kernel
+// of its own (k_nee).
+constexpr uint32_t kSplitNeeLights = 8;
 // Adjoint limits: the per-block gradient accumulator lives in shared memory
 // (3 x materials + lights floats) and a throughput tangent list holds at
 // most one entry per bounce.
@@ -380,6 +383,10 @@ struct WaveArgs {
   int det;
   int slots;    // branch slots per path (1 without alpha)
   float4* pend;
+  // Forward bake: k_shade leaves one next-event record per opaque hit,
+  // five float4 planes of ext_cap entries: (position, path), (normal,
+  // vertex), (ray direction, alpha), (albedo / pi, beta.x), (beta.yz).
+  float4* nee_rec;
   // Adjoint (path replay).  path_L holds each path's adjoint weight
   // dLoss/dL (RGB).  Every extend-queue entry carries the forward-mode
   // tangent of its throughput, d beta_c / d albedo_{m,c}, as a list of
@@ -590,7 +597,81 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
 // constant, so the gradient follows from the throughput tangents: d(beta X)
 // = D X + beta dX for a collected term X, and the child tangent of a bounce
 // with factor f = alpha rho h is D f + [m] beta alpha h.
+// Next-event estimation at a path vertex (src/light.cpp:82-189): the light
+// weights, NLS picks and one shadow-queue entry per visible candidate.  All
+// lanes of the warp call it (queue pushes are warp-aggregated); lanes with
+// opaque_hit false take part without work.  BWD adds the gradient packets.
 template <bool BWD>
+__device__ __forceinline__ void nee_hit(const WaveArgs& a, const BakeItem* B, uint32_t b, f3 hit_pos, f3 N, f3 wo,
+                                        f3 aop, f3 beta, float alpha, uint32_t path, uint32_t vertex,
+                                        uint32_t texel, uint32_t sample, int depth, bool opaque_hit, uint32_t ntan,
+                                        f3 adj, bool param, int mat_id, int cur, int i) {
+  Event ev;
+  ev.init(opaque_hit ? B->seed : 0u, texel, sample, vertex, EV_NEE);
+  float wcache[kWeightCache];
+  float sum = opaque_hit ? light_weight_sum<true>(B->sc, hit_pos, N, ev, wo, aop, wcache) : 0.f;
+  bool any_light = opaque_hit && !(sum < 1e-6f);
+  const int nls = opaque_hit ? B->nls : 0;
+  for (int j = 0; j < a.NLS; ++j) {
+    LightEval e;
+    bool ok = false;
+    f3 c = {0.f, 0.f, 0.f};
+    float scale = 0.f;
+    if (any_light && j < nls) {
+      ok = pick_light<true, BWD>(B->sc, hit_pos, N, ev, wo, aop, sum,
+                                 ev.u(3 * (int)B->sc.area_light_count + j), wcache, e);
+      if (ok) {
+        float pdf = e.w / sum;
+        float joint = pdf * e.apdf;
+        ok = !(joint < 1e-3f);
+        if (ok) c = cmul(beta, alpha * ((e.rad / joint) / (float)nls));
+        scale = alpha / (joint * (float)nls);
+      }
+    }
+    int slot = warp_push(a.cnt + CNT_SHADOW, ok);
+    if (ok && slot_ok(a, slot, a.sh_cap)) {
+      uint32_t target = path, kind = 0u;
+      if (BWD) {
+        // packet: tangents x X, own albedo, light parameter
+        const f3 X = e.rad * scale;
+        uint32_t np = 0;
+        for (uint32_t k = 0; k < ntan; ++k) {
+          float4 t = a.tan[cur][(int64_t)k * a.ext_cap + i];
+          f3 v = cmul(adj, cmul(f3{t.x, t.y, t.z}, X));
+          a.pk[(int64_t)np++ * a.sh_cap + slot] = make_float4(v.x, v.y, v.z, t.w);
+        }
+        if (param) {
+          f3 v = cmul(adj, cmul(beta, e.dalb * scale));
+          a.pk[(int64_t)np++ * a.sh_cap + slot] = make_float4(v.x, v.y, v.z, __uint_as_float((uint32_t)mat_id));
+        }
+        if (e.lpar) {
+          a.pk[(int64_t)np++ * a.sh_cap + slot] =
+              make_float4(dot(cmul(adj, beta), e.dpar) * scale, 0.f, 0.f, __uint_as_float(e.idx | kLightFlag));
+        } else if (e.pmat >= 0) {
+          f3 v = cmul(adj, cmul(beta, e.dpar * scale));
+          a.pk[(int64_t)np++ * a.sh_cap + slot] = make_float4(v.x, v.y, v.z, __uint_as_float((uint32_t)e.pmat));
+        }
+        a.pend[slot] = make_float4(__uint_as_float(np), 0.f, 0.f, 0.f);
+        target = (uint32_t)slot;
+        kind = 2u;
+      } else {
+        const uint32_t vslot = vertex - (1u << depth);
+        if (a.det && vslot < (uint32_t)a.slots) {
+          target = ((path * (uint32_t)a.slots + vslot) * (uint32_t)a.NLS + (uint32_t)j);
+          a.pend[target] = make_float4(c.x, c.y, c.z, 0.f);
+          kind = 2u;
+        }
+      }
+      a.sh.o[slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, e.tfar);
+      a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float(target));
+      a.sh.c[slot] = make_float4(c.x, c.y, c.z, __uint_as_float(kind | (b << 2)));
+    }
+  }
+}
+
+// SPLIT (forward only): next-event estimation is left to k_nee through a
+// record per opaque hit instead of running inline.
+template <bool BWD, bool SPLIT = false>
 __global__ void SHB_SHADE_BOUNDS k_shade(WaveArgs a, int cur, int depth) {
   extern __shared__ float sgrad[];
   if (BWD) grad_zero(sgrad, a.n_params);
@@ -699,67 +780,21 @@ __global__ void SHB_SHADE_BOUNDS k_shade(WaveArgs a, int cur, int depth) {
       f3 v = cmul(adj, beta) * (alpha * mat.emission);
       warp_grad_entry(sgrad, a, make_float4(v.x, v.y, v.z, __uint_as_float((uint32_t)max(mat_id, 0))), em_on);
     }
-    // NEE at the hit (src/light.cpp:82-189)
+    // NEE at the hit (src/light.cpp:82-189): inline, or (SPLIT) a record per
+    // opaque hit for k_nee
     f3 wo = -d;
-    Event ev;
-    ev.init(opaque_hit ? B->seed : 0u, texel, sample, vertex, EV_NEE);
-    float wcache[kWeightCache];
-    float sum = opaque_hit ? light_weight_sum<true>(B->sc, hit_pos, N, ev, wo, aop, wcache) : 0.f;
-    bool any_light = opaque_hit && !(sum < 1e-6f);
-    const int nls = opaque_hit ? B->nls : 0;
-    for (int j = 0; j < a.NLS; ++j) {
-      LightEval e;
-      bool ok = false;
-      f3 c = {0.f, 0.f, 0.f};
-      float scale = 0.f;
-      if (any_light && j < nls) {
-        ok = pick_light<true, BWD>(B->sc, hit_pos, N, ev, wo, aop, sum,
-                                   ev.u(3 * (int)B->sc.area_light_count + j), wcache, e);
-        if (ok) {
-          float pdf = e.w / sum;
-          float joint = pdf * e.apdf;
-          ok = !(joint < 1e-3f);
-          if (ok) c = cmul(beta, alpha * ((e.rad / joint) / (float)nls));
-          scale = alpha / (joint * (float)nls);
-        }
-      }
-      int slot = warp_push(a.cnt + CNT_SHADOW, ok);
-      if (ok && slot_ok(a, slot, a.sh_cap)) {
-        uint32_t target = path, kind = 0u;
-        if (BWD) {
-          // packet: tangents x X, own albedo, light parameter
-          const f3 X = e.rad * scale;
-          uint32_t np = 0;
-          for (uint32_t k = 0; k < ntan; ++k) {
-            float4 t = a.tan[cur][(int64_t)k * a.ext_cap + i];
-            f3 v = cmul(adj, cmul(f3{t.x, t.y, t.z}, X));
-            a.pk[(int64_t)np++ * a.sh_cap + slot] = make_float4(v.x, v.y, v.z, t.w);
-          }
-          if (param) {
-            f3 v = cmul(adj, cmul(beta, e.dalb * scale));
-            a.pk[(int64_t)np++ * a.sh_cap + slot] = make_float4(v.x, v.y, v.z, __uint_as_float((uint32_t)mat_id));
-          }
-          if (e.lpar) {
-            a.pk[(int64_t)np++ * a.sh_cap + slot] =
-                make_float4(dot(cmul(adj, beta), e.dpar) * scale, 0.f, 0.f, __uint_as_float(e.idx | kLightFlag));
-          } else if (e.pmat >= 0) {
-            f3 v = cmul(adj, cmul(beta, e.dpar * scale));
-            a.pk[(int64_t)np++ * a.sh_cap + slot] = make_float4(v.x, v.y, v.z, __uint_as_float((uint32_t)e.pmat));
-          }
-          a.pend[slot] = make_float4(__uint_as_float(np), 0.f, 0.f, 0.f);
-          target = (uint32_t)slot;
-          kind = 2u;
-        } else {
-          const uint32_t vslot = vertex - (1u << depth);
-          if (a.det && vslot < (uint32_t)a.slots) {
-            target = ((path * (uint32_t)a.slots + vslot) * (uint32_t)a.NLS + (uint32_t)j);
-            a.pend[target] = make_float4(c.x, c.y, c.z, 0.f);
-            kind = 2u;
-          }
-        }
-        a.sh.o[slot] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, e.tfar);
-        a.sh.d[slot] = make_float4(e.ray_d.x, e.ray_d.y, e.ray_d.z, __uint_as_float(target));
-        a.sh.c[slot] = make_float4(c.x, c.y, c.z, __uint_as_float(kind | (b << 2)));
+    if (BWD || !SPLIT) {
+      nee_hit<BWD>(a, B, b, hit_pos, N, wo, aop, beta, alpha, path, vertex, texel, sample, depth, opaque_hit, ntan,
+                   adj, param, mat_id, cur, i);
+    } else {
+      const int rs = warp_push(a.cnt + CNT_NEE, opaque_hit);
+      if (opaque_hit && slot_ok(a, rs, a.ext_cap)) {
+        const int64_t C = a.ext_cap;
+        a.nee_rec[rs] = make_float4(hit_pos.x, hit_pos.y, hit_pos.z, __uint_as_float(path));
+        a.nee_rec[C + rs] = make_float4(N.x, N.y, N.z, __uint_as_float(vertex));
+        a.nee_rec[2 * C + rs] = make_float4(d.x, d.y, d.z, alpha);
+        a.nee_rec[3 * C + rs] = make_float4(aop.x, aop.y, aop.z, beta.x);
+        a.nee_rec[4 * C + rs] = make_float4(beta.y, beta.z, 0.f, 0.f);
       }
     }
     // indirect (src/material.cpp:113-162, src/baker.cpp:131-148)
@@ -819,6 +854,46 @@ __global__ void SHB_SHADE_BOUNDS k_shade(WaveArgs a, int cur, int depth) {
     }
   }
   if (BWD) grad_flush(sgrad, a.n_params, a.grad);
+}
+
+// Next-event estimation of the forward bake over the dense record queue
+// k_shade filled (CNT_NEE): the same arithmetic as the inline call of the
+// adjoint, with fewer live registers and every lane on an opaque hit.
+__global__ void SHB_SHADE_BOUNDS k_nee(WaveArgs a, int cur, int depth) {
+  const int n = min(a.cnt[CNT_NEE], a.ext_cap);
+  const int warps = gridDim.x * (blockDim.x >> 5);
+  const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  const int64_t C = a.ext_cap;
+  for (int base = warp_id * 32; base < n; base += warps * 32) {
+    const int i = base + lane;
+    const bool active = i < n;
+    f3 hit_pos = {0.f, 0.f, 0.f}, N = {0.f, 0.f, 1.f}, d = {0.f, 0.f, 1.f}, aop = {0.f, 0.f, 0.f},
+       beta = {0.f, 0.f, 0.f};
+    float alpha = 0.f;
+    uint32_t path = 0, vertex = 0, texel = 0, sample = 0, b = 0;
+    const BakeItem* B = a.bakes;
+    if (active) {
+      const float4 r0 = a.nee_rec[i], r1 = a.nee_rec[C + i], r2 = a.nee_rec[2 * C + i],
+                   r3 = a.nee_rec[3 * C + i], r4 = a.nee_rec[4 * C + i];
+      hit_pos = {r0.x, r0.y, r0.z};
+      path = __float_as_uint(r0.w);
+      N = {r1.x, r1.y, r1.z};
+      vertex = __float_as_uint(r1.w);
+      d = {r2.x, r2.y, r2.z};
+      alpha = r2.w;
+      aop = {r3.x, r3.y, r3.z};
+      beta = {r3.w, r4.x, r4.y};
+      const PathInfo pi = a.info[path];
+      b = pi.x;
+      B = a.bakes + b;
+      texel = pi.y;
+      sample = pi.z;
+    }
+    const f3 wo = -d;
+    nee_hit<false>(a, B, b, hit_pos, N, wo, aop, beta, alpha, path, vertex, texel, sample, depth, active, 0u,
+                   f3{0.f, 0.f, 0.f}, false, -1, cur, i);
+  }
 }
 
 // Adds the gradient packets of the visible shadow rays (BWD): count in
@@ -1264,6 +1339,19 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   a.det = det ? 1 : 0;
   a.slots = slots;
   a.pend = (det || bwd) ? c->scratch[24].as<float4>() : nullptr;
+  // Next-event estimation runs as its own kernel when the light loop
+  // dominates shading (kSplitNeeLights or more lights): the hit kernel
+  // then needs 56 registers instead of 118 and every k_nee lane is on an
+  // opaque hit.  With few lights the record round trip costs more (room, 5
+  // lights: shading +18 %; atrium, 24 lights: -9 %).
+  uint32_t max_lights = 0;
+  for (const BakeSpec& sp : specs) max_lights = std::max(max_lights, sp.scene->light_count);
+  const bool split_nee = !bwd && max_lights >= kSplitNeeLights;
+  a.nee_rec = nullptr;
+  if (split_nee) {
+    SHB_TRY(c->scratch[0].reserve(sizeof(float4) * 5 * (size_t)ext_cap));
+    a.nee_rec = c->scratch[0].as<float4>();
+  }
   a.dsh = bwd ? specs[0].dsh : nullptr;
   a.ntan = ntan;
   a.npk = npk;
@@ -1337,8 +1425,16 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
                     cnt + CNT_ERROR, c64);
       close_stamp(pe);
       Pair pd = stamp(2);
-      if (bwd) k_shade<true><<<sgrid, kThreads, gsmem, st>>>(a, cur, k);
-      else k_shade<false><<<sgrid, kThreads, 0, st>>>(a, cur, k);
+      if (bwd) {
+        k_shade<true><<<sgrid, kThreads, gsmem, st>>>(a, cur, k);
+      } else if (split_nee) {
+        cudaMemsetAsync(cnt + CNT_NEE, 0, sizeof(int), st);
+        k_shade<false, true><<<sgrid, kThreads, 0, st>>>(a, cur, k);
+        k_nee<<<sgrid, kThreads, 0, st>>>(a, cur, k);
+        launches++;
+      } else {
+        k_shade<false><<<sgrid, kThreads, 0, st>>>(a, cur, k);
+      }
       close_stamp(pd);
       Pair ps = stamp(1);
       launch_shadow(st, tgrid, bk, nbk, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, a.pend,

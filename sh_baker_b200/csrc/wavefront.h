@@ -38,6 +38,7 @@ enum CounterSlot {
   CNT_FETCH_EXT = 3,
   CNT_FETCH_SHADOW = 4,
   CNT_ERROR = 5,
+  CNT_NEE = 6,  // next-event records of the current depth (forward bake)
   CNT_COUNT = 8
 };
 enum ErrorBits : int { ERR_STACK = 1, ERR_QUEUE = 2, ERR_ITER = 4 };
