@@ -591,12 +591,6 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
 }
 
 // --------------------------------------------------------------- shade ---
-// One path vertex of Trace (src/baker.cpp:70-149) in throughput form.
-// BWD: the same vertex replayed for the adjoint.  The contributions are
-// multilinear in the parameters once the light-selection pdfs are held
-// constant, so the gradient follows from the throughput tangents: d(beta X)
-// = D X + beta dX for a collected term X, and the child tangent of a bounce
-// with factor f = alpha rho h is D f + [m] beta alpha h.
 // Next-event estimation at a path vertex (src/light.cpp:82-189): the light
 // weights, NLS picks and one shadow-queue entry per visible candidate.  All
 // lanes of the warp call it (queue pushes are warp-aggregated); lanes with
@@ -669,6 +663,12 @@ __device__ __forceinline__ void nee_hit(const WaveArgs& a, const BakeItem* B, ui
   }
 }
 
+// One path vertex of Trace (src/baker.cpp:70-149) in throughput form.
+// BWD: the same vertex replayed for the adjoint.  The contributions are
+// multilinear in the parameters once the light-selection pdfs are held
+// constant, so the gradient follows from the throughput tangents: d(beta X)
+// = D X + beta dX for a collected term X, and the child tangent of a bounce
+// with factor f = alpha rho h is D f + [m] beta alpha h.
 // SPLIT (forward only): next-event estimation is left to k_nee through a
 // record per opaque hit instead of running inline.
 template <bool BWD, bool SPLIT = false>
