@@ -293,7 +293,12 @@ typedef struct shb_batch_options {
   int32_t share_paths;  /* bakes of fewer paths share waves with others;
                            larger ones get waves of their own (0: default
                            or tuned, which is half a wave; -1: no sharing) */
-  int32_t reserved[2];
+  int32_t nee_split;    /* next-event estimation of the forward bake: 0 its
+                           own kernel where the light loop is long (punctual
+                           lights + 4 x area lights >= 16), 1 inline in the
+                           hit kernel, 2 its own kernel; results are
+                           bit-identical either way                        */
+  int32_t reserved[1];
   const char* tune_cache; /* tuning file; NULL: $SHB_TUNE_CACHE or
                              $HOME/.cache/sh_baker_b200/autotune.txt        */
 } shb_batch_options;

@@ -113,7 +113,7 @@ class BatchItem(C.Structure):
 class BatchOptions(C.Structure):
     _fields_ = [("use_graph", C.c_int32), ("autotune", C.c_int32), ("wave_paths", C.c_int32),
                 ("tile_texels", C.c_int32), ("grid_scale", C.c_int32), ("share_paths", C.c_int32),
-                ("reserved", C.c_int32 * 2),
+                ("nee_split", C.c_int32), ("reserved", C.c_int32 * 1),
                 ("tune_cache", C.c_char_p)]
 
 

@@ -304,12 +304,15 @@ class BatchBake:
 
 
 def bake_batch(ctx: Context, bakes, use_graph: bool = True, autotune: bool = False, tune_cache: Optional[str] = None,
-               wave_paths: int = 0, tile_texels: int = 0, grid_scale: int = 0, share_paths: int = 0, outputs=None):
+               wave_paths: int = 0, tile_texels: int = 0, grid_scale: int = 0, share_paths: int = 0,
+               nee_split: int = 0, outputs=None):
     """Runs many bakes in one persistent launch (shb_bake_batch).  Returns
     ([(sh, env)] device tensors of W*s*H*s*27 and W*s*H*s floats, stats).
     `outputs` may supply those tensors (reused across calls).  Bakes of fewer
     than `share_paths` paths share waves, larger ones get their own (0: half
-    a wave or the tuned value; -1: no sharing)."""
+    a wave or the tuned value; -1: no sharing).  `nee_split`: next-event
+    estimation as its own kernel by light-loop cost (0), never (1) or
+    always (2); the results do not change."""
     import torch
     n = len(bakes)
     items = (A.BatchItem * max(1, n))()
@@ -330,6 +333,7 @@ def bake_batch(ctx: Context, bakes, use_graph: bool = True, autotune: bool = Fal
     opts.tile_texels = tile_texels
     opts.grid_scale = grid_scale
     opts.share_paths = share_paths
+    opts.nee_split = nee_split
     opts.tune_cache = tune_cache.encode() if tune_cache else None
     st = A.BakeStats()
     A.check(ctx.lib.shb_bake_batch(ctx.h, C.addressof(items), n, C.byref(opts), C.byref(st)))

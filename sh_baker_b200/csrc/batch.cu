@@ -235,6 +235,7 @@ extern "C" shb_status shb_bake_batch(shb_context* ctx, const shb_batch_item* ite
   if (options && options->grid_scale > 0) prm.grid_scale = options->grid_scale;
   if (options && options->share_paths > 0) prm.share_paths = options->share_paths;
   if (options && options->share_paths < 0) prm.share_paths = 0;
+  if (options && options->nee_split >= 0 && options->nee_split <= 2) prm.nee_split = options->nee_split;
   uint64_t l0 = ctx->launches;
   SHB_TRY(bake_batch_device(ctx, specs, prm, stats));
   if (stats) stats->kernel_launches = ctx->launches - l0;

@@ -41,9 +41,10 @@ constexpr int kThreads = 256;
 // wave is shrunk by 2^min(bounces, kMaxBranchLog).  Branch slots beyond that
 // (more than six transmissive bounces) fall back to atomic accumulation.
 constexpr int kMaxBranchLog = 6;
-// Lights from which the forward bake runs next-event estimation as a kernel
-// of its own (k_nee).
-constexpr uint32_t kSplitNeeLights = 8;
+// Light-loop cost from which the forward bake runs next-event estimation as
+// a kernel of its own (k_nee): punctual lights count 1, area lights 4 (each
+// samples a triangle and a point and looks up its emission).
+constexpr uint32_t kSplitNeeCost = 16;
 // Adjoint limits: the per-block gradient accumulator lives in shared memory
 // (3 x materials + lights floats) and a throughput tangent list holds at
 // most one entry per bounce.
@@ -1147,11 +1148,16 @@ shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n,
 
 namespace {
 
+uint32_t nee_cost(const shb_scene& sc) {
+  return (sc.light_count - sc.area_light_count) + 4u * sc.area_light_count;
+}
+
 struct Wave {
   int tile_begin, n_tiles;
   int64_t P, n_tex;
   int max_bounces;
   int bake;  // the one bake whose tiles fill the wave, else -1
+  uint32_t nee_cost;  // largest light-loop cost (nee_cost) of its bakes
 };
 
 // Splits every bake's valid texels into tiles of whole texels (all their
@@ -1163,10 +1169,10 @@ void plan_waves(const std::vector<BakeSpec>& specs, const std::vector<int>& n_va
                 int64_t tile_texels, int64_t share_paths, std::vector<Tile>& tiles, std::vector<Wave>& waves) {
   tiles.clear();
   waves.clear();
-  Wave cur{0, 0, 0, 0, 0, -1};
+  Wave cur{0, 0, 0, 0, 0, -1, 0};
   auto flush = [&] {
     if (cur.n_tiles > 0) waves.push_back(cur);
-    cur = Wave{(int)tiles.size(), 0, 0, 0, 0, -1};
+    cur = Wave{(int)tiles.size(), 0, 0, 0, 0, -1, 0};
   };
   auto add = [&](size_t b, int64_t cap) {
     const int64_t spp = specs[b].cfg.samples;
@@ -1188,6 +1194,7 @@ void plan_waves(const std::vector<BakeSpec>& specs, const std::vector<int>& n_va
       cur.P += paths;
       cur.n_tex += nt;
       cur.max_bounces = std::max(cur.max_bounces, specs[b].cfg.bounces);
+      cur.nee_cost = std::max(cur.nee_cost, nee_cost(*specs[b].scene));
     }
   };
   for (size_t b = 0; b < specs.size(); ++b) {
@@ -1351,16 +1358,18 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   a.det = det ? 1 : 0;
   a.slots = slots;
   a.pend = (det || bwd) ? c->scratch[24].as<float4>() : nullptr;
-  // Next-event estimation runs as its own kernel when the light loop
-  // dominates shading (kSplitNeeLights or more lights): the hit kernel
-  // then needs 56 registers instead of 118 and every k_nee lane is on an
-  // opaque hit.  With few lights the record round trip costs more (room, 5
-  // lights: shading +18 %; atrium, 24 lights: -9 %).
-  uint32_t max_lights = 0;
-  for (const BakeSpec& sp : specs) max_lights = std::max(max_lights, sp.scene->light_count);
-  const bool split_nee = !bwd && max_lights >= kSplitNeeLights;
+  // Next-event estimation runs as its own kernel in waves whose light loop
+  // dominates shading (cost kSplitNeeCost or more): the hit kernel then
+  // needs 56 registers instead of 118 and every k_nee lane is on an opaque
+  // hit.  With a short loop the record round trip costs more (room, 5
+  // punctual lights: shading +18 %; atrium, 9 punctual + 15 area: -10 %).
+  bool any_split = false;
+  auto splits = [&](const Wave& w) {
+    return !bwd && (prm.nee_split == 2 || (prm.nee_split == 0 && w.nee_cost >= kSplitNeeCost));
+  };
+  for (const Wave& w : waves) any_split = any_split || splits(w);
   a.nee_rec = nullptr;
-  if (split_nee) {
+  if (any_split) {
     SHB_TRY(c->scratch[0].reserve(sizeof(float4) * 5 * (size_t)ext_cap));
     a.nee_rec = c->scratch[0].as<float4>();
   }
@@ -1419,6 +1428,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
     a.n_tiles = w.n_tiles;
     a.P = w.P;
     a.n_tex = w.n_tex;
+    const bool split_nee = splits(w);
     // traversal of a one-bake wave skips the per-ray bake lookup
     const BakeItem* bk = w.bake >= 0 ? d_items + w.bake : d_items;
     const int nbk = w.bake >= 0 ? 1 : nb;

@@ -222,6 +222,7 @@ struct BatchParams {
   int64_t tile_texels = int64_t(1) << 30; // texels per work tile
   int grid_scale = 1;                     // traversal grid = grid_scale x SMs x occupancy
   int64_t share_paths = -1;               // bakes of fewer paths share waves (-1: wave_paths / 2)
+  int nee_split = 0;                      // next-event kernel: 0 by light-loop cost, 1 inline, 2 separate
   bool use_graph = false;                 // capture the waves in one CUDA graph
   // Path-replay adjoint instead of the forward bake (one bake): gradients of
   // sum(dsh * SH) accumulate into grad[3 * mat_count + light_count] (device,

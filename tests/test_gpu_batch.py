@@ -75,3 +75,17 @@ def test_autotune_persists_per_shape_class(gpu_ctx, tmp_path):
     assert cache.read_text().splitlines() == lines  # second batch reads the entry
     for (sh, env), (sh2, env2), (rsh, renv) in zip(outs, outs2, ref):
         assert sh.cpu().numpy().tobytes() == rsh.tobytes() == sh2.cpu().numpy().tobytes()
+
+
+def test_nee_kernel_split_is_bit_identical(gpu_ctx):
+    """Next-event estimation inline in the hit kernel (nee_split=1) or as its
+    own kernel over per-hit records (nee_split=2) gives the same bits, with
+    one and two light samples, alpha branching and area lights."""
+    bakes = make_batch(gpu_ctx)
+    ref = plain(bakes)
+    for split in (1, 2):
+        outs, st = api.bake_batch(gpu_ctx, bakes, use_graph=False, wave_paths=1 << 14, nee_split=split)
+        assert st.error_flags == 0
+        for (sh, env), (rsh, renv) in zip(outs, ref):
+            assert sh.cpu().numpy().tobytes() == rsh.tobytes()
+            assert env.cpu().numpy().tobytes() == renv.tobytes()
