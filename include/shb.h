@@ -211,6 +211,9 @@ SHB_API int32_t shb_abi_version(void);
 SHB_API const char* shb_last_error(void);
 SHB_API shb_status shb_context_create(const shb_options* options,
                                       shb_context** out);
+/* Releases the handle and the context's scratch memory.  Scenes and
+ * G-buffers made from the context keep it alive until they are destroyed,
+ * in any order; the handle must not be used again. */
 SHB_API shb_status shb_context_destroy(shb_context* ctx);
 /* Replaces the context's stream with a caller-owned cudaStream_t (or 0 for
  * the context's own stream). */

@@ -29,8 +29,10 @@ struct CachedBlock {
   size_t bytes;
 };
 
-std::mutex g_cache_mu;
-std::vector<CachedBlock> g_cache;
+// Never destroyed: device buffers can still be released while the
+// process tears down its statics at exit.
+std::mutex& g_cache_mu = *new std::mutex;
+std::vector<CachedBlock>& g_cache = *new std::vector<CachedBlock>;
 int g_contexts = 0;  // live contexts; the cache is emptied with the last
 constexpr size_t kCacheBytesPerDevice = size_t(8) << 30;
 
@@ -88,6 +90,25 @@ void block_release(int dev, void* ptr, size_t bytes) {
   }
   if (!cached) cudaFree(ptr);
   if (dev >= 0 && dev != cur) cudaSetDevice(cur);
+}
+
+void ctx_retain(shb_context* c) { c->refs.fetch_add(1); }
+
+// Drops one reference; the last frees the context and its own stream.
+void ctx_release(shb_context* c) {
+  if (c->refs.fetch_sub(1) != 1) return;
+  cudaSetDevice(c->device);
+  if (c->own_stream) {
+    cudaStreamSynchronize(c->own_stream);
+    cudaStreamDestroy(c->own_stream);
+  }
+  delete c;
+  bool last = false;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    last = --g_contexts == 0;
+  }
+  if (last) cache_flush(-1);
 }
 
 shb_status DevBuf::reserve(size_t n) {
@@ -318,14 +339,8 @@ shb_status shb_context_destroy(shb_context* ctx) {
   for (auto& b : ctx->scratch) b.release();
   ctx->counters.release();
   delete ctx->pipe_gbuf;
-  if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
-  delete ctx;
-  bool last = false;
-  {
-    std::lock_guard<std::mutex> lk(g_cache_mu);
-    last = --g_contexts == 0;
-  }
-  if (last) cache_flush(-1);
+  ctx->pipe_gbuf = nullptr;
+  shb::ctx_release(ctx);
   return SHB_OK;
 }
 
@@ -518,15 +533,18 @@ shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene
     delete s;
     return rc;
   }
+  ctx_retain(s->ctx);
   *out = s;
   return SHB_OK;
 }
 
 shb_status shb_scene_destroy(shb_scene* s) {
   if (!s) return SHB_OK;
-  cudaSetDevice(s->ctx->device);
-  cudaStreamSynchronize(s->ctx->stream);
+  shb_context* c = s->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
   delete s;
+  ctx_release(c);
   return SHB_OK;
 }
 
@@ -582,6 +600,7 @@ shb_status shb_rasterize(shb_scene* s, const shb_raster_config* cfg, shb_surface
     delete g;
     return rc;
   }
+  ctx_retain(g->ctx);
   *out_gbuffer = g;
   return SHB_OK;
 }
@@ -606,6 +625,7 @@ shb_status shb_gbuffer_upload(shb_context* ctx, const shb_surface_point* points,
     delete g;
     return rc;
   }
+  ctx_retain(g->ctx);
   *out = g;
   return SHB_OK;
 }
@@ -628,9 +648,11 @@ shb_status shb_gbuffer_dims(const shb_gbuffer* g, int32_t* width, int32_t* heigh
 
 shb_status shb_gbuffer_destroy(shb_gbuffer* g) {
   if (!g) return SHB_OK;
-  cudaSetDevice(g->ctx->device);
-  cudaStreamSynchronize(g->ctx->stream);
+  shb_context* c = g->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
   delete g;
+  ctx_release(c);
   return SHB_OK;
 }
 

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
+
 #include <string>
 #include <utility>
 #include <vector>
@@ -145,6 +147,11 @@ struct SceneView {
 
 // Opaque handles of the C ABI.
 struct shb_context {
+  // One reference for the handle and one per live scene or G-buffer made
+  // from it: shb_context_destroy drops the first, and the context (its
+  // stream included) is freed when the last one goes, so destroying scenes
+  // after their context stays valid.
+  std::atomic<int> refs{1};
   int device = 0;
   int profiling = 0;
   cudaStream_t own_stream = nullptr;
