@@ -139,9 +139,13 @@ __device__ void sample_area(const SceneView& sc, const DLight& L, Event& ev, int
   float w = 1.0f - u1 - u2;
   f3 v0 = {a.x, a.y, a.z}, v1 = {b.x, b.y, b.z}, v2 = {c.x, c.y, c.z};
   point = w * v0 + u1 * v1 + u2 * v2;
-  f2 uv = {0.f, 0.f};
-  if (info.y & kAreaHasUv) uv = w * f2{b.w, c.w} + u1 * f2{d.x, d.y} + u2 * f2{d.z, d.w};
-  rad = get_emission(sc, load_mat(sc, L.mat), uv);
+  if (L.emis_const) {
+    rad = {L.er, L.eg, L.eb};
+  } else {
+    f2 uv = {0.f, 0.f};
+    if (info.y & kAreaHasUv) uv = w * f2{b.w, c.w} + u1 * f2{d.x, d.y} + u2 * f2{d.z, d.w};
+    rad = get_emission(sc, load_mat(sc, L.mat), uv);
+  }
   pdf = a.w;
 }
 

@@ -147,6 +147,37 @@ void srgb_table(float out[256]) {
 
 void srgb_upload(const float table[256]);
 
+// Emission constants of the area lights (DLight::er/eg/eb, emis_const): for
+// a material whose albedo does not vary over the surface, albedo *
+// emission with the float products get_emission makes on the device.
+void area_emission_consts(shb_scene* s) {
+  for (uint32_t l = 0; l < s->light_count; ++l) {
+    DLight& L = s->h_lights[l];
+    L.emis_const = 0;
+    L.er = L.eg = L.eb = 0.f;
+    if (L.type != SHB_LIGHT_AREA) continue;
+    if (L.mat < 0 || (uint32_t)L.mat >= s->mat_count) {  // load_mat's default: no emission
+      L.emis_const = 1;
+      continue;
+    }
+    const DMat& M = s->h_mats[L.mat];
+    float a[3];
+    if (M.use_override) {
+      for (int c = 0; c < 3; ++c) a[c] = M.override_rgb[c];
+    } else if (s->h_light_albedo_const[l]) {
+      for (int c = 0; c < 3; ++c) a[c] = s->h_light_albedo[3 * l + c];
+    } else {
+      continue;
+    }
+    L.emis_const = 1;
+    if (M.emission > 0.0f) {
+      L.er = a[0] * M.emission;
+      L.eg = a[1] * M.emission;
+      L.eb = a[2] * M.emission;
+    }
+  }
+}
+
 // Rotation part of an affine map (Eigen Transform::rotation(): polar
 // decomposition M = U S V^T, R = U diag(x,1,1) V^T, x = sign det(U V^T)),
 // by cyclic Jacobi on M^T M in double precision.
@@ -501,6 +532,26 @@ shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene
   s->h_geoms = geoms;
   s->h_mats = mats;
   s->h_lights = lights;
+  {
+    float srgb[256];
+    srgb_table(srgb);
+    s->h_light_albedo.assign(3 * (size_t)s->light_count, 0.f);
+    s->h_light_albedo_const.assign(s->light_count, 0);
+    for (uint32_t l = 0; l < s->light_count; ++l) {
+      const DLight& L = lights[l];
+      if (L.type != SHB_LIGHT_AREA || L.mat < 0 || (uint32_t)L.mat >= s->mat_count) continue;
+      const DMat& M = mats[L.mat];
+      if (M.c == 0) {  // get_albedo's default grey
+        for (int c = 0; c < 3; ++c) s->h_light_albedo[3 * l + c] = 0.8f;
+        s->h_light_albedo_const[l] = 1;
+      } else if (M.w == 1 && M.h == 1) {
+        for (int c = 0; c < 3; ++c) s->h_light_albedo[3 * l + c] = srgb[pix[M.pix_offset + c]];
+        s->h_light_albedo_const[l] = 1;
+      }
+    }
+    area_emission_consts(s);
+    lights = s->h_lights;
+  }
   shb_status rc = SHB_OK;
   auto chk = [&](shb_status x) {
     if (rc == SHB_OK) rc = x;
@@ -814,10 +865,11 @@ shb_status shb_scene_set_params(shb_scene* s, const float* albedo_rgb, const uin
     }
   if (light_intensity)
     for (uint32_t l = 0; l < s->light_count; ++l) s->h_lights[l].intensity = light_intensity[l];
+  if (albedo_rgb) area_emission_consts(s);  // overrides change area emission
   cudaStream_t st = s->ctx->stream;
   if (albedo_rgb && s->mat_count)
     SHB_CUDA(cudaMemcpyAsync(s->mats.ptr, s->h_mats.data(), sizeof(DMat) * s->mat_count, cudaMemcpyHostToDevice, st));
-  if (light_intensity && s->light_count)
+  if ((light_intensity || albedo_rgb) && s->light_count)
     SHB_CUDA(cudaMemcpyAsync(s->lights.ptr, s->h_lights.data(), sizeof(DLight) * s->light_count,
                              cudaMemcpyHostToDevice, st));
   SHB_CUDA(cudaStreamSynchronize(st));

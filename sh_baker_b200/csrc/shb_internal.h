@@ -97,6 +97,11 @@ struct DLight {
   int32_t geom;      // area: geometry index
   int32_t mat;       // area: material index
   int32_t area_ord;  // area: ordinal among area lights (RNG slots)
+  // area: emission when it is the same at every point (the material's
+  // albedo is untextured, a 1x1 texture or an override), computed on the
+  // host with the device's operations; emis_const 0: look it up per sample
+  float er, eg, eb;
+  int32_t emis_const;
 };
 
 // Compressed 8-wide BVH node (80 bytes).  Children boxes are quantised on
@@ -181,6 +186,10 @@ struct shb_scene {
   std::vector<shb::DGeom> h_geoms;
   std::vector<shb::DMat> h_mats;      // host copies, edited by shb_scene_set_params
   std::vector<shb::DLight> h_lights;
+  // per light: the albedo of a 1x1 or untextured material (3 floats) and
+  // whether that albedo is constant, for the area-emission constants
+  std::vector<float> h_light_albedo;
+  std::vector<uint8_t> h_light_albedo_const;
   // BVH
   shb::DevBuf bvh_nodes, bvh_tris;
   uint32_t bvh_node_count = 0, bvh_tri_count = 0, bvh_depth = 0;
