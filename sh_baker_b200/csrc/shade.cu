@@ -539,7 +539,36 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
     ev.init(active ? B->seed : 0u, texel, sample, 0, EV_NEE);
     const f3 zero3 = {0.f, 0.f, 0.f};
     float wcache[kWeightCache];
-    float sum = active ? light_weight_sum<false>(B->sc, P0, N, ev, zero3, zero3, wcache) : 0.f;
+    float sum = 0.f;
+    // Without area lights the weights depend on the texel only.  When the
+    // warp's paths all belong to one texel (spp >= 32 mostly), lane j
+    // evaluates light j and the lanes share the weights by shuffle; each
+    // lane still sums them in light order, so the result is the same.
+    const unsigned act = __ballot_sync(0xFFFFFFFFu, active);
+    const uint64_t key = active ? ((uint64_t)b << 32 | texel) : ~0ull;
+    const int lead = act ? __ffs(act) - 1 : 0;
+    const uint64_t key0 = __shfl_sync(0xFFFFFFFFu, key, lead);
+    const bool coop =
+        act && __all_sync(0xFFFFFFFFu, !active || (key == key0 && B->sc.area_light_count == 0 &&
+                                                   B->sc.light_count <= kWeightCache));
+    if (coop) {
+      const BakeItem* BL = a.bakes + (uint32_t)(key0 >> 32);
+      const f3 Pl = {__shfl_sync(0xFFFFFFFFu, P0.x, lead), __shfl_sync(0xFFFFFFFFu, P0.y, lead),
+                     __shfl_sync(0xFFFFFFFFu, P0.z, lead)};
+      const f3 Nl = {__shfl_sync(0xFFFFFFFFu, N.x, lead), __shfl_sync(0xFFFFFFFFu, N.y, lead),
+                     __shfl_sync(0xFFFFFFFFu, N.z, lead)};
+      const uint32_t nl = BL->sc.light_count;
+      const float mine = (uint32_t)lane < nl ? eval_light<false>(BL->sc, (uint32_t)lane, Pl, Nl, ev, zero3, zero3).w
+                                             : 0.f;
+      for (uint32_t i = 0; i < nl; ++i) {
+        const float w = __shfl_sync(0xFFFFFFFFu, mine, (int)i);
+        wcache[i] = w;
+        sum += w;
+      }
+      if (!active) sum = 0.f;
+    } else if (active) {
+      sum = light_weight_sum<false>(B->sc, P0, N, ev, zero3, zero3, wcache);
+    }
     bool any_light = active && !(sum < 1e-6f);
     const int nls = active ? B->nls : 0;
     for (int j = 0; j < a.NLS; ++j) {
