@@ -1,6 +1,6 @@
 """Global relative RMSE of the GPU bake against the 4096-spp FP64 CPU oracle
 (tests/golden/fp64_<workload>.npz, made by tests/golden/make_fp64_reference.py)
-on a 32x32 crop of the output lightmap, at the workload's own spp.
+on a 64x64 crop of the output lightmap, at the workload's own spp.
 
 The reference estimator samples primary directions uniformly over the
 hemisphere (src/baker.cpp:38-46), so at matched spp its Monte-Carlo noise
