@@ -410,6 +410,37 @@ def run_adjoint(args):
     ctx.close()
 
 
+def accuracy(w, scene, ctx):
+    """Global relative RMSE of a GPU bake, at the workload's spp and bounces,
+    against the committed 4096-spp FP64 oracle fixture of the workload
+    (tests/golden/fp64_<kind>.npz, a crop of the output lightmap), over all
+    valid texels x 27 coefficients.  None when no fixture matches the
+    workload's size."""
+    import numpy as np
+
+    from sh_baker_b200 import api
+    path = ROOT / "tests" / "golden" / f"fp64_{w['kind']}.npz"
+    if not path.exists():
+        return None
+    ref = np.load(path)
+    W, H, ss, size, x0, y0 = (int(ref[k]) for k in ("width", "height", "ss", "size", "x0", "y0"))
+    if (W, H, ss, int(ref["bounces"])) != (w["width"], w["height"], w["ss"], w["bounces"]):
+        return None
+    pts = api.RasterizeScene(scene, api.RasterConfig(W, H, ss), ctx=ctx).reshape(H * ss, W * ss)
+    crop = np.ascontiguousarray(pts[y0 * ss:(y0 + size) * ss, x0 * ss:(x0 + size) * ss]).reshape(-1)
+    rc = api.RasterConfig(size, size, ss)
+    got = api.BakeSHLightMap(scene, crop, rc, api.BakeConfig(samples=w["spp"], bounces=w["bounces"], seed=2024),
+                             ctx=ctx)
+    g = api.DownsampleSHTexture(got.sh_texture, ss, ctx=ctx).reshape(size, size, 27)
+    valid, r = ref["valid"], ref["sh"]
+    err = float(np.linalg.norm((g - r)[valid]) / np.linalg.norm(r[valid]))
+    err_l0 = float(np.linalg.norm((g - r)[valid][:, :3]) / np.linalg.norm(r[valid][:, :3]))
+    floor = float(np.linalg.norm(ref["se"][valid]) / np.linalg.norm(r[valid]))
+    return {"rel_rmse_vs_fp64": err, "rel_rmse_l0_vs_fp64": err_l0, "fp64_own_error": floor,
+            "fp64_spp": int(ref["spp"]),
+            "crop": f"{size}x{size} output texels at ({x0},{y0}), supersample {ss}", "spp": w["spp"]}
+
+
 def config_of(w, scene):
     return {"workload": f"procedural {w['kind']}: {scene.triangle_count} triangles, lightmap {w['width']}x{w['height']}"
                         f" supersample {w['ss']}, {w['spp']} spp, {w['bounces']} bounces, dilation {w['dilation']}",
@@ -660,7 +691,8 @@ def main():
                                     "launches": sum(s.extend_launches for s in stats) // args.steps},
                     "any_hit": {"rays": sh_rays // args.steps,
                                 "launches": sum(s.shadow_launches for s in stats) // args.steps}},
-                "rays_per_texel_sample": (ext_rays + sh_rays) / max(ts, 1)}
+                "rays_per_texel_sample": (ext_rays + sh_rays) / max(ts, 1),
+                "accuracy": accuracy(w, scene, ctx) if world == 1 else None}
         print(json.dumps(line), flush=True)
     del sh, env
     g.close()
