@@ -3,9 +3,10 @@
 For each workload a crop of the output lightmap (64 x 64 texels,
 supersample 3) is baked by the CPU oracle in double precision at 4096
 samples per supersampled texel (Philox stream, seed 987654, independent of
-every GPU seed), then box-downsampled like the pipeline.  The atrium's crop
-is a lit region: its corner is dim enough that 4096 samples still leave
-most of the signal as noise.  Written as float32 to
+every GPU seed), then box-downsampled like the pipeline.  The crops are lit
+regions, chosen by a quick low-spp bake of candidate crops: the lightmaps'
+corners are dim enough that 4096 samples still leave much of the signal
+as noise there.  Written as float32 to
 tests/golden/fp64_<workload>.npz with the crop position and per-texel
 standard errors.
 
@@ -27,7 +28,7 @@ from sh_baker_b200 import scenes  # noqa: E402
 
 CROPS = {
     # workload: (scene factory, width, height, ss, bounces, crop x0, crop y0, crop size)
-    "room": (lambda: scenes.procedural_room(seed=2, res=1024), 1024, 1024, 3, 3, 0, 0, 64),
+    "room": (lambda: scenes.procedural_room(seed=2, res=1024), 1024, 1024, 3, 3, 384, 128, 64),
     "atrium": (lambda: scenes.atrium(seed=3, res=2048), 2048, 2048, 3, 4, 512, 256, 64),
 }
 SPP = 4096
