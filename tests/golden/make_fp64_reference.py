@@ -29,7 +29,7 @@ from sh_baker_b200 import scenes  # noqa: E402
 CROPS = {
     # workload: (scene factory, width, height, ss, bounces, crop x0, crop y0, crop size)
     "room": (lambda: scenes.procedural_room(seed=2, res=1024), 1024, 1024, 3, 3, 384, 128, 64),
-    "atrium": (lambda: scenes.atrium(seed=3, res=2048), 2048, 2048, 3, 4, 512, 256, 64),
+    "atrium": (lambda: scenes.atrium(seed=3, res=2048), 2048, 2048, 3, 4, 512, 256, 128),
 }
 SPP = 4096
 SEED = 987654
