@@ -13,7 +13,7 @@ import pytest
 
 from oracle import pyoracle as O
 from sh_baker_b200 import api, scenes
-from sh_baker_b200.scene import AREA, DIRECTIONAL, POINT, Geometry, Light, Material, Scene, Texture
+from sh_baker_b200.scene import AREA, Geometry, Light, Material, Scene, Texture
 
 pytestmark = pytest.mark.gpu
 

@@ -3,7 +3,6 @@ EvalSHBasis in glsl/viz.frag:42-99 as arithmetic): shb_sh_preview,
 shb_exr_load_channels, shb_write_png and the sh_cvt command line."""
 import ctypes as C
 import subprocess
-import tempfile
 import zlib
 from pathlib import Path
 
