@@ -436,8 +436,9 @@ def accuracy(w, scene, ctx):
     err = float(np.linalg.norm((g - r)[valid]) / np.linalg.norm(r[valid]))
     err_l0 = float(np.linalg.norm((g - r)[valid][:, :3]) / np.linalg.norm(r[valid][:, :3]))
     floor = float(np.linalg.norm(ref["se"][valid]) / np.linalg.norm(r[valid]))
+    expected = floor * float(np.sqrt(int(ref["spp"]) / w["spp"] + 1.0))
     return {"rel_rmse_vs_fp64": err, "rel_rmse_l0_vs_fp64": err_l0, "fp64_own_error": floor,
-            "fp64_spp": int(ref["spp"]),
+            "unbiased_predicted": expected, "fp64_spp": int(ref["spp"]),
             "crop": f"{size}x{size} output texels at ({x0},{y0}), supersample {ss}", "spp": w["spp"]}
 
 

@@ -1,12 +1,17 @@
 """Global relative RMSE of the GPU bake against the 4096-spp FP64 CPU oracle
 (tests/golden/fp64_<workload>.npz, made by tests/golden/make_fp64_reference.py)
-on a 64x64 crop of the output lightmap, at the workload's own spp.
+on a crop of the output lightmap (room 64x64, atrium 128x128), at the
+workload's own spp.
 
 The reference estimator samples primary directions uniformly over the
 hemisphere (src/baker.cpp:38-46), so at matched spp its Monte-Carlo noise
-alone can exceed 1 %.  The yardstick is therefore the reference algorithm
-itself (the oracle restatement on the reference's mt19937 stream) at the
-same spp: the GPU must reach 1 % or be no less accurate than that.
+alone exceeds 1 %.  The yardstick is therefore the error an unbiased
+estimator of the same variance has at that spp, which the fixture's
+per-texel standard errors predict: ||se|| sqrt(4096 / spp + 1) / ||ref||
+(the bake's noise plus the fixture's own).  The GPU must reach 1 % or stay
+within 25 % of that prediction.  The reference algorithm itself (the oracle
+on the reference's mt19937 stream) is held to the same gate, which checks
+the prediction; both errors are printed.
 """
 from pathlib import Path
 
@@ -45,6 +50,8 @@ def test_relative_rmse_vs_fp64_oracle(gpu_ctx, name, spp):
     e_gpu = rel_rmse(g, r, valid)
     e_cpu = rel_rmse(c, r, valid)
     floor = float(np.linalg.norm(ref["se"][valid]) / np.linalg.norm(r[valid]))
-    print(f"{name}: rel. RMSE vs FP64@4096: GPU {e_gpu:.4f}, reference algorithm {e_cpu:.4f} "
-          f"(FP64 reference's own error {floor:.4f}) at {spp} spp")
-    assert e_gpu <= max(0.01, 1.25 * e_cpu), (e_gpu, e_cpu)
+    expected = floor * float(np.sqrt(int(ref["spp"]) / spp + 1.0))
+    print(f"{name}: rel. RMSE vs FP64@{int(ref['spp'])}: GPU {e_gpu:.4f}, reference algorithm {e_cpu:.4f}, "
+          f"unbiased estimator predicted {expected:.4f} (FP64 reference's own error {floor:.4f}) at {spp} spp")
+    assert e_cpu <= max(0.01, 1.25 * expected), (e_cpu, expected)
+    assert e_gpu <= max(0.01, 1.25 * expected), (e_gpu, expected)
