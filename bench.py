@@ -447,9 +447,16 @@ def config_of(w, scene):
                         f" supersample {w['ss']}, {w['spp']} spp, {w['bounces']} bounces, dilation {w['dilation']}",
             "triangles": scene.triangle_count, "width": w["width"], "height": w["height"],
             "supersample_scale": w["ss"], "samples": w["spp"], "bounces": w["bounces"], "dilation": w["dilation"],
-            "l2": "inputs larger than L2: G-buffer %.0f MB + outputs %.0f MB per step" % (
-                w["width"] * w["ss"] * w["height"] * w["ss"] * 64 / 1e6,
-                w["width"] * w["ss"] * w["height"] * w["ss"] * 112 / 1e6)}
+            "l2": l2_note(w)}
+
+
+def l2_note(w):
+    """Whether one step's G-buffer reads and SH/env writes exceed the 126 MB
+    L2, so that steps do not hit each other's data in cache."""
+    n = w["width"] * w["ss"] * w["height"] * w["ss"]
+    gb, out = n * 64 / 1e6, n * 112 / 1e6
+    kind = "inputs larger than L2" if gb + out > 126 else "inputs fit in the 126 MB L2 (a parity case)"
+    return "%s: G-buffer %.0f MB + outputs %.0f MB per step" % (kind, gb, out)
 
 
 def run_exr(args):
