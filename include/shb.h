@@ -19,6 +19,8 @@
  * are owned by the opaque handles.  Every entry point returns a shb_status;
  * shb_last_error() returns a thread-local message for the last failure.
  * One context owns one CUDA stream; use one context per host thread.
+ * Entry points run on their context's device and give the calling thread
+ * its previous current device back before they return.
  *
  * Memory layouts are binary compatible with the reference's Eigen structs:
  *   shb_surface_point == sh_baker::SurfacePoint (64 bytes, Vector4f 16-byte
@@ -360,14 +362,18 @@ SHB_API shb_status shb_dilate(shb_context* ctx, int32_t kind, int32_t width,
  * with a deadline where cudaMalloc's implicit synchronisation is not
  * acceptable).  Same passes and results as shb_dilate on device pointers
  * (pixels and mask on the context's device, updated in place).  The
- * ping-pong scratch lives in one fixed 16 MiB array inside the library,
- * which every GPU that loads the library holds until the process exits.  At
+ * ping-pong scratch lives in one fixed 16 MiB array inside the library.
+ * Its device address is looked up by shb_context_create, so every device
+ * that has had a context holds the array from then until the process
+ * exits, and this call itself neither loads code nor reserves memory.  At
  * most about 153,000 texels of SH9, 3.3 million of float or 8.3 million of
  * uint8, and at most 4096 passes; larger requests return
- * SHB_ERR_INVALID_ARG.  The first call on a device looks up the array's
- * device address; make that first call before any stream capture.  All
- * calls share the array, so calls that overlap on the GPU (other host
- * threads or streams) race and must be serialised by the caller. */
+ * SHB_ERR_INVALID_ARG.  The call only enqueues work on the context's
+ * stream and returns: the results are ready once that stream has been
+ * synchronised.  All calls share the array, so calls that overlap on the
+ * GPU (other contexts, host threads or streams) race and must be ordered
+ * by the caller; calls on one context's stream are ordered by the stream.
+ * The calling thread's current device is the same on return. */
 SHB_API shb_status shb_dilate_noalloc(shb_context* ctx, int32_t kind, int32_t width,
                                       int32_t height, void* pixels, uint8_t* mask,
                                       int32_t passes);

@@ -5,9 +5,11 @@ this image; the oracle is a restatement.  The reference's vendored EXR
 library (src/tinyexr_impl.cpp + src/miniz.c) does compile: build_ref()
 compiles it where it lies in the reference tree, together with
 oracle/exr_ref_harness.cpp, into oracle/_ref/libexr_ref.so (only when the
-reference tree is present)."""
+reference tree is present).  The reference's `src` folder is
+$SHB_REFERENCE_SRC, else `reference/src` beside this repository's folder."""
 from __future__ import annotations
 
+import os
 import subprocess
 import sys
 from pathlib import Path
@@ -28,7 +30,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     return LIB
 
 
-REF_SRC = Path("/root/reference/src")
+REF_SRC = Path(os.environ.get("SHB_REFERENCE_SRC", str(HERE.parent.parent / "reference" / "src")))
 REF_DIR = HERE / "_ref"
 REF_LIB = REF_DIR / "libexr_ref.so"
 

@@ -49,16 +49,24 @@ def _newer(out: Path, deps) -> bool:
 def build(verbose: bool = False, force: bool = False) -> Path:
     BUILD.mkdir(exist_ok=True)
     headers = [CSRC / h for h in HEADERS] + [PKG.parent / "include" / "shb.h"]
-    objs = []
+    objs, cmds = [], []
     for src, flags in SOURCES.items():
         s = CSRC / src
         o = BUILD / (src + ".o")
         objs.append(o)
         if force or _newer(o, [s, *headers, Path(__file__)]):
-            cmd = [nvcc(), *ARCH, *COMMON, *flags, "-c", str(s), "-o", str(o)]
+            cmds.append([nvcc(), *ARCH, *COMMON, *flags, "-c", str(s), "-o", str(o)])
+    if cmds:
+        from concurrent.futures import ThreadPoolExecutor
+
+        def run(cmd):
             if verbose:
                 print(" ".join(cmd), flush=True)
             subprocess.run(cmd, check=True)
+
+        with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+            for f in [pool.submit(run, c) for c in cmds]:
+                f.result()
     if force or _newer(LIB, objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lz", "-Xlinker", "--no-undefined"]
         if verbose:

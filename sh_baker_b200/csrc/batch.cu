@@ -177,7 +177,7 @@ extern "C" shb_status shb_bake_batch(shb_context* ctx, const shb_batch_item* ite
   }
   if (stats) std::memset(stats, 0, sizeof(*stats));
   if (count <= 0) return SHB_OK;
-  SHB_CUDA(cudaSetDevice(ctx->device));
+  SHB_ON_DEVICE(ctx->device);
   std::vector<BakeSpec> specs;
   specs.reserve(count);
   for (int i = 0; i < count; ++i) {

@@ -37,7 +37,7 @@ constexpr int kThreads = 256;
 
 inline int grid_for(int64_t n) {
   int64_t g = (n + kThreads - 1) / kThreads;
-  if (g > 148 * 32) g = 148 * 32;
+  if (g > sm_count() * 32) g = sm_count() * 32;
   return (int)(g < 1 ? 1 : g);
 }
 

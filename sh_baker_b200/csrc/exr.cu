@@ -183,9 +183,9 @@ shb_status write_exr(shb_context* c, const float* d_sh, const float* d_env, int 
   uint8_t* d_raw = c->scratch[26].as<uint8_t>();
   uint8_t* d_pred = d_raw + total;
   const int64_t samples = (int64_t)W * H * t.n;
-  const int grid = (int)std::min<int64_t>((samples + 255) / 256, 148 * 16);
+  const int grid = (int)std::min<int64_t>((samples + 255) / 256, shb::sm_count() * 16);
   k_exr_raw<<<grid, 256, 0, st>>>(d_sh, d_env, W, H, t, reinterpret_cast<uint16_t*>(d_raw));
-  const int grid2 = (int)std::min<int64_t>((total + 255) / 256, 148 * 16);
+  const int grid2 = (int)std::min<int64_t>((total + 255) / 256, shb::sm_count() * 16);
   k_exr_predict<<<grid2, 256, 0, st>>>(d_raw, line_bytes, H, total, d_pred);
   count_launch(c, 2);
   SHB_CUDA(cudaGetLastError());

@@ -88,7 +88,7 @@ __global__ void k_sh_preview(const float* __restrict__ sh, int64_t n, const floa
 
 shb_status sh_preview_device(shb_context* c, const float* d_sh, int64_t n, const float* d_normals, const float dir[3],
                              int mode, int reinhard, uint8_t* d_out) {
-  const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 16);
+  const int grid = (int)std::min<int64_t>((n + 255) / 256, shb::sm_count() * 16);
   if (n > 0)
     k_sh_preview<<<grid, 256, 0, c->stream>>>(d_sh, n, d_normals, make_float3(dir[0], dir[1], dir[2]), mode,
                                               reinhard, d_out);

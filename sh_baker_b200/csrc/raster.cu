@@ -17,7 +17,7 @@ constexpr int kThreads = 256;
 
 inline int grid_for(int64_t n, int threads = kThreads) {
   int64_t g = (n + threads - 1) / threads;
-  if (g > 148 * 64) g = 148 * 64;
+  if (g > sm_count() * 64) g = sm_count() * 64;
   return (int)(g < 1 ? 1 : g);
 }
 
@@ -467,8 +467,9 @@ shb_status dilate_device(shb_context* c, int kind, int w, int h, void* pixels, u
 // synchronisation and unpredictable latency are not acceptable.  For them
 // shb_dilate_noalloc runs the same dilation passes as shb_dilate, but the
 // ping-pong copy of the pixels and mask and the per-pass change flags live
-// in the fixed array below.  The library holds that array on every GPU that
-// loads it until the process exits.
+// in the fixed array below.  Its device address is looked up when a
+// context is created on a device (noalloc_prepare), so the array is held on
+// every device that has had a context, from then until the process exits.
 
 namespace {
 
@@ -503,6 +504,14 @@ shb_status noalloc_scratch(int device, unsigned char** out) {
 
 }  // namespace
 
+namespace shb {
+shb_status noalloc_prepare(int device) {
+  if (device < 0 || device >= kNoAllocMaxDevices) return SHB_OK;  // the entry point reports it
+  unsigned char* p = nullptr;
+  return noalloc_scratch(device, &p);
+}
+}  // namespace shb
+
 extern "C" SHB_API shb_status shb_dilate_noalloc(shb_context* ctx, int32_t kind, int32_t width, int32_t height,
                                                  void* pixels, uint8_t* mask, int32_t passes) {
   using namespace shb;
@@ -519,9 +528,18 @@ extern "C" SHB_API shb_status shb_dilate_noalloc(shb_context* ctx, int32_t kind,
     set_error("NULL argument");
     return SHB_ERR_INVALID_ARG;
   }
-  const int64_t n = (int64_t)width * height;
+  const int64_t n = (int64_t)width * height;  // width, height > 0 and < 2^31: no overflow
   const int ch = kind == SHB_DILATE_SH9 ? 27 : 1;
   const size_t esz = kind == SHB_DILATE_U8 ? 1 : 4;
+  auto too_large = [&](const std::string& need) {
+    set_error("shb_dilate_noalloc: " + std::to_string(width) + "x" + std::to_string(height) + " texels need " + need +
+              " bytes of scratch; the fixed array holds " + std::to_string(kNoAllocScratchBytes) +
+              " (about 153,000 texels of SH9, 3.3 M of float, 8.3 M of uint8)");
+    return SHB_ERR_INVALID_ARG;
+  };
+  // every texel needs at least one mask byte of scratch: bound n before the
+  // byte counts below are formed
+  if (n > (int64_t)kNoAllocScratchBytes) return too_large("more than " + std::to_string(n));
   const size_t pbytes = esz * (size_t)n * ch;
   const size_t pbytes_aligned = (pbytes + 255) & ~size_t(255);
   const size_t need = kNoAllocFlagBytes + pbytes_aligned + (size_t)n;
@@ -529,13 +547,8 @@ extern "C" SHB_API shb_status shb_dilate_noalloc(shb_context* ctx, int32_t kind,
     set_error("shb_dilate_noalloc: at most " + std::to_string(kNoAllocMaxPasses) + " passes");
     return SHB_ERR_INVALID_ARG;
   }
-  if (need > kNoAllocScratchBytes) {
-    set_error("shb_dilate_noalloc: " + std::to_string(width) + "x" + std::to_string(height) + " texels need " +
-              std::to_string(need) + " bytes of scratch; the fixed array holds " +
-              std::to_string(kNoAllocScratchBytes) + " (about 153,000 texels of SH9, 3.3 M of float, 8.3 M of uint8)");
-    return SHB_ERR_INVALID_ARG;
-  }
-  SHB_CUDA(cudaSetDevice(ctx->device));
+  if (need > kNoAllocScratchBytes) return too_large(std::to_string(need));
+  SHB_ON_DEVICE(ctx->device);
   unsigned char* base = nullptr;
   SHB_TRY(noalloc_scratch(ctx->device, &base));
   int* changed = reinterpret_cast<int*>(base);
@@ -563,6 +576,5 @@ extern "C" SHB_API shb_status shb_dilate_noalloc(shb_context* ctx, int32_t kind,
     SHB_CUDA(cudaMemcpyAsync(mask, masks[1], (size_t)n, cudaMemcpyDeviceToDevice, st));
   }
   SHB_CUDA(cudaGetLastError());
-  SHB_CUDA(cudaStreamSynchronize(st));
   return SHB_OK;
 }

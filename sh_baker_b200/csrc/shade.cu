@@ -1117,7 +1117,7 @@ struct ValidPred {
 
 inline int grid_for(int64_t n) {
   int64_t g = (n + kThreads - 1) / kThreads;
-  if (g > 148 * 8) g = 148 * 8;
+  if (g > sm_count() * 8) g = sm_count() * 8;
   return (int)(g < 1 ? 1 : g);
 }
 
@@ -1146,7 +1146,7 @@ shb_status build_area_tris(shb_scene* s) {
     SHB_TRY(tmp.reserve(sizeof(uint4) * entries.size()));
     SHB_CUDA(cudaMemcpyAsync(tmp.ptr, entries.data(), sizeof(uint4) * entries.size(), cudaMemcpyHostToDevice, st));
     const int n = (int)entries.size();
-    k_area_tris<<<std::min((n + 255) / 256, 148 * 8), 256, 0, st>>>(s->view(), tmp.as<uint4>(), n,
+    k_area_tris<<<std::min((n + 255) / 256, sm_count() * 8), 256, 0, st>>>(s->view(), tmp.as<uint4>(), n,
                                                                       s->area_tris.as<float4>());
     count_launch(s->ctx, 1);
     SHB_CUDA(cudaGetLastError());
@@ -1423,7 +1423,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   const size_t gsmem = bwd ? sizeof(float) * (size_t)n_params : 0;
 
   const int tgrid = traversal_grid(c->device) * std::max(1, prm.grid_scale);
-  const int sgrid = 148 * 8;
+  const int sgrid = sm_count() * 8;
   const bool timed = c->profiling && !prm.use_graph;
   struct Pair {
     cudaEvent_t a, b;

@@ -92,12 +92,29 @@ void block_release(int dev, void* ptr, size_t bytes) {
   if (dev >= 0 && dev != cur) cudaSetDevice(cur);
 }
 
+int sm_count() {
+  static std::atomic<int> cache[64];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0) dev = 0;
+  if (dev < 64) {
+    int v = cache[dev].load(std::memory_order_relaxed);
+    if (v > 0) return v;
+  }
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms < 1) {
+    cudaGetLastError();
+    sms = 1;
+  }
+  if (dev < 64) cache[dev].store(sms, std::memory_order_relaxed);
+  return sms;
+}
+
 void ctx_retain(shb_context* c) { c->refs.fetch_add(1); }
 
 // Drops one reference; the last frees the context and its own stream.
 void ctx_release(shb_context* c) {
   if (c->refs.fetch_sub(1) != 1) return;
-  cudaSetDevice(c->device);
+  ::shb::DeviceScope _shb_device_scope(c->device);
   if (c->own_stream) {
     cudaStreamSynchronize(c->own_stream);
     cudaStreamDestroy(c->own_stream);
@@ -329,7 +346,7 @@ shb_status shb_context_create(const shb_options* options, shb_context** out) {
   }
   int dev = options ? options->device : 0;
   if (dev < 0 || dev >= ndev) return bad("device ordinal out of range");
-  SHB_CUDA(cudaSetDevice(dev));
+  SHB_ON_DEVICE(dev);
   cudaDeviceProp prop;
   SHB_CUDA(cudaGetDeviceProperties(&prop, dev));
   if (prop.major < 10) {
@@ -355,6 +372,14 @@ shb_status shb_context_create(const shb_options* options, shb_context** out) {
     delete c;
     return cuda_fail(e, "sRGB table upload");
   }
+  // shb_dilate_noalloc's fixed array: its address is resolved here, so that
+  // the entry point itself never loads a module or reserves memory
+  shb_status ns = noalloc_prepare(dev);
+  if (ns != SHB_OK) {
+    cudaStreamDestroy(c->own_stream);
+    delete c;
+    return ns;
+  }
   {
     std::lock_guard<std::mutex> lk(g_cache_mu);
     ++g_contexts;
@@ -365,7 +390,7 @@ shb_status shb_context_create(const shb_options* options, shb_context** out) {
 
 shb_status shb_context_destroy(shb_context* ctx) {
   if (!ctx) return SHB_OK;
-  cudaSetDevice(ctx->device);
+  ::shb::DeviceScope _shb_device_scope(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   for (auto& b : ctx->scratch) b.release();
   ctx->counters.release();
@@ -395,7 +420,7 @@ shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene
   if (d->geometry_count && !d->geometries) return bad("geometries is NULL");
   if (d->material_count && !d->materials) return bad("materials is NULL");
   if (d->light_count && !d->lights) return bad("lights is NULL");
-  SHB_CUDA(cudaSetDevice(ctx->device));
+  SHB_ON_DEVICE(ctx->device);
   cudaStream_t st = ctx->stream;
   std::vector<float> ov, on, tuv, luv, ot, lin, rot;
   std::vector<uint32_t> vidx, tgeom, vgeom;
@@ -592,7 +617,7 @@ shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene
 shb_status shb_scene_destroy(shb_scene* s) {
   if (!s) return SHB_OK;
   shb_context* c = s->ctx;
-  cudaSetDevice(c->device);
+  ::shb::DeviceScope _shb_device_scope(c->device);
   cudaStreamSynchronize(c->stream);
   delete s;
   ctx_release(c);
@@ -601,7 +626,7 @@ shb_status shb_scene_destroy(shb_scene* s) {
 
 shb_status shb_scene_rebuild_bvh(shb_scene* s) {
   if (!s) return bad("scene is NULL");
-  SHB_CUDA(cudaSetDevice(s->ctx->device));
+  SHB_ON_DEVICE(s->ctx->device);
   SHB_TRY(build_bvh(s));
   SHB_CUDA(cudaStreamSynchronize(s->ctx->stream));
   return SHB_OK;
@@ -625,7 +650,7 @@ shb_status rasterize_into(shb_scene* s, const shb_raster_config* cfg, shb_gbuffe
     return bad("raster width, height and supersample_scale must be positive");
   int64_t W = (int64_t)cfg->width * cfg->supersample_scale, H = (int64_t)cfg->height * cfg->supersample_scale;
   if (W > 65535 || H > 65535 || W * H > (1ll << 31) - 1) return bad("raster size too large");
-  SHB_CUDA(cudaSetDevice(s->ctx->device));
+  SHB_ON_DEVICE(s->ctx->device);
   g->ctx = s->ctx;
   g->width = (int)W;
   g->height = (int)H;
@@ -660,7 +685,7 @@ shb_status shb_gbuffer_upload(shb_context* ctx, const shb_surface_point* points,
                               shb_gbuffer** out) {
   if (!ctx || !points || !out) return bad("NULL argument");
   if (width <= 0 || height <= 0) return bad("width and height must be positive");
-  SHB_CUDA(cudaSetDevice(ctx->device));
+  SHB_ON_DEVICE(ctx->device);
   auto* g = new shb_gbuffer();
   g->ctx = ctx;
   g->width = width;
@@ -683,7 +708,7 @@ shb_status shb_gbuffer_upload(shb_context* ctx, const shb_surface_point* points,
 
 shb_status shb_gbuffer_download(const shb_gbuffer* g, shb_surface_point* points) {
   if (!g || !points) return bad("NULL argument");
-  SHB_CUDA(cudaSetDevice(g->ctx->device));
+  SHB_ON_DEVICE(g->ctx->device);
   SHB_CUDA(cudaMemcpyAsync(points, g->points.ptr, sizeof(shb_surface_point) * (size_t)g->width * g->height,
                            cudaMemcpyDeviceToHost, g->ctx->stream));
   SHB_CUDA(cudaStreamSynchronize(g->ctx->stream));
@@ -700,7 +725,7 @@ shb_status shb_gbuffer_dims(const shb_gbuffer* g, int32_t* width, int32_t* heigh
 shb_status shb_gbuffer_destroy(shb_gbuffer* g) {
   if (!g) return SHB_OK;
   shb_context* c = g->ctx;
-  cudaSetDevice(c->device);
+  ::shb::DeviceScope _shb_device_scope(c->device);
   cudaStreamSynchronize(c->stream);
   delete g;
   ctx_release(c);
@@ -709,7 +734,7 @@ shb_status shb_gbuffer_destroy(shb_gbuffer* g) {
 
 shb_status shb_validity_mask(shb_context* ctx, const shb_gbuffer* g, uint8_t* mask_out, int32_t device_ptr) {
   if (!ctx || !g || !mask_out) return bad("NULL argument");
-  SHB_CUDA(cudaSetDevice(ctx->device));
+  SHB_ON_DEVICE(ctx->device);
   int64_t n = (int64_t)g->width * g->height;
   uint8_t* d = mask_out;
   if (!device_ptr) {
@@ -726,7 +751,7 @@ shb_status shb_downsample_validity_mask(shb_context* ctx, const uint8_t* in, int
                                         int32_t scale, uint8_t* out, int32_t device_ptrs) {
   if (!ctx || !in || !out) return bad("NULL argument");
   if (width <= 0 || height <= 0 || scale <= 0) return bad("width, height and scale must be positive");
-  SHB_CUDA(cudaSetDevice(ctx->device));
+  SHB_ON_DEVICE(ctx->device);
   size_t nin = (size_t)width * scale * height * scale, nout = (size_t)width * height;
   const uint8_t* din = in;
   uint8_t* dout = out;
@@ -753,7 +778,7 @@ shb_status shb_bake(shb_scene* s, const shb_gbuffer* g, const shb_raster_config*
   int64_t W = (int64_t)rc->width * rc->supersample_scale, H = (int64_t)rc->height * rc->supersample_scale;
   if (W != g->width || H != g->height) return bad("G-buffer size does not match raster_config (W*s x H*s)");
   if (s->bvh_depth > 64) return bad("BVH deeper than the traversal stack");
-  SHB_CUDA(cudaSetDevice(s->ctx->device));
+  SHB_ON_DEVICE(s->ctx->device);
   shb_context* c = s->ctx;
   uint64_t l0 = c->launches;
   size_t n = (size_t)W * H;
@@ -783,7 +808,7 @@ shb_status shb_save_sh_lightmap(shb_context* ctx, const float* sh, const float* 
   if (!ctx || !sh || !path || !*path) return bad("NULL argument");
   if (width <= 0 || height <= 0) return bad("Invalid SHTexture dimensions or empty pixels.");
   if (mode < SHB_SAVE_COMBINED || mode > SHB_SAVE_LUMINANCE_PACKED) return bad("unknown save mode");
-  SHB_CUDA(cudaSetDevice(ctx->device));
+  SHB_ON_DEVICE(ctx->device);
   const size_t n = (size_t)width * height;
   const float* dsh = sh;
   const float* denv = env;
@@ -808,7 +833,7 @@ shb_status shb_sh_preview(shb_context* ctx, const float* sh, int32_t width, int3
   if (width <= 0 || height <= 0) return bad("empty image");
   if (mode < SHB_PREVIEW_L0 || mode > SHB_PREVIEW_SH_PACKED) return bad("unknown preview mode");
   if (mode != SHB_PREVIEW_L0 && !normals && !direction) return bad("a direction or normals is needed");
-  SHB_CUDA(cudaSetDevice(ctx->device));
+  SHB_ON_DEVICE(ctx->device);
   const size_t n = (size_t)width * height;
   const size_t in_floats = 27 * n + (normals ? 3 * n : 0);
   SHB_TRY(ctx->scratch[27].reserve(sizeof(float) * in_floats + 3 * n));
@@ -848,7 +873,7 @@ shb_status shb_write_png(const char* path, int32_t width, int32_t height, int32_
 shb_status shb_scene_set_params(shb_scene* s, const float* albedo_rgb, const uint8_t* use_override,
                                 const float* light_intensity) {
   if (!s) return bad("NULL scene");
-  SHB_CUDA(cudaSetDevice(s->ctx->device));
+  SHB_ON_DEVICE(s->ctx->device);
   if (albedo_rgb)
     for (uint32_t m = 0; m < s->mat_count; ++m)
       for (int c = 0; c < 3; ++c)
@@ -888,7 +913,7 @@ shb_status shb_backward(shb_scene* s, const shb_gbuffer* g, const shb_raster_con
   int64_t W = (int64_t)rc->width * rc->supersample_scale, H = (int64_t)rc->height * rc->supersample_scale;
   if (W != g->width || H != g->height) return bad("G-buffer size does not match raster_config (W*s x H*s)");
   if (s->bvh_depth > 64) return bad("BVH deeper than the traversal stack");
-  SHB_CUDA(cudaSetDevice(s->ctx->device));
+  SHB_ON_DEVICE(s->ctx->device);
   shb_context* c = s->ctx;
   uint64_t l0 = c->launches;
   const size_t n = (size_t)W * H;
@@ -919,7 +944,7 @@ shb_status shb_downsample(shb_context* ctx, const float* in, int32_t in_width, i
                           int32_t scale, float* out, int32_t device_ptrs) {
   if (!ctx || !in || !out) return bad("NULL argument");
   if (in_width <= 0 || in_height <= 0 || channels <= 0 || scale <= 0) return bad("sizes must be positive");
-  SHB_CUDA(cudaSetDevice(ctx->device));
+  SHB_ON_DEVICE(ctx->device);
   size_t nin = (size_t)in_width * in_height * channels;
   size_t nout = scale <= 1 ? nin : (size_t)(in_width / scale) * (in_height / scale) * channels;
   const float* din = in;
@@ -944,7 +969,7 @@ shb_status shb_dilate(shb_context* ctx, int32_t kind, int32_t width, int32_t hei
   if (kind < SHB_DILATE_SH9 || kind > SHB_DILATE_U8) return bad("bad dilate kind");
   if (width <= 0 || height <= 0 || passes <= 0) return SHB_OK;  // reference: nothing to do
   if (!pixels || !mask) return bad("NULL argument");
-  SHB_CUDA(cudaSetDevice(ctx->device));
+  SHB_ON_DEVICE(ctx->device);
   size_t n = (size_t)width * height;
   size_t pbytes = n * (kind == SHB_DILATE_SH9 ? 27 * 4 : (kind == SHB_DILATE_F32 ? 4 : 1));
   void* dp = pixels;
@@ -971,7 +996,7 @@ shb_status shb_bake_pipeline(shb_scene* s, const shb_pipeline_config* cfg, float
   if (!s || !cfg || !sh_out || !env_out) return bad("NULL argument");
   if (cfg->width <= 0 || cfg->height <= 0 || cfg->supersample_scale <= 0) return bad("sizes must be positive");
   shb_context* c = s->ctx;
-  SHB_CUDA(cudaSetDevice(c->device));
+  SHB_ON_DEVICE(c->device);
   const int ss = cfg->supersample_scale;
   shb_raster_config rc{cfg->width, cfg->height, ss};
   if (!c->pipe_gbuf) c->pipe_gbuf = new shb_gbuffer();
@@ -1024,7 +1049,7 @@ shb_status shb_find_occlusion(shb_scene* s, const shb_ray* rays, int64_t count, 
   if (!s || (count > 0 && (!rays || !hits))) return bad("NULL argument");
   if (count <= 0) return SHB_OK;
   shb_context* c = s->ctx;
-  SHB_CUDA(cudaSetDevice(c->device));
+  SHB_ON_DEVICE(c->device);
   const shb_ray* dr = rays;
   shb_hit* dh = hits;
   if (!device_ptrs) {

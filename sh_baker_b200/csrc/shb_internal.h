@@ -27,6 +27,36 @@ shb_status cuda_fail(cudaError_t e, const char* what);
     if (_e != cudaSuccess) return ::shb::cuda_fail(_e, #call);     \
   } while (0)
 
+// Makes `dev` the calling thread's current device for the rest of the
+// scope and gives the thread its previous current device back on exit, so
+// that entry points of the C ABI leave the caller's device selection as
+// they found it.
+struct DeviceScope {
+  int prev = -1;
+  cudaError_t status = cudaSuccess;
+  explicit DeviceScope(int dev) {
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess) cur = -1;
+    if (cur == dev) return;
+    status = cudaSetDevice(dev);
+    if (status == cudaSuccess) prev = cur;
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceScope(const DeviceScope&) = delete;
+  DeviceScope& operator=(const DeviceScope&) = delete;
+};
+
+// DeviceScope for the rest of the enclosing function; returns SHB_ERR_CUDA
+// when the device cannot be made current.
+#define SHB_ON_DEVICE(dev)                                                       \
+  ::shb::DeviceScope _shb_device_scope(dev);                                     \
+  do {                                                                           \
+    if (_shb_device_scope.status != cudaSuccess)                                 \
+      return ::shb::cuda_fail(_shb_device_scope.status, "cudaSetDevice");        \
+  } while (0)
+
 #define SHB_TRY(call)                      \
   do {                                     \
     shb_status _s = (call);                \
@@ -206,6 +236,10 @@ struct shb_gbuffer {
 
 namespace shb {
 
+// Streaming multiprocessors of the calling thread's current device (cached
+// per device); grids of the grid-stride kernels are sized in multiples of it.
+int sm_count();
+
 // launch bookkeeping
 inline void count_launch(shb_context* c, uint64_t n = 1) { c->launches += n; }
 
@@ -249,6 +283,9 @@ struct BatchParams {
 
 shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs, const BatchParams& prm,
                              shb_bake_stats* stats);
+// Looks up the device address of shb_dilate_noalloc's fixed scratch array
+// on `device` (current) and caches it (raster.cu).
+shb_status noalloc_prepare(int device);
 shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n, shb_hit* d_hits);
 // SaveSHLightMap (exr.cu): device SH (27 f32) and env (f32, nullable) texels.
 shb_status save_sh_lightmap_device(shb_context* c, const float* d_sh, const float* d_env, int W, int H,

@@ -393,7 +393,7 @@ void launch_shadow(cudaStream_t st, int grid, const BakeItem* bakes, int n_bakes
 void launch_closest_rays(cudaStream_t st, const BvhView& bvh, const shb_ray* rays, int64_t n, float4* hits, int* err) {
   if (n <= 0) return;
   int64_t g = (n + 127) / 128;
-  if (g > 148 * 16) g = 148 * 16;
+  if (g > sm_count() * 16) g = sm_count() * 16;
   k_closest_rays<<<(int)g, 128, 0, st>>>(bvh, rays, n, hits, err);
 }
 

@@ -6,7 +6,9 @@ implicit synchronisation is not acceptable) cannot let the library
 allocate.  This entry point keeps its scratch in a fixed array inside the
 library; the test calls it through the C ABI on device buffers the test
 allocates, twice in a row, and checks each result byte for byte against the
-existing shb_dilate entry point (the tolerance the dilation tests use).
+existing shb_dilate entry point (the tolerance the dilation tests use).  It
+also checks that a call takes no device memory and leaves the calling
+thread's current device as it was.
 
 The file name sorts last so that a run stopping at the first failure has
 already run every other test.
@@ -60,6 +62,24 @@ def test_noalloc_matches_dilate_two_calls(gpu_ctx, kind, w, h, passes):
         assert got_p.tobytes() == ref_p.tobytes(), f"pixels differ on call {call}"
 
 
+def test_noalloc_takes_no_device_memory(gpu_ctx):
+    import torch
+    w, h, passes = 300, 200, 6
+    px, mask = inputs(A.DILATE_SH9, w, h, 0.1, 5)
+    dp = torch.from_numpy(px).cuda()
+    dm = torch.from_numpy(mask).cuda()
+    args = (gpu_ctx.h, A.DILATE_SH9, w, h, C.c_void_p(dp.data_ptr()), C.c_void_p(dm.data_ptr()), passes)
+    A.check(gpu_ctx.lib.shb_dilate_noalloc(*args))  # warm-up: kernels loaded
+    torch.cuda.synchronize()
+    free_before, _ = torch.cuda.mem_get_info()
+    dev_before = torch.cuda.current_device()
+    A.check(gpu_ctx.lib.shb_dilate_noalloc(*args))
+    torch.cuda.synchronize()
+    free_after, _ = torch.cuda.mem_get_info()
+    assert free_after >= free_before, f"the call took {free_before - free_after} bytes of device memory"
+    assert torch.cuda.current_device() == dev_before
+
+
 def test_noalloc_rejects_sizes_beyond_the_array(gpu_ctx):
     import torch
     w = h = 512  # 512*512 SH9 texels need ~27 MiB, the array holds 16 MiB
@@ -68,4 +88,10 @@ def test_noalloc_rejects_sizes_beyond_the_array(gpu_ctx):
     st = gpu_ctx.lib.shb_dilate_noalloc(gpu_ctx.h, A.DILATE_SH9, w, h, C.c_void_p(dp.data_ptr()),
                                         C.c_void_p(dm.data_ptr()), 2)
     assert st == 1  # SHB_ERR_INVALID_ARG
+    assert b"fixed array" in gpu_ctx.lib.shb_last_error()
+    # sizes whose byte counts would overflow are rejected before they are formed
+    big = 1 << 30
+    st = gpu_ctx.lib.shb_dilate_noalloc(gpu_ctx.h, A.DILATE_SH9, big, big, C.c_void_p(dp.data_ptr()),
+                                        C.c_void_p(dm.data_ptr()), 2)
+    assert st == 1
     assert b"fixed array" in gpu_ctx.lib.shb_last_error()
