@@ -61,16 +61,24 @@ def bytes_per_ray(n_tris: int) -> int:
     return L * 80 + 4 * 48
 
 
-def dram_bytes_per_ray(kind: str, kernel: str):
-    """ncu DRAM bytes (read + write) per ray of a traversal kernel, from the
-    committed summary of the small case of the same scene
-    (profiles/traversal_dram_<kind>_small.md); None when absent."""
+def traversal_profile(kind: str, kernel: str):
+    """Per-ray ncu figures of a traversal kernel from the committed summary
+    of the small case of the same scene (profiles/traversal_<kind>_small.md,
+    its table row `| closest_hit | ... |`): DRAM bytes, L2 bytes and warp
+    instructions per ray and active lanes per warp instruction.  None when
+    absent.  The per-ray figures do not depend on the lightmap size, so they
+    are scaled by the live ray counts of the full workload."""
     import re
-    p = ROOT / "profiles" / f"traversal_dram_{kind}_small.md"
+    p = ROOT / "profiles" / f"traversal_{kind}_small.md"
     if not p.exists():
         return None
-    m = re.search(rf"^\| {kernel} \|.*\| ([0-9.]+) \|$", p.read_text(), re.M)
-    return float(m.group(1)) if m else None
+    m = re.search(rf"^\| {kernel} \| ([0-9.]+) \| ([0-9.]+) \| ([0-9.]+) \| ([0-9.]+) \| ([0-9.]+) \|$",
+                  p.read_text(), re.M)
+    if not m:
+        return None
+    rays, dram, l2, inst, lanes = (float(g) for g in m.groups())
+    return {"profiled_rays": int(rays), "dram_bytes_per_ray": dram, "l2_bytes_per_ray": l2,
+            "warp_inst_per_ray": inst, "active_lanes": lanes, "source": f"profiles/{p.name}"}
 
 
 def measured_peak():
@@ -222,27 +230,24 @@ def pinned_scene(scene, pin):
     return s
 
 
-def run_batched(args):
+def batched_result(steps: int, warmup: int):
     """64 independent procedural rooms (1k-100k triangles, 128^2-1024^2,
     32-256 spp, 2-4 bounces, 1-8 point lights): one shb_bake_batch (CUDA
     graph, autotuned launch structure) per step versus the same 64 bakes
     through the plain shb_bake path one at a time.  Scenes are uploaded and
-    rasterised once, untimed, for both."""
+    rasterised once, untimed, for both; the first warm-up call tunes."""
     import tempfile
 
     import torch
 
-    from sh_baker_b200 import api
-    from sh_baker_b200 import build as B
-    from sh_baker_b200 import scenes
-    B.build()
+    from sh_baker_b200 import api, scenes
     torch.cuda.set_device(0)
     mix = scenes.batched_mix(seed=4, n=64)
     ctx = api.Context(device=0)
     stream = torch.cuda.Stream()
     ctx.set_stream(stream.cuda_stream)
     bakes, outs = [], []
-    for i, m in enumerate(mix):
+    for m in mix:
         ds = api.DeviceScene(ctx, m["scene"])
         rc = api.RasterConfig(m["width"], m["height"], 1)
         g = api.rasterize_to_device(ds, rc)
@@ -251,7 +256,7 @@ def run_batched(args):
         outs.append((torch.empty(n * 27, dtype=torch.float32, device="cuda"),
                      torch.empty(n, dtype=torch.float32, device="cuda")))
     tune = str(Path(tempfile.mkdtemp()) / "autotune.txt")
-    for _ in range(args.warmup):  # the first batched call tunes and caches
+    for _ in range(max(warmup, 1)):  # the first batched call tunes and caches
         api.bake_batch(ctx, bakes, use_graph=True, autotune=True, tune_cache=tune, outputs=outs)
     for b, (sh, env) in zip(bakes, outs):
         api.bake_plain_device(b, sh, env)
@@ -270,51 +275,58 @@ def run_batched(args):
     clocks.start()
     l0 = ctx.kernel_launches()
     b_ms, ts = 0.0, 0
-    for _ in range(args.steps):
+    for _ in range(steps):
         ms, (_, st) = timed(lambda: api.bake_batch(ctx, bakes, use_graph=True, autotune=True, tune_cache=tune,
                                                    outputs=outs))
         b_ms += ms
         ts += st.texel_samples
     launches = ctx.kernel_launches() - l0
     s_ms = 0.0
-    for _ in range(args.steps):
+    for _ in range(steps):
         ms, _ = timed(lambda: [api.bake_plain_device(b, sh, env) for b, (sh, env) in zip(bakes, outs)])
         s_ms += ms
     clk = clocks.stop()
     tuned = Path(tune).read_text().split()
-    value = ts / (b_ms / 1e3)
-    seq = ts / (s_ms / 1e3)
     tris = [m["scene"].triangle_count for m in mix]
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": b_ms / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "64 procedural rooms, 1k-100k triangles, 128^2-1024^2, 32-256 spp, 2-4 bounces, "
-                                   "1-8 point lights; one persistent launch in a CUDA graph",
-                       "bakes": 64, "triangles_total": int(sum(tris)), "texel_samples_per_step": ts // args.steps},
-            "sequential": {"value": seq, "ms_per_step": s_ms / args.steps},
-            "speedup_vs_sequential": s_ms / b_ms, "autotuned": {"wave_paths": int(tuned[1]),
-                                                                "tile_texels": int(tuned[2]),
-                                                                "grid_scale": int(tuned[3]),
-                                                                "share_paths": int(tuned[4])},
-            "gpu_launches": int(launches), "clocks": clk}
-    print(json.dumps(line), flush=True)
+    res = {"value": ts / (b_ms / 1e3), "ms_per_step": b_ms / steps, "steps": steps, "warmup": warmup,
+           "sequential": {"value": ts / (s_ms / 1e3), "ms_per_step": s_ms / steps},
+           "speedup_vs_sequential": s_ms / b_ms,
+           "autotuned": {"wave_paths": int(tuned[1]), "tile_texels": int(tuned[2]), "grid_scale": int(tuned[3]),
+                         "share_paths": int(tuned[4])},
+           "workload": "64 procedural rooms, 1k-100k triangles, 128^2-1024^2, 32-256 spp, 2-4 bounces, "
+                       "1-8 point lights; shb_bake_batch in a CUDA graph vs 64 plain shb_bake calls",
+           "bakes": 64, "triangles_total": int(sum(tris)), "texel_samples_per_step": ts // steps,
+           "gpu_launches": int(launches), "clocks": clk}
     ctx.close()
+    return res
 
 
-def run_adjoint(args):
+def run_batched(args):
+    from sh_baker_b200 import build as B
+    B.build()
+    r = batched_result(args.steps, args.warmup)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": r["workload"], "bakes": r["bakes"], "triangles_total": r["triangles_total"],
+                       "texel_samples_per_step": r["texel_samples_per_step"]},
+            "sequential": r["sequential"], "speedup_vs_sequential": r["speedup_vs_sequential"],
+            "autotuned": r["autotuned"], "gpu_launches": r["gpu_launches"], "clocks": r["clocks"]}
+    print(json.dumps(line), flush=True)
+
+
+def adjoint_result(steps: int, warmup: int):
     """Adjoint bake: procedural room (2,412 triangles) at lightmap 512^2,
-    supersample 3 (the room workload's), 64 spp, 3 bounces.  Loss = sum (SH - SH_target)^2 with the
-    target baked at albedos x U[0.8, 1.2] and light intensities x U[0.5, 2].
-    A step = forward bake + dLoss/dSH + path-replay backward; both halves are
-    timed with CUDA events.  The gradient of all 8x3 albedos and 5 intensities
-    is compared with central differences (h = 1e-3, common random numbers)."""
+    supersample 3 (the room workload's), 64 spp, 3 bounces.  Loss = sum
+    (SH - SH_target)^2 with the target baked at albedos x U[0.8, 1.2] and
+    light intensities x U[0.5, 2].  A step = forward bake + dLoss/dSH +
+    path-replay backward; both halves are timed with CUDA events.  The
+    gradient of all 8x3 albedos and 5 intensities is compared with central
+    differences (h = 1e-3, common random numbers)."""
     import numpy as np
     import torch
 
-    from oracle.pyoracle import srgb_to_linear
     from sh_baker_b200 import api, scenes
-    from sh_baker_b200 import build as B
-    B.build()
     torch.cuda.set_device(0)
     res, spp, bounces = 512, 64, 3
     sc = scenes.procedural_room(seed=2, res=res)
@@ -325,8 +337,7 @@ def run_adjoint(args):
     rc = api.RasterConfig(res, res, 3)
     g = api.rasterize_to_device(ds, rc)
     bake = api.BatchBake(ds, g, rc, api.BakeConfig(samples=spp, bounces=bounces, seed=2))
-    lut = np.array([srgb_to_linear(i) for i in range(256)], np.float32)
-    albedo = np.stack([lut[m.albedo.pixel_data[:3]] for m in sc.materials]).astype(np.float32)
+    albedo = api.material_linear_albedo(sc)
     inten = np.array([l.intensity for l in sc.lights], np.float32)
     rng = np.random.default_rng(5)
     n = g.width * g.height
@@ -353,23 +364,22 @@ def run_adjoint(args):
         torch.cuda.synchronize()
         return e0.elapsed_time(e1), e1.elapsed_time(e2), st.texel_samples, (d_alb, d_li)
 
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         step()
     clocks = ClockSampler(0)
     clocks.start()
     l0 = ctx.kernel_launches()
     f_ms = b_ms = 0.0
     ts = 0
-    for _ in range(args.steps):
+    for _ in range(steps):
         fm, bm, t, grads = step()
         f_ms += fm
         b_ms += bm
         ts += t
     launches = ctx.kernel_launches() - l0
     clk = clocks.stop()
-    # central differences under common random numbers (same seed)
 
-    def loss(a, i):
+    def loss(a, i):  # central differences under common random numbers (same seed)
         ds.set_params(a, i)
         with torch.cuda.stream(stream):
             api.bake_plain_device(bake, sh, env)
@@ -396,18 +406,29 @@ def run_adjoint(args):
     fd = np.concatenate([fd_alb.reshape(-1), fd_li * inten])
     rel = float(np.linalg.norm(got - fd) / np.linalg.norm(fd))
     worst = float(np.max(np.abs(got - fd)) / np.max(np.abs(fd)))
-    line = {"metric": METRIC, "value": ts / (b_ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": (f_ms + b_ms) / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "adjoint bake: procedural room 2,412 triangles, lightmap 512x512, supersample 3, "
-                                   "64 spp, 3 bounces; loss sum (SH - SH_target)^2, 8x3 albedos + 5 intensities",
-                       "texel_samples_per_step": ts // args.steps},
-            "forward_ms": f_ms / args.steps, "backward_ms": b_ms / args.steps,
-            "backward_over_forward": b_ms / f_ms,
-            "fd_check": {"h": h, "rel_l2_err": rel, "max_err_over_max": worst},
-            "gpu_launches": int(launches), "clocks": clk}
-    print(json.dumps(line), flush=True)
+    out = {"value": ts / (b_ms / 1e3), "ms_per_step": (f_ms + b_ms) / steps, "steps": steps, "warmup": warmup,
+           "workload": "adjoint bake: procedural room 2,412 triangles, lightmap 512x512, supersample 3, 64 spp, "
+                       "3 bounces; loss sum (SH - SH_target)^2, 8x3 albedos + 5 intensities",
+           "texel_samples_per_step": ts // steps, "forward_ms": f_ms / steps, "backward_ms": b_ms / steps,
+           "backward_over_forward": b_ms / f_ms, "fd_rel_l2": rel,
+           "fd_check": {"h": h, "rel_l2_err": rel, "max_err_over_max": worst},
+           "gpu_launches": int(launches), "clocks": clk}
     ctx.close()
+    return out
+
+
+def run_adjoint(args):
+    from sh_baker_b200 import build as B
+    B.build()
+    r = adjoint_result(args.steps, args.warmup)
+    line = {"metric": METRIC, "value": r["value"], "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": r["workload"], "texel_samples_per_step": r["texel_samples_per_step"]},
+            "forward_ms": r["forward_ms"], "backward_ms": r["backward_ms"],
+            "backward_over_forward": r["backward_over_forward"], "fd_check": r["fd_check"],
+            "gpu_launches": r["gpu_launches"], "clocks": r["clocks"]}
+    print(json.dumps(line), flush=True)
 
 
 def accuracy(w, scene, ctx):
@@ -546,17 +567,109 @@ def run_exr(args):
     print(json.dumps(line), flush=True)
 
 
+def roofline_of(stats, steps, scene, w, ms, clk):
+    """Roofline of the dominant traversal kernel.  Traversal of incoherent
+    rays is bound by instruction issue (dependent node fetches hit L1/L2,
+    ncu shows ~80 % issue activity and DRAM traffic < 10 % of the model's
+    bytes), so the bound reported is issue: warp instructions per ray (ncu,
+    small case of the same scene) x rays traced / kernel time, against the
+    SMs' issue slots (SMs x 4 schedulers x median SM clock under load).  The
+    model-byte HBM figure (SURVEY-style algorithmic bytes per ray over the
+    measured copy bandwidth) is kept beside it as `hbm_model`."""
+    import torch
+    ext_ms = sum(s.extend_kernel_ms for s in stats)
+    sh_ms = sum(s.shadow_kernel_ms for s in stats)
+    ext_rays = sum(s.extend_rays for s in stats)
+    sh_rays = sum(s.shadow_rays for s in stats)
+    bpr = bytes_per_ray(scene.triangle_count)
+    dom = "closest_hit" if ext_ms >= sh_ms else "any_hit"
+    k_ms, k_rays = (ext_ms, ext_rays) if dom == "closest_hit" else (sh_ms, sh_rays)
+    k_launch = sum((s.extend_launches if dom == "closest_hit" else s.shadow_launches) for s in stats)
+    rays_per_launch = k_rays / max(k_launch, 1)
+    hbm_achieved = k_rays * bpr / (k_ms / 1e3) / 1e9 if k_ms > 0 else 0.0
+    peak, peak_kind = measured_peak()
+    prof = traversal_profile(w["kind"], dom)
+    sms = torch.cuda.get_device_properties(torch.cuda.current_device()).multi_processor_count
+    mhz = (clk or {}).get("sm_mhz") or (clk or {}).get("sm_max_mhz") or 1965.0
+    issue_peak = sms * 4 * mhz * 1e6 / 1e9  # G warp instructions / s
+    roof = {"kernel": dom, "bound": "issue", "unit": "G warp-inst/s",
+            "peak": issue_peak, "peak_source": f"{sms} SMs x 4 schedulers x {mhz:.0f} MHz (median SM clock sampled "
+                                              "during the timed region)",
+            "achieved": None, "frac": None, "traffic": None,
+            "rays_per_launch": rays_per_launch, "launch_ms": k_ms / max(k_launch, 1),
+            "kernel_ms": {"closest_hit": ext_ms / steps, "any_hit": sh_ms / steps,
+                          "shade": sum(s.shade_kernel_ms for s in stats) / steps},
+            "rays_per_s": (ext_rays + sh_rays) / (ms / 1e3),
+            "hbm_model": {"bytes_per_ray": bpr, "achieved": hbm_achieved, "peak": peak, "unit": "GB/s",
+                          "frac": hbm_achieved / peak, "peak_source": peak_kind}}
+    if prof:
+        inst = prof["warp_inst_per_ray"] * k_rays / (k_ms / 1e3) / 1e9 if k_ms > 0 else 0.0
+        roof.update({"achieved": inst, "frac": inst / issue_peak,
+                     "traffic": prof["dram_bytes_per_ray"] * rays_per_launch,
+                     "warp_inst_per_ray": prof["warp_inst_per_ray"], "active_lanes": prof["active_lanes"],
+                     "l2_bytes_per_ray": prof["l2_bytes_per_ray"], "dram_bytes_per_ray": prof["dram_bytes_per_ray"],
+                     "profile": prof["source"]})
+    return roof
+
+
+def accuracy_at_fixture_spp(w, scene, ctx):
+    """The bake of the FP64 fixture's crop at the fixture's own spp (4096):
+    relative RMSE against the fixture, the noise floor two independent
+    4096-spp estimates have (sqrt 2 x the fixture's own error), the
+    systematic part left after that noise is taken out, and the GPU rate of
+    that bake (CUDA events, BVH already built)."""
+    import numpy as np
+    import torch
+
+    from sh_baker_b200 import _capi as A
+    from sh_baker_b200 import api
+    path = ROOT / "tests" / "golden" / f"fp64_{w['kind']}.npz"
+    if not path.exists():
+        return None
+    ref = np.load(path)
+    W, H, ss, size, x0, y0 = (int(ref[k]) for k in ("width", "height", "ss", "size", "x0", "y0"))
+    if (W, H, ss, int(ref["bounces"])) != (w["width"], w["height"], w["ss"], w["bounces"]):
+        return None
+    spp = int(ref["spp"])
+    pts = api.RasterizeScene(scene, api.RasterConfig(W, H, ss), ctx=ctx).reshape(H * ss, W * ss)
+    crop = np.ascontiguousarray(pts[y0 * ss:(y0 + size) * ss, x0 * ss:(x0 + size) * ss]).reshape(-1)
+    ds = api.DeviceScene(ctx, scene)
+    g = api.GBuffer.from_points(ctx, crop, size * ss, size * ss)
+    rc = api.RasterConfig(size, size, ss)
+    n = (size * ss) ** 2
+    sh = torch.empty(n * 27, dtype=torch.float32, device="cuda")
+    env = torch.empty(n, dtype=torch.float32, device="cuda")
+    bake = api.BatchBake(ds, g, rc, api.BakeConfig(samples=spp, bounces=w["bounces"], seed=4242))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    st = api.bake_plain_device(bake, sh, env)
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    got = sh.cpu().numpy().reshape(size, ss, size, ss, 27).mean(axis=(1, 3))
+    valid, r = ref["valid"], ref["sh"].astype(np.float64)
+    d2 = float(np.sum((got - r)[valid] ** 2))
+    o2 = float(np.sum(r[valid] ** 2))
+    se2 = float(np.sum(ref["se"].astype(np.float64)[valid] ** 2))
+    g.close()
+    ds.close()
+    return {"spp": spp, "rel_rmse_vs_fp64": (d2 / o2) ** 0.5, "noise_floor": (2 * se2 / o2) ** 0.5,
+            "systematic_est": max(0.0, d2 - 2 * se2) ** 0.5 / o2 ** 0.5,
+            "texel_samples_per_s": st.texel_samples / dt, "seconds": dt}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="room", choices=sorted(WORKLOADS) + ["batched", "adjoint", "exr"])
+    ap.add_argument("--workload", default="atrium", choices=sorted(WORKLOADS) + ["batched", "adjoint", "exr"])
     ap.add_argument("--cpu-seconds", type=float, default=15.0)
     ap.add_argument("--ref-step-seconds", type=float, default=5.0)
+    ap.add_argument("--e2e-steps", type=int, default=3, help="timed end-to-end steps (after one warm-up)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-sub", action="store_true", help="skip the batched and adjoint sub-results")
     args = ap.parse_args()
     if args.workload in ("batched", "adjoint", "exr"):
         if args.impl == "ours" and int(os.environ.get("RANK", "0")) == 0:
@@ -629,27 +742,9 @@ def main():
     clk = clocks.stop()
     ts = sum(s.texel_samples for s in stats)
     ms, ts, value = job_rate(ms, ts, dist)
-
-    # roofline of the dominant kernel (closest-hit or any-hit traversal)
-    ext_ms = sum(s.extend_kernel_ms for s in stats)
-    sh_ms = sum(s.shadow_kernel_ms for s in stats)
+    roof = roofline_of(stats, args.steps, scene, w, ms, clk)
     ext_rays = sum(s.extend_rays for s in stats)
     sh_rays = sum(s.shadow_rays for s in stats)
-    bpr = bytes_per_ray(scene.triangle_count)
-    dom = "closest_hit" if ext_ms >= sh_ms else "any_hit"
-    k_ms, k_rays = (ext_ms, ext_rays) if dom == "closest_hit" else (sh_ms, sh_rays)
-    k_launch = sum((s.extend_launches if dom == "closest_hit" else s.shadow_launches) for s in stats)
-    achieved = k_rays * bpr / (k_ms / 1e3) / 1e9 if k_ms > 0 else 0.0
-    peak, peak_kind = measured_peak()
-    per_ray = dram_bytes_per_ray(w["kind"], dom)
-    traffic = per_ray * (k_rays / max(k_launch, 1)) if per_ray else None
-    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": dom, "peak_source": peak_kind,
-            "bytes_per_ray": bpr, "rays_per_launch": k_rays / max(k_launch, 1),
-            "launch_ms": k_ms / max(k_launch, 1),
-            "kernel_ms": {"closest_hit": ext_ms / args.steps, "any_hit": sh_ms / args.steps,
-                          "shade": sum(s.shade_kernel_ms for s in stats) / args.steps},
-            "rays_per_s": (ext_rays + sh_rays) / (ms / 1e3)}
 
     # end to end through the public API from pinned host memory
     e2e = None
@@ -662,7 +757,8 @@ def main():
         desc, keep = pack_scene(pscene)
         h2d = sum(a.nbytes for a in keep if isinstance(a, np.ndarray))
         e_times, e_ts = [], 0
-        for i in range(args.warmup + args.steps):
+        e_steps = max(1, min(args.steps, args.e2e_steps))
+        for i in range(1 + e_steps):
             ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             torch.cuda.synchronize()
             ea.record(stream)
@@ -675,18 +771,21 @@ def main():
             lib.shb_scene_destroy(h)
             eb.record(stream)
             torch.cuda.synchronize()
-            if i >= args.warmup:
+            if i >= 1:
                 e_times.append(ea.elapsed_time(eb))
                 e_ts += st.texel_samples
         e_ms, e_ts, e_val = job_rate(sum(e_times), e_ts, dist)
         e2e = {"value": e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(o_sh.nbytes + o_env.nbytes + o_mask.nbytes),
-               "ms_per_step": e_ms / args.steps}
+               "ms_per_step": e_ms / e_steps, "steps": e_steps, "warmup": 1,
+               "region": "scene upload from pinned host memory, raster, BVH build, bake, masks, downsample, "
+                         "dilation, read-back of SH, env visibility and mask (shb_bake_pipeline)"}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         pts = g.download()
         cpu = cpu_baseline(scene, pts, w, args.cpu_seconds, os.cpu_count() or 1)
+        del pts
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -699,12 +798,23 @@ def main():
                                     "launches": sum(s.extend_launches for s in stats) // args.steps},
                     "any_hit": {"rays": sh_rays // args.steps,
                                 "launches": sum(s.shadow_launches for s in stats) // args.steps}},
-                "rays_per_texel_sample": (ext_rays + sh_rays) / max(ts, 1),
-                "accuracy": accuracy(w, scene, ctx) if world == 1 else None}
-        print(json.dumps(line), flush=True)
+                "rays_per_texel_sample": (ext_rays + sh_rays) / max(ts, 1)}
     del sh, env
     g.close()
     ds.close()
+    if rank == 0 and world == 1:
+        acc = accuracy(w, scene, ctx)
+        if acc is not None:
+            acc["at_fixture_spp"] = accuracy_at_fixture_spp(w, scene, ctx)
+        line["accuracy"] = acc
+        if not args.no_sub:
+            # the metric's other two parts, shortened: batched vs sequential and adjoint vs forward
+            line["batched"] = batched_result(steps=2, warmup=1)
+            line["adjoint"] = adjoint_result(steps=2, warmup=1)
+    elif rank == 0:
+        line["accuracy"] = None
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
         dist.barrier()

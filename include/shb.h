@@ -44,6 +44,12 @@ extern "C" {
 
 #define SHB_ABI_VERSION 1
 
+/* Every device loop and queue is bounded.  A bounded loop that runs out
+ * (a ray's traversal steps) sets a device error flag and returns; the host
+ * maps it to SHB_ERR_TIMEOUT.  A bounded capacity that is exceeded (the
+ * traversal stack, a ray queue) maps to SHB_ERR_INTERNAL.  Either way the
+ * kernels end, the context stays usable and shb_bake_stats.error_flags
+ * holds the flags (1 stack, 2 queue, 4 traversal steps). */
 typedef enum shb_status {
   SHB_OK = 0,
   SHB_ERR_INVALID_ARG = 1,
@@ -211,6 +217,16 @@ typedef struct shb_gbuffer shb_gbuffer;
 
 SHB_API int32_t shb_abi_version(void);
 SHB_API const char* shb_last_error(void);
+
+/* Test hook (no counterpart in the reference): from now on, the device
+ * allocation the library makes after `n` more successful ones fails with
+ * SHB_ERR_OOM, once; n < 0 turns the hook off.  Host side only: the
+ * allocation is refused before cudaMalloc is called. */
+SHB_API void shb_test_fail_allocation_after(int32_t n);
+
+/* SRGBToLinear (src/colorspace.h:10-14) of every 8-bit value, the table
+ * GetAlbedo (src/material.cpp:69-85) reads: out[256] floats.  Host only. */
+SHB_API void shb_srgb_to_linear_table(float* out);
 SHB_API shb_status shb_context_create(const shb_options* options,
                                       shb_context** out);
 /* Releases the handle and the context's scratch memory.  Scenes and
@@ -303,9 +319,15 @@ typedef struct shb_batch_options {
                            lights + 4 x area lights >= 16), 1 inline in the
                            hit kernel, 2 its own kernel; results are
                            bit-identical either way                        */
-  int32_t reserved[1];
+  int32_t max_traversal_steps; /* bound of the traversal loop of one ray
+                           (0: 4,194,304); a ray that reaches it ends the
+                           bake with SHB_ERR_TIMEOUT                        */
   const char* tune_cache; /* tuning file; NULL: $SHB_TUNE_CACHE or
                              $HOME/.cache/sh_baker_b200/autotune.txt        */
+  int32_t queue_capacity; /* entries of each ray queue (0: sized to the
+                           wave); a smaller capacity drops the rays that do
+                           not fit and ends the bake with SHB_ERR_INTERNAL */
+  int32_t reserved[3];
 } shb_batch_options;
 
 SHB_API shb_status shb_bake_batch(shb_context* ctx, const shb_batch_item* items, int32_t count,

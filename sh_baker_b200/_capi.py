@@ -113,8 +113,8 @@ class BatchItem(C.Structure):
 class BatchOptions(C.Structure):
     _fields_ = [("use_graph", C.c_int32), ("autotune", C.c_int32), ("wave_paths", C.c_int32),
                 ("tile_texels", C.c_int32), ("grid_scale", C.c_int32), ("share_paths", C.c_int32),
-                ("nee_split", C.c_int32), ("reserved", C.c_int32 * 1),
-                ("tune_cache", C.c_char_p)]
+                ("nee_split", C.c_int32), ("max_traversal_steps", C.c_int32),
+                ("tune_cache", C.c_char_p), ("queue_capacity", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class Options(C.Structure):
@@ -132,6 +132,8 @@ vp = C.c_void_p
 SIGNATURES = {
     "shb_abi_version": (C.c_int32, []),
     "shb_last_error": (C.c_char_p, []),
+    "shb_srgb_to_linear_table": (None, [vp]),
+    "shb_test_fail_allocation_after": (None, [C.c_int32]),
     "shb_context_create": (C.c_int, [C.POINTER(Options), C.POINTER(vp)]),
     "shb_context_destroy": (C.c_int, [vp]),
     "shb_context_set_stream": (C.c_int, [vp, vp]),

@@ -293,6 +293,27 @@ def Dilate(width: int, height: int, pixels: np.ndarray, mask: np.ndarray, passes
     A.check(ctx.lib.shb_dilate(ctx.h, kind, width, height, pixels.ctypes.data, mask.ctypes.data, passes, 0))
 
 
+def srgb_to_linear_table() -> np.ndarray:
+    """SRGBToLinear (src/colorspace.h:10-14) of every 8-bit value, as the
+    library computes it for GetAlbedo."""
+    out = np.empty(256, np.float32)
+    A.load().shb_srgb_to_linear_table(out.ctypes.data)
+    return out
+
+
+def material_linear_albedo(scene) -> np.ndarray:
+    """Linear RGB albedo of each material's first albedo texel (the 1x1
+    textures of the procedural scenes): the starting values of the adjoint's
+    base-colour parameters (shb_scene_set_params)."""
+    lut = srgb_to_linear_table()
+    out = np.full((len(scene.materials), 3), 0.8, np.float32)
+    for m, mat in enumerate(scene.materials):
+        px = mat.albedo.pixel_data
+        if px is not None and np.size(px) >= 3:
+            out[m] = lut[np.asarray(px).reshape(-1)[:3]]
+    return out
+
+
 @dataclass
 class BatchBake:
     """One bake of a batch: an uploaded scene, its device G-buffer and the
@@ -305,14 +326,18 @@ class BatchBake:
 
 def bake_batch(ctx: Context, bakes, use_graph: bool = True, autotune: bool = False, tune_cache: Optional[str] = None,
                wave_paths: int = 0, tile_texels: int = 0, grid_scale: int = 0, share_paths: int = 0,
-               nee_split: int = 0, outputs=None):
+               nee_split: int = 0, outputs=None, max_traversal_steps: int = 0, queue_capacity: int = 0,
+               check: bool = True):
     """Runs many bakes in one persistent launch (shb_bake_batch).  Returns
     ([(sh, env)] device tensors of W*s*H*s*27 and W*s*H*s floats, stats).
     `outputs` may supply those tensors (reused across calls).  Bakes of fewer
     than `share_paths` paths share waves, larger ones get their own (0: half
     a wave or the tuned value; -1: no sharing).  `nee_split`: next-event
     estimation as its own kernel by light-loop cost (0), never (1) or
-    always (2); the results do not change."""
+    always (2); the results do not change.  `max_traversal_steps` and
+    `queue_capacity` lower the device bounds (0: defaults).  With
+    check=False a failing status is returned as a third value instead of
+    raised, with the stats of the failed call."""
     import torch
     n = len(bakes)
     items = (A.BatchItem * max(1, n))()
@@ -335,8 +360,13 @@ def bake_batch(ctx: Context, bakes, use_graph: bool = True, autotune: bool = Fal
     opts.share_paths = share_paths
     opts.nee_split = nee_split
     opts.tune_cache = tune_cache.encode() if tune_cache else None
+    opts.max_traversal_steps = max_traversal_steps
+    opts.queue_capacity = queue_capacity
     st = A.BakeStats()
-    A.check(ctx.lib.shb_bake_batch(ctx.h, C.addressof(items), n, C.byref(opts), C.byref(st)))
+    status = ctx.lib.shb_bake_batch(ctx.h, C.addressof(items), n, C.byref(opts), C.byref(st))
+    if not check:
+        return outs, st, status
+    A.check(status)
     return outs, st
 
 

@@ -236,6 +236,16 @@ extern "C" shb_status shb_bake_batch(shb_context* ctx, const shb_batch_item* ite
   if (options && options->share_paths > 0) prm.share_paths = options->share_paths;
   if (options && options->share_paths < 0) prm.share_paths = 0;
   if (options && options->nee_split >= 0 && options->nee_split <= 2) prm.nee_split = options->nee_split;
+  if (options && options->max_traversal_steps < 0) {
+    set_error("max_traversal_steps must not be negative");
+    return SHB_ERR_INVALID_ARG;
+  }
+  if (options && options->queue_capacity < 0) {
+    set_error("queue_capacity must not be negative");
+    return SHB_ERR_INVALID_ARG;
+  }
+  if (options) prm.max_iters = (uint32_t)options->max_traversal_steps;
+  if (options) prm.queue_cap = options->queue_capacity;
   uint64_t l0 = ctx->launches;
   SHB_TRY(bake_batch_device(ctx, specs, prm, stats));
   if (stats) stats->kernel_launches = ctx->launches - l0;

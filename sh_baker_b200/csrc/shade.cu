@@ -1155,6 +1155,15 @@ shb_status build_area_tris(shb_scene* s) {
   return SHB_OK;
 }
 
+// Status of a bake or query whose kernels raised device error flags: a
+// bounded loop that ran out is SHB_ERR_TIMEOUT, an exceeded capacity
+// SHB_ERR_INTERNAL.
+shb_status device_error(int err) {
+  set_error(std::string("bounded device failure:") + (err & ERR_STACK ? " traversal stack overflow" : "") +
+            (err & ERR_QUEUE ? " ray queue overflow" : "") + (err & ERR_ITER ? " traversal step limit reached" : ""));
+  return (err & (ERR_STACK | ERR_QUEUE)) ? SHB_ERR_INTERNAL : SHB_ERR_TIMEOUT;
+}
+
 shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n, shb_hit* d_hits) {
   shb_context* c = s->ctx;
   if (n <= 0) return SHB_OK;
@@ -1170,10 +1179,7 @@ shb_status find_occlusion_device(shb_scene* s, const shb_ray* d_rays, int64_t n,
   int err = 0;
   SHB_CUDA(cudaMemcpyAsync(&err, cnt + CNT_ERROR, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   SHB_CUDA(cudaStreamSynchronize(c->stream));
-  if (err) {
-    set_error("traversal stack overflow");
-    return SHB_ERR_INTERNAL;
-  }
+  if (err) return device_error(err);
   return SHB_OK;
 }
 
@@ -1344,8 +1350,12 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   plan_waves(specs, n_valid, wave_paths, prm.tile_texels, share, tiles, waves);
   int64_t Pmax = 0;
   for (const Wave& w : waves) Pmax = std::max(Pmax, w.P);
-  const int64_t ext_cap = std::max<int64_t>(Pmax * mult, 1);
-  const int64_t sh_cap = (Pmax + ext_cap) * NLS;
+  int64_t ext_cap = std::max<int64_t>(Pmax * mult, 1);
+  int64_t sh_cap = (Pmax + ext_cap) * NLS;
+  if (prm.queue_cap > 0) {  // a smaller queue drops what does not fit (ERR_QUEUE)
+    ext_cap = std::min(ext_cap, prm.queue_cap);
+    sh_cap = std::min(sh_cap, prm.queue_cap);
+  }
   if (ext_cap > INT32_MAX || sh_cap > INT32_MAX) {
     set_error("wave too large");
     return SHB_ERR_INVALID_ARG;
@@ -1477,7 +1487,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       cudaMemsetAsync(cnt + CNT_FETCH_EXT, 0, sizeof(int) * 2, st);
       Pair pe = stamp(0);
       launch_extend(st, tgrid, bk, nbk, a.info, a.ext[cur], cnt + cur, a.ext_cap, a.hits, cnt + CNT_FETCH_EXT,
-                    cnt + CNT_ERROR, c64);
+                    cnt + CNT_ERROR, c64, prm.max_iters);
       close_stamp(pe);
       Pair pd = stamp(2);
       if (bwd) {
@@ -1493,7 +1503,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       close_stamp(pd);
       Pair ps = stamp(1);
       launch_shadow(st, tgrid, bk, nbk, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, a.pend,
-                    cnt + CNT_FETCH_SHADOW, cnt + CNT_ERROR, c64);
+                    cnt + CNT_FETCH_SHADOW, cnt + CNT_ERROR, c64, prm.max_iters);
       close_stamp(ps);
       if (bwd) {
         k_apply<<<sgrid, kThreads, gsmem, st>>>(a);
@@ -1571,11 +1581,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
     stats->extend_launches = ext_launches;
     stats->shadow_launches = sh_launches;
   }
-  if (err) {
-    set_error(std::string("bounded device failure:") + (err & ERR_STACK ? " traversal stack overflow" : "") +
-              (err & ERR_QUEUE ? " ray queue overflow" : "") + (err & ERR_ITER ? " traversal iteration limit" : ""));
-    return SHB_ERR_INTERNAL;
-  }
+  if (err) return device_error(err);
   return SHB_OK;
 }
 

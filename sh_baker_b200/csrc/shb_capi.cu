@@ -128,10 +128,18 @@ void ctx_release(shb_context* c) {
   if (last) cache_flush(-1);
 }
 
+// shb_test_fail_allocation_after: allocations left before one is refused
+// (negative: off).
+std::atomic<int> g_fail_alloc_countdown{-1};
+
 shb_status DevBuf::reserve(size_t n) {
   if (n <= bytes && ptr) return SHB_OK;
   release();
   if (n == 0) n = 16;
+  if (g_fail_alloc_countdown.load() >= 0 && g_fail_alloc_countdown.fetch_sub(1) == 0) {
+    set_error("device allocation of " + std::to_string(n) + " bytes refused (shb_test_fail_allocation_after)");
+    return SHB_ERR_OOM;
+  }
   int d = 0;
   SHB_CUDA(cudaGetDevice(&d));
   if (cache_take(d, n, &ptr, &bytes)) {
@@ -334,6 +342,12 @@ extern "C" {
 int32_t shb_abi_version(void) { return SHB_ABI_VERSION; }
 
 const char* shb_last_error(void) { return g_last_error.c_str(); }
+
+void shb_test_fail_allocation_after(int32_t n) { shb::g_fail_alloc_countdown.store(n < 0 ? -1 : n); }
+
+void shb_srgb_to_linear_table(float* out) {
+  if (out) srgb_table(out);
+}
 
 shb_status shb_context_create(const shb_options* options, shb_context** out) {
   if (!out) return bad("out is NULL");

@@ -274,6 +274,8 @@ struct BatchParams {
   int64_t share_paths = -1;               // bakes of fewer paths share waves (-1: wave_paths / 2)
   int nee_split = 0;                      // next-event kernel: 0 by light-loop cost, 1 inline, 2 separate
   bool use_graph = false;                 // capture the waves in one CUDA graph
+  uint32_t max_iters = 0;                 // traversal steps of one ray (0: default)
+  int64_t queue_cap = 0;                  // entries per ray queue (0: sized to the wave)
   // Path-replay adjoint instead of the forward bake (one bake): gradients of
   // sum(dsh * SH) accumulate into grad[3 * mat_count + light_count] (device,
   // zeroed by the call).

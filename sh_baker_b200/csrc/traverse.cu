@@ -36,7 +36,7 @@ constexpr int kTravThreads = 128;
 #endif
 constexpr int kPostpone = SHB_POSTPONE;  // fewer lanes than this on triangles: postpone them
 constexpr uint32_t kNodeGroup = 0x80000000u;
-constexpr uint32_t kMaxIters = 1u << 22;
+constexpr uint32_t kMaxIters = 1u << 22;  // default bound of one ray's traversal steps
 
 struct TravRay {
   float ox, oy, oz, dx, dy, dz;
@@ -193,8 +193,8 @@ __device__ __forceinline__ void intersect_node(const BvhView& bvh, const Walk& w
 // One step: visit one node (or take a popped triangle group) and test the
 // current triangle group.  Returns true when the ray is finished.
 template <bool ANY>
-__device__ __forceinline__ bool walk_step(const BvhView& bvh, Walk& w, uint2* stack, int* err) {
-  if (++w.iters > kMaxIters) {
+__device__ __forceinline__ bool walk_step(const BvhView& bvh, Walk& w, uint2* stack, int* err, uint32_t max_iters) {
+  if (++w.iters > max_iters) {
     atomicOr(err, ERR_ITER);
     return true;
   }
@@ -264,7 +264,8 @@ __device__ __forceinline__ void load_ray(TravRay& r, float4 o, float4 d) {
 // Persistent queue consumer: lanes refill from the queue as their rays end.
 // `bvh_of(i, o, d)` gives the BVH of queue entry i (its bake's).
 template <bool SHADOW, class Q, class B, class Fin>
-__device__ __forceinline__ void consume(const Q& q, int n, int* fetch, int* err, B&& bvh_of, Fin&& finish) {
+__device__ __forceinline__ void consume(const Q& q, int n, int* fetch, int* err, uint32_t max_iters, B&& bvh_of,
+                                       Fin&& finish) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   uint2 stack[kStack];
@@ -295,7 +296,7 @@ __device__ __forceinline__ void consume(const Q& q, int n, int* fetch, int* err,
     }
     if (!__any_sync(0xFFFFFFFFu, ray >= 0)) break;
     if (ray >= 0) {
-      if (walk_step<SHADOW>(bvh, w, stack, err)) {
+      if (walk_step<SHADOW>(bvh, w, stack, err, max_iters)) {
         finish(ray, w);
         ray = -1;
       }
@@ -307,14 +308,14 @@ __global__ void SHB_TRAV_BOUNDS k_extend(const BakeItem* __restrict__ bakes, int
                                                         const PathInfo* __restrict__ info, ExtQueue q,
                                                         const int* __restrict__ n_ptr, int cap,
                                                         float4* __restrict__ hits, int* fetch, int* err,
-                                                        Counters64* stats) {
+                                                        Counters64* stats, uint32_t max_iters) {
   const int n = min(*n_ptr, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&stats->extend_rays, (unsigned long long)n);
   const BvhView bvh0 = bakes[0].bvh;
   auto bvh_of = [&](int, float4 o, float4) {
     return n_bakes == 1 ? bvh0 : bakes[info[__float_as_uint(o.w)].x].bvh;
   };
-  consume<false>(q, n, fetch, err, bvh_of, [&](int i, const Walk& w) {
+  consume<false>(q, n, fetch, err, max_iters, bvh_of, [&](int i, const Walk& w) {
     hits[i] = w.hit ? make_float4(w.tmax, w.u, w.v, __uint_as_float(w.prim))
                     : make_float4(0.f, 0.f, 0.f, __uint_as_float(kMissPrim));
   });
@@ -324,14 +325,14 @@ __global__ void SHB_TRAV_BOUNDS k_shadow(const BakeItem* __restrict__ bakes, int
                                                         const int* __restrict__ n_ptr, int cap,
                                                         float4* __restrict__ path_L, float4* __restrict__ nee_li,
                                                         float4* __restrict__ pend, int* fetch, int* err,
-                                                        Counters64* stats) {
+                                                        Counters64* stats, uint32_t max_iters) {
   const int n = min(*n_ptr, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&stats->shadow_rays, (unsigned long long)n);
   const BvhView bvh0 = bakes[0].bvh;
   auto bvh_of = [&](int i, float4, float4) {
     return n_bakes == 1 ? bvh0 : bakes[__float_as_uint(q.c[i].w) >> 2].bvh;
   };
-  consume<true>(q, n, fetch, err, bvh_of, [&](int i, const Walk& w) {
+  consume<true>(q, n, fetch, err, max_iters, bvh_of, [&](int i, const Walk& w) {
     float4 c = q.c[i];
     uint32_t target = __float_as_uint(q.d[i].w);
     const uint32_t kind = __float_as_uint(c.w) & 3u;
@@ -362,7 +363,7 @@ __global__ void k_closest_rays(BvhView bvh, const shb_ray* __restrict__ rays, in
     w.r.dz = sr.direction[2];
     prepare(w.r);
     walk_init(w, bvh, sr.tnear, sr.tfar);
-    while (!walk_step<false>(bvh, w, stack, err)) {
+    while (!walk_step<false>(bvh, w, stack, err, kMaxIters)) {
     }
     hits[i] = w.hit ? make_float4(w.tmax, w.u, w.v, __uint_as_float(w.prim))
                     : make_float4(0.f, 0.f, 0.f, __uint_as_float(kMissPrim));
@@ -381,13 +382,16 @@ int traversal_grid(int device) {
 }
 
 void launch_extend(cudaStream_t st, int grid, const BakeItem* bakes, int n_bakes, const PathInfo* info, ExtQueue q,
-                   const int* n, int cap, float4* hits, int* fetch, int* err, Counters64* stats) {
-  k_extend<<<grid, kTravThreads, 0, st>>>(bakes, n_bakes, info, q, n, cap, hits, fetch, err, stats);
+                   const int* n, int cap, float4* hits, int* fetch, int* err, Counters64* stats, uint32_t max_iters) {
+  k_extend<<<grid, kTravThreads, 0, st>>>(bakes, n_bakes, info, q, n, cap, hits, fetch, err, stats,
+                                          max_iters ? max_iters : kMaxIters);
 }
 
 void launch_shadow(cudaStream_t st, int grid, const BakeItem* bakes, int n_bakes, ShadowQueue q, const int* n, int cap,
-                   float4* path_L, float4* nee_li, float4* pend, int* fetch, int* err, Counters64* stats) {
-  k_shadow<<<grid, kTravThreads, 0, st>>>(bakes, n_bakes, q, n, cap, path_L, nee_li, pend, fetch, err, stats);
+                   float4* path_L, float4* nee_li, float4* pend, int* fetch, int* err, Counters64* stats,
+                   uint32_t max_iters) {
+  k_shadow<<<grid, kTravThreads, 0, st>>>(bakes, n_bakes, q, n, cap, path_L, nee_li, pend, fetch, err, stats,
+                                          max_iters ? max_iters : kMaxIters);
 }
 
 void launch_closest_rays(cudaStream_t st, const BvhView& bvh, const shb_ray* rays, int64_t n, float4* hits, int* err) {

@@ -77,10 +77,13 @@ using PathInfo = uint4;
 // slot, 2 pending hit-NEE slot), bits 2.. = bake index.
 
 // Launch helpers for the persistent traversal kernels (traverse.cu).
+// max_iters bounds the traversal steps of one ray (0: the default,
+// 2^22); a ray that reaches it sets ERR_ITER and ends.
 void launch_extend(cudaStream_t st, int grid, const BakeItem* bakes, int n_bakes, const PathInfo* info, ExtQueue q,
-                   const int* n, int cap, float4* hits, int* fetch, int* err, Counters64* stats);
+                   const int* n, int cap, float4* hits, int* fetch, int* err, Counters64* stats, uint32_t max_iters);
 void launch_shadow(cudaStream_t st, int grid, const BakeItem* bakes, int n_bakes, ShadowQueue q, const int* n, int cap,
-                   float4* path_L, float4* nee_li, float4* pend, int* fetch, int* err, Counters64* stats);
+                   float4* path_L, float4* nee_li, float4* pend, int* fetch, int* err, Counters64* stats,
+                   uint32_t max_iters);
 void launch_closest_rays(cudaStream_t st, const BvhView& bvh, const shb_ray* rays, int64_t n, float4* hits,
                          int* err);
 int traversal_grid(int device);
