@@ -39,6 +39,8 @@ WORKLOADS = {
     # supersample 3, 256 spp, 4 bounces, dilation 4
     "atrium": dict(kind="atrium", width=2048, height=2048, ss=3, spp=256, bounces=4, dilation=4, seed=3),
     "atrium_small": dict(kind="atrium", width=512, height=512, ss=1, spp=32, bounces=4, dilation=4, seed=3),
+    # the atrium at a quarter of its supersampled texels: tuning runs of a few seconds per step
+    "atrium_mid": dict(kind="atrium", width=1024, height=1024, ss=3, spp=64, bounces=4, dilation=4, seed=3),
 }
 
 

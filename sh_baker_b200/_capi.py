@@ -6,6 +6,7 @@ fallback.  load() raises if libshb.so is missing or cannot be loaded.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -186,11 +187,14 @@ class ShbError(RuntimeError):
 
 
 def load(path: Path | str | None = None):
-    """Loads libshb.so (building is a separate step: sh_baker_b200.build)."""
+    """Loads libshb.so (building is a separate step: sh_baker_b200.build).
+    $SHB_LIBRARY names another build of the same sources (a tuning variant
+    from sh_baker_b200.build.build(variant=...))."""
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    env = os.environ.get("SHB_LIBRARY")
+    p = Path(path) if path else (Path(env) if env else LIB_PATH)
     if not p.exists():
         raise RuntimeError(f"libshb.so not found at {p}; run `python -m sh_baker_b200.build` (no CPU fallback exists)")
     lib = C.CDLL(str(p))

@@ -46,16 +46,22 @@ def _newer(out: Path, deps) -> bool:
     return any(Path(d).stat().st_mtime > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    BUILD.mkdir(exist_ok=True)
+def build(verbose: bool = False, force: bool = False, variant: str | None = None, defines=()) -> Path:
+    """Builds libshb.so.  A `variant` builds the same sources with extra
+    preprocessor `defines` (tuning options such as SHB_NEE_BLOCKS_PER_SM=2)
+    into _build_<variant>/libshb.so, loaded through $SHB_LIBRARY."""
+    build_dir = BUILD if variant is None else PKG / f"_build_{variant}"
+    lib = LIB if variant is None else build_dir / "libshb.so"
+    build_dir.mkdir(exist_ok=True)
     headers = [CSRC / h for h in HEADERS] + [PKG.parent / "include" / "shb.h"]
     objs, cmds = [], []
+    dflags = [f"-D{d}" for d in defines]
     for src, flags in SOURCES.items():
         s = CSRC / src
-        o = BUILD / (src + ".o")
+        o = build_dir / (src + ".o")
         objs.append(o)
         if force or _newer(o, [s, *headers, Path(__file__)]):
-            cmds.append([nvcc(), *ARCH, *COMMON, *flags, "-c", str(s), "-o", str(o)])
+            cmds.append([nvcc(), *ARCH, *COMMON, *flags, *dflags, "-c", str(s), "-o", str(o)])
     if cmds:
         from concurrent.futures import ThreadPoolExecutor
 
@@ -67,13 +73,14 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
             for f in [pool.submit(run, c) for c in cmds]:
                 f.result()
-    if force or _newer(LIB, objs):
-        cmd = [nvcc(), *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lz", "-Xlinker", "--no-undefined"]
+    if force or _newer(lib, objs):
+        cmd = [nvcc(), *ARCH, "-shared", "-o", str(lib), *map(str, objs), "-lz", "-Xlinker", "--no-undefined"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    build_cli(verbose, force)
-    return LIB
+    if variant is None:
+        build_cli(verbose, force)
+    return lib
 
 
 CLI = PKG / "bin" / "sh_baker"

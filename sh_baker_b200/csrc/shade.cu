@@ -187,8 +187,9 @@ struct LightEval {
 // Incoming radiance without visibility (src/light.h:34-49,72-95,117-144,
 // 166-188); with HIT, times cos x BRDF (src/light.h:51-203).
 template <bool HIT, bool BWD = false>
-__device__ LightEval eval_light(const SceneView& sc, uint32_t li, f3 P, f3 N, Event& ev, f3 wo, f3 aop) {
-  DLight L = sc.lights[li];
+__device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint32_t li, f3 P, f3 N, Event& ev, f3 wo,
+                                f3 aop) {
+  DLight L = lights[li];
   LightEval e;
   e.apdf = 1.0f;
   if (BWD) {
@@ -279,12 +280,16 @@ __device__ LightEval eval_light(const SceneView& sc, uint32_t li, f3 P, f3 N, Ev
 // are never picked).
 // Weights of up to kWeightCache lights are kept from the summing pass, so
 // the pick only re-evaluates the chosen light; beyond that every light is
-// re-evaluated (same values either way: evaluation is deterministic).
+// re-evaluated (same values either way: evaluation is deterministic).  The
+// cache of a thread is wcache[i * ws]: a local array (ws 1) or the thread's
+// column of a block-wide array in shared memory (ws = threads per block).
+// `lights` is the bake's light table in global memory or the block's copy
+// of it in shared memory.
 constexpr uint32_t kWeightCache = 32;
 
 template <bool HIT, bool BWD = false>
-__device__ bool pick_light(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3 aop, float sum, float u,
-                           const float* wcache, LightEval& out) {
+__device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, f3 wo, f3 aop, float sum,
+                           float u, const float* wcache, int ws, LightEval& out) {
   float target = u * sum;
   float cum = 0.f;
   int last = -1;
@@ -293,33 +298,80 @@ __device__ bool pick_light(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3
     float w;
     LightEval e;
     if (cached) {
-      w = wcache[i];
+      w = wcache[i * ws];
     } else {
-      e = eval_light<HIT, BWD>(sc, i, P, N, ev, wo, aop);
+      e = eval_light<HIT, BWD>(sc, lights, i, P, N, ev, wo, aop);
       w = e.w;
     }
     cum += w;
     if (w > 0.f) last = (int)i;
     if (target < cum) {
-      out = cached ? eval_light<HIT, BWD>(sc, i, P, N, ev, wo, aop) : e;
+      out = cached ? eval_light<HIT, BWD>(sc, lights, i, P, N, ev, wo, aop) : e;
       return true;
     }
   }
   if (last < 0) return false;
-  out = eval_light<HIT, BWD>(sc, (uint32_t)last, P, N, ev, wo, aop);
+  out = eval_light<HIT, BWD>(sc, lights, (uint32_t)last, P, N, ev, wo, aop);
   return true;
 }
 
 template <bool HIT>
-__device__ float light_weight_sum(const SceneView& sc, f3 P, f3 N, Event& ev, f3 wo, f3 aop, float* wcache) {
+__device__ float light_weight_sum(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, f3 wo, f3 aop,
+                                  float* wcache, int ws) {
   float sum = 0.0f;
   const bool cached = sc.light_count <= kWeightCache;
   for (uint32_t i = 0; i < sc.light_count; ++i) {
-    float w = eval_light<HIT>(sc, i, P, N, ev, wo, aop).w;
-    if (cached) wcache[i] = w;
+    float w = eval_light<HIT>(sc, lights, i, P, N, ev, wo, aop).w;
+    if (cached) wcache[i * ws] = w;
     sum += w;
   }
   return sum;
+}
+
+// Forward next-event kernels keep the light table of a one-bake wave in
+// shared memory (SHB_SMEM_LIGHTS) and the light weights of a vertex in
+// shared memory instead of a local array (SHB_SMEM_WCACHE).
+#ifndef SHB_SMEM_LIGHTS
+#define SHB_SMEM_LIGHTS 0
+#endif
+#ifndef SHB_SMEM_WCACHE
+#define SHB_SMEM_WCACHE 0
+#endif
+constexpr uint32_t kSmemLights = 64;
+
+// The table of bake `bake` in the block's shared copy `s` when the wave has
+// one bake and few enough lights, else the global table.  Every thread of
+// the block calls this once, before any early exit.
+__device__ __forceinline__ const DLight* stage_lights(const BakeItem* bakes, int bake, DLight* s) {
+  if (!SHB_SMEM_LIGHTS || bake < 0) return bake >= 0 ? bakes[bake].sc.lights : nullptr;
+  const SceneView& sc = bakes[bake].sc;
+  if (sc.light_count > kSmemLights) return sc.lights;
+  const uint32_t* src = reinterpret_cast<const uint32_t*>(sc.lights);
+  uint32_t* dst = reinterpret_cast<uint32_t*>(s);
+  const uint32_t words = sc.light_count * (uint32_t)(sizeof(DLight) / 4);
+  for (uint32_t k = threadIdx.x; k < words; k += blockDim.x) dst[k] = __ldg(src + k);
+  __syncthreads();
+  return s;
+}
+
+// Dynamic shared memory of the forward next-event kernels: the staged light
+// table, then the weight cache (kWeightCache floats per thread).
+constexpr size_t kSmemLightBytes = SHB_SMEM_LIGHTS ? kSmemLights * sizeof(DLight) : 0;
+constexpr size_t kSmemWcacheBytes = SHB_SMEM_WCACHE ? kWeightCache * kThreads * sizeof(float) : 0;
+constexpr size_t kNeeSmemBytes = kSmemLightBytes + kSmemWcacheBytes;
+
+struct NeeSmem {
+  DLight* lights;
+  float* wc;
+  int ws;
+};
+__device__ __forceinline__ NeeSmem nee_smem(float* dyn) {
+  NeeSmem m;
+  m.lights = reinterpret_cast<DLight*>(dyn);
+  m.wc = SHB_SMEM_WCACHE ? reinterpret_cast<float*>(reinterpret_cast<char*>(dyn) + kSmemLightBytes) + threadIdx.x
+                         : nullptr;
+  m.ws = SHB_SMEM_WCACHE ? (int)blockDim.x : 1;
+  return m;
 }
 
 // Warp-aggregated queue slot: every lane of the warp must call this.
@@ -366,6 +418,7 @@ __device__ __forceinline__ f3 primary_dir(const SP& sp, uint32_t seed, uint32_t 
 struct WaveArgs {
   const BakeItem* bakes;  // device table
   int n_bakes;
+  int one_bake;           // the one bake of this wave's tiles, else -1
   const Tile* tiles;      // this wave's tiles (device)
   int n_tiles;
   int64_t P;              // paths in the wave
@@ -497,6 +550,9 @@ __device__ __forceinline__ int find_tile(const WaveArgs& a, int64_t x) {
 // ------------------------------------------------------------- generate --
 template <bool BWD>
 __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
+  extern __shared__ float dyn_smem[];
+  const NeeSmem sm = nee_smem(dyn_smem);
+  const DLight* wave_lights = BWD ? nullptr : stage_lights(a.bakes, a.one_bake, sm.lights);
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
   const int64_t warp_id = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   const int lane = threadIdx.x & 31;
@@ -538,7 +594,10 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
     Event ev;
     ev.init(active ? B->seed : 0u, texel, sample, 0, EV_NEE);
     const f3 zero3 = {0.f, 0.f, 0.f};
-    float wcache[kWeightCache];
+    float wlocal[SHB_SMEM_WCACHE && !BWD ? 1 : kWeightCache];
+    float* wcache = SHB_SMEM_WCACHE && !BWD ? sm.wc : wlocal;
+    const int ws = SHB_SMEM_WCACHE && !BWD ? sm.ws : 1;
+    const DLight* lights = wave_lights ? wave_lights : B->sc.lights;
     float sum = 0.f;
     // Without area lights the weights depend on the texel only.  When the
     // warp's paths all belong to one texel (spp >= 32 mostly), lane j
@@ -558,16 +617,17 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
       const f3 Nl = {__shfl_sync(0xFFFFFFFFu, N.x, lead), __shfl_sync(0xFFFFFFFFu, N.y, lead),
                      __shfl_sync(0xFFFFFFFFu, N.z, lead)};
       const uint32_t nl = BL->sc.light_count;
-      const float mine = (uint32_t)lane < nl ? eval_light<false>(BL->sc, (uint32_t)lane, Pl, Nl, ev, zero3, zero3).w
-                                             : 0.f;
+      const DLight* ll = wave_lights ? wave_lights : BL->sc.lights;
+      const float mine =
+          (uint32_t)lane < nl ? eval_light<false>(BL->sc, ll, (uint32_t)lane, Pl, Nl, ev, zero3, zero3).w : 0.f;
       for (uint32_t i = 0; i < nl; ++i) {
         const float w = __shfl_sync(0xFFFFFFFFu, mine, (int)i);
-        wcache[i] = w;
+        wcache[i * ws] = w;
         sum += w;
       }
       if (!active) sum = 0.f;
     } else if (active) {
-      sum = light_weight_sum<false>(B->sc, P0, N, ev, zero3, zero3, wcache);
+      sum = light_weight_sum<false>(B->sc, lights, P0, N, ev, zero3, zero3, wcache, ws);
     }
     bool any_light = active && !(sum < 1e-6f);
     const int nls = active ? B->nls : 0;
@@ -576,8 +636,8 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
       bool ok = false;
       float joint = 1.f;
       if (any_light && j < nls) {
-        ok = pick_light<false, BWD>(B->sc, P0, N, ev, zero3, zero3, sum,
-                                    ev.u(3 * (int)B->sc.area_light_count + j), wcache, e);
+        ok = pick_light<false, BWD>(B->sc, lights, P0, N, ev, zero3, zero3, sum,
+                                    ev.u(3 * (int)B->sc.area_light_count + j), wcache, ws, e);
         if (ok) {
           float pdf = e.w / sum;
           joint = pdf * e.apdf;
@@ -633,11 +693,14 @@ template <bool BWD>
 __device__ __forceinline__ void nee_hit(const WaveArgs& a, const BakeItem* B, uint32_t b, f3 hit_pos, f3 N, f3 wo,
                                         f3 aop, f3 beta, float alpha, uint32_t path, uint32_t vertex,
                                         uint32_t texel, uint32_t sample, int depth, bool opaque_hit, uint32_t ntan,
-                                        f3 adj, bool param, int mat_id, int cur, int i) {
+                                        f3 adj, bool param, int mat_id, int cur, int i, const DLight* lights,
+                                        float* wshared, int ws) {
   Event ev;
   ev.init(opaque_hit ? B->seed : 0u, texel, sample, vertex, EV_NEE);
-  float wcache[kWeightCache];
-  float sum = opaque_hit ? light_weight_sum<true>(B->sc, hit_pos, N, ev, wo, aop, wcache) : 0.f;
+  float wlocal[SHB_SMEM_WCACHE && !BWD ? 1 : kWeightCache];
+  float* wcache = wshared ? wshared : wlocal;
+  if (!wshared) ws = 1;
+  float sum = opaque_hit ? light_weight_sum<true>(B->sc, lights, hit_pos, N, ev, wo, aop, wcache, ws) : 0.f;
   bool any_light = opaque_hit && !(sum < 1e-6f);
   const int nls = opaque_hit ? B->nls : 0;
   for (int j = 0; j < a.NLS; ++j) {
@@ -646,8 +709,8 @@ __device__ __forceinline__ void nee_hit(const WaveArgs& a, const BakeItem* B, ui
     f3 c = {0.f, 0.f, 0.f};
     float scale = 0.f;
     if (any_light && j < nls) {
-      ok = pick_light<true, BWD>(B->sc, hit_pos, N, ev, wo, aop, sum,
-                                 ev.u(3 * (int)B->sc.area_light_count + j), wcache, e);
+      ok = pick_light<true, BWD>(B->sc, lights, hit_pos, N, ev, wo, aop, sum,
+                                 ev.u(3 * (int)B->sc.area_light_count + j), wcache, ws, e);
       if (ok) {
         float pdf = e.w / sum;
         float joint = pdf * e.apdf;
@@ -709,6 +772,9 @@ template <bool BWD, bool SPLIT = false>
 __global__ void SHB_SHADE_BOUNDS k_shade(WaveArgs a, int cur, int depth) {
   extern __shared__ float sgrad[];
   if (BWD) grad_zero(sgrad, a.n_params);
+  // forward inline next-event estimation: the staged light table and weight cache
+  const NeeSmem sm = nee_smem(sgrad);
+  const DLight* wave_lights = (BWD || SPLIT) ? nullptr : stage_lights(a.bakes, a.one_bake, sm.lights);
   const int n = min(a.cnt[cur], a.ext_cap);
   const int nxt = cur ^ 1;
   const int warps = gridDim.x * (blockDim.x >> 5);
@@ -819,7 +885,8 @@ __global__ void SHB_SHADE_BOUNDS k_shade(WaveArgs a, int cur, int depth) {
     f3 wo = -d;
     if (BWD || !SPLIT) {
       nee_hit<BWD>(a, B, b, hit_pos, N, wo, aop, beta, alpha, path, vertex, texel, sample, depth, opaque_hit, ntan,
-                   adj, param, mat_id, cur, i);
+                   adj, param, mat_id, cur, i, wave_lights ? wave_lights : B->sc.lights,
+                   (BWD || !SHB_SMEM_WCACHE) ? nullptr : sm.wc, sm.ws);
     } else {
       const int rs = warp_push(a.cnt + CNT_NEE, opaque_hit);
       if (opaque_hit && slot_ok(a, rs, a.ext_cap)) {
@@ -906,6 +973,9 @@ __global__ void SHB_SHADE_BOUNDS k_shade(WaveArgs a, int cur, int depth) {
 #define SHB_NEE_BOUNDS __launch_bounds__(kThreads)
 #endif
 __global__ void SHB_NEE_BOUNDS k_nee(WaveArgs a, int cur, int depth) {
+  extern __shared__ float dyn_smem[];
+  const NeeSmem sm = nee_smem(dyn_smem);
+  const DLight* wave_lights = stage_lights(a.bakes, a.one_bake, sm.lights);
   const int n = min(a.cnt[CNT_NEE], a.ext_cap);
   const int warps = gridDim.x * (blockDim.x >> 5);
   const int warp_id = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -938,7 +1008,8 @@ __global__ void SHB_NEE_BOUNDS k_nee(WaveArgs a, int cur, int depth) {
     }
     const f3 wo = -d;
     nee_hit<false>(a, B, b, hit_pos, N, wo, aop, beta, alpha, path, vertex, texel, sample, depth, active, 0u,
-                   f3{0.f, 0.f, 0.f}, false, -1, cur, i);
+                   f3{0.f, 0.f, 0.f}, false, -1, cur, i, wave_lights ? wave_lights : B->sc.lights,
+                   SHB_SMEM_WCACHE ? sm.wc : nullptr, sm.ws);
   }
 }
 
@@ -1477,8 +1548,9 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
     const int nbk = w.bake >= 0 ? 1 : nb;
     cudaMemsetAsync(cnt, 0, sizeof(int) * (CNT_FETCH_SHADOW + 1), st);
     Pair pg = stamp(2);
+    a.one_bake = w.bake;
     if (bwd) k_generate<true><<<grid_for(w.P), kThreads, 0, st>>>(a);
-    else k_generate<false><<<grid_for(w.P), kThreads, 0, st>>>(a);
+    else k_generate<false><<<grid_for(w.P), kThreads, kNeeSmemBytes, st>>>(a);
     close_stamp(pg);
     launches++;
     for (int k = 0; k <= w.max_bounces; ++k) {
@@ -1495,10 +1567,10 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       } else if (split_nee) {
         cudaMemsetAsync(cnt + CNT_NEE, 0, sizeof(int), st);
         k_shade<false, true><<<sgrid, kThreads, 0, st>>>(a, cur, k);
-        k_nee<<<sgrid, kThreads, 0, st>>>(a, cur, k);
+        k_nee<<<sgrid, kThreads, kNeeSmemBytes, st>>>(a, cur, k);
         launches++;
       } else {
-        k_shade<false><<<sgrid, kThreads, 0, st>>>(a, cur, k);
+        k_shade<false><<<sgrid, kThreads, kNeeSmemBytes, st>>>(a, cur, k);
       }
       close_stamp(pd);
       Pair ps = stamp(1);
