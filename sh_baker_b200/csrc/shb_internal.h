@@ -149,7 +149,20 @@ struct alignas(16) WideNode {
   uint32_t qhi[6];    // qhi_x[8], qhi_y[8], qhi_z[8]
 };
 static_assert(sizeof(WideNode) == 80, "WideNode must be 80 bytes");
-// meta byte: 0 = empty slot; internal child: 1; leaf: count<<5 | offset.
+// meta byte = count << 5 | position: the child contributes `count` bits
+// from `position` to a node's hit mask.  Empty slot: 0.  Leaf: its
+// triangle count and its first triangle's offset from tri_base (< 24).
+// Internal child in slot s: count 1, position 24 + s (the traversal XORs s
+// with the ray octant, so the hit mask's bits 24..31 are in visiting order).
+
+// SHB_TRAV_FOLD: the builder leaves one quantisation step of margin on
+// every side of every child box, which lets the traversal fold the byte ->
+// float conversion of a plane into its FMA (t = (2^23 + q) s + (a - 2^23 s),
+// off by at most half a step, so the box test stays conservative).  Builder
+// and traversal read the same setting.
+#ifndef SHB_TRAV_FOLD
+#define SHB_TRAV_FOLD 0
+#endif
 
 struct BvhView {
   const WideNode* nodes;

@@ -122,6 +122,11 @@ __device__ __forceinline__ float byte_f(uint32_t w, int k) {
   return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | (uint32_t)k)) - 8388608.0f;
 }
 
+// Byte k of w as the float 2^23 + byte (one byte permute).
+__device__ __forceinline__ float byte_raw(uint32_t w, int k) {
+  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | (uint32_t)k));
+}
+
 // Traversal state of one ray.  Groups are (base, bits): a node group has
 // kNodeGroup set, the internal-child mask in bits 8..15 and the remaining
 // hit slots (in ray-octant order) in bits 0..7; a triangle group has the
@@ -149,8 +154,43 @@ __device__ __forceinline__ void walk_init(Walk& w, const BvhView& bvh, float tne
   w.prim = kMissPrim;
 }
 
+// max / min of three floats, NaN operands ignored like fmaxf / fminf
+// (PTX three-input max.f32 / min.f32).
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+  float r;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+__device__ __forceinline__ float min3f(float a, float b, float c) {
+  float r;
+  asm("min.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+  return r;
+}
+// Mask of `width` bits from bit `pos` (both taken modulo 32 / clamped like
+// PTX bmsk.clamp: width 0 gives 0).
+__device__ __forceinline__ uint32_t bit_mask(uint32_t pos, uint32_t width) {
+  uint32_t r;
+  asm("bmsk.clamp.b32 %0, %1, %2;" : "=r"(r) : "r"(pos), "r"(width));
+  return r;
+}
+__device__ __forceinline__ uint32_t bfe(uint32_t x, uint32_t pos, uint32_t len) {
+  uint32_t r;
+  asm("bfe.u32 %0, %1, %2, %3;" : "=r"(r) : "r"(x), "r"(pos), "r"(len));
+  return r;
+}
+
+#ifndef SHB_TRAV_V2
+#define SHB_TRAV_V2 1
+#endif
+
 // Tests the 8 children of `node`; returns the internal children as a node
 // group and the hit leaf triangles as a triangle group.
+//
+// Every child adds its meta byte's bits to one 32-bit hit mask (triangles
+// in bits 0..23, internal children at 24 + slot): the internal children's
+// slots are first XORed with the ray octant, four at a time, so bits
+// 24..31 come out in visiting order (the compressed wide BVH traversal of
+// Ylitie, Karras and Laine 2017).
 __device__ __forceinline__ void intersect_node(const BvhView& bvh, const Walk& w, uint32_t node, uint2& Gn,
                                                uint2& Tn) {
   const TravRay& r = w.r;
@@ -170,8 +210,40 @@ __device__ __forceinline__ void intersect_node(const BvhView& bvh, const Walk& w
   if (oct & 1u) { uint32_t t0 = lx0, t1 = lx1; lx0 = hx0; lx1 = hx1; hx0 = t0; hx1 = t1; }
   if (oct & 2u) { uint32_t t0 = ly0, t1 = ly1; ly0 = hy0; ly1 = hy1; hy0 = t0; hy1 = t1; }
   if (oct & 4u) { uint32_t t0 = lz0, t1 = lz1; lz0 = hz0; lz1 = hz1; hz0 = t0; hz1 = t1; }
-  uint32_t hits_int = 0, hits_tri = 0;
   const float tlim = w.tmax * 1.0000004f;
+#if SHB_TRAV_V2
+#if SHB_TRAV_FOLD
+  // planes decode to 2^23 + q; the 2^23 s goes into the offset
+  ax = fmaf(-8388608.0f, sx, ax);
+  ay = fmaf(-8388608.0f, sy, ay);
+  az = fmaf(-8388608.0f, sz, az);
+#define SHB_PLANE(w, k) byte_raw(w, k)
+#else
+#define SHB_PLANE(w, k) byte_f(w, k)
+#endif
+  const uint32_t oct4 = oct * 0x01010101u;
+  // internal children have position bits 3 and 4 both set (24..31)
+  const uint32_t m_lo = n1.z ^ (__vcmpeq4(n1.z & 0x18181818u, 0x18181818u) & oct4);
+  const uint32_t m_hi = n1.w ^ (__vcmpeq4(n1.w & 0x18181818u, 0x18181818u) & oct4);
+  uint32_t hm = 0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int k = j & 3;
+    const uint32_t mw = j < 4 ? m_lo : m_hi;
+    float t0x = fmaf(SHB_PLANE(j < 4 ? lx0 : lx1, k), sx, ax), t1x = fmaf(SHB_PLANE(j < 4 ? hx0 : hx1, k), sx, ax);
+    float t0y = fmaf(SHB_PLANE(j < 4 ? ly0 : ly1, k), sy, ay), t1y = fmaf(SHB_PLANE(j < 4 ? hy0 : hy1, k), sy, ay);
+    float t0z = fmaf(SHB_PLANE(j < 4 ? lz0 : lz1, k), sz, az), t1z = fmaf(SHB_PLANE(j < 4 ? hz0 : hz1, k), sz, az);
+    const float tmin_c = fmaxf(max3f(t0x, t0y, t0z), w.tnear);
+    const float tmax_c = fminf(min3f(t1x, t1y, t1z), tlim);
+    const uint32_t bits = bit_mask(bfe(mw, 8 * k, 5), bfe(mw, 8 * k + 5, 3));
+    if (tmin_c <= tmax_c) hm |= bits;
+  }
+#undef SHB_PLANE
+  Gn = make_uint2(n1.x, kNodeGroup | (imask << 8) | (hm >> 24));
+  Tn = make_uint2(n1.y, hm & 0x00FFFFFFu);
+#else
+  static_assert(!SHB_TRAV_FOLD, "the folded plane decode needs SHB_TRAV_V2");
+  uint32_t hits_int = 0, hits_tri = 0;
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
     uint32_t meta = ((j < 4 ? n1.z : n1.w) >> (8 * (j & 3))) & 0xFFu;
@@ -188,6 +260,7 @@ __device__ __forceinline__ void intersect_node(const BvhView& bvh, const Walk& w
   }
   Gn = make_uint2(n1.x, kNodeGroup | (imask << 8) | hits_int);
   Tn = make_uint2(n1.y, hits_tri);
+#endif
 }
 
 // One step: visit one node (or take a popped triangle group) and test the
