@@ -288,6 +288,7 @@ def batched_result(steps: int, warmup: int):
         ms, _ = timed(lambda: [api.bake_plain_device(b, sh, env) for b, (sh, env) in zip(bakes, outs)])
         s_ms += ms
     clk = clocks.stop()
+    head = batched_headroom(api, bakes, outs, stream, timed)
     tuned = Path(tune).read_text().split()
     tris = [m["scene"].triangle_count for m in mix]
     res = {"value": ts / (b_ms / 1e3), "ms_per_step": b_ms / steps, "steps": steps, "warmup": warmup,
@@ -298,9 +299,41 @@ def batched_result(steps: int, warmup: int):
            "workload": "64 procedural rooms, 1k-100k triangles, 128^2-1024^2, 32-256 spp, 2-4 bounces, "
                        "1-8 point lights; shb_bake_batch in a CUDA graph vs 64 plain shb_bake calls",
            "bakes": 64, "triangles_total": int(sum(tris)), "texel_samples_per_step": ts // steps,
-           "gpu_launches": int(launches), "clocks": clk}
+           "gpu_launches": int(launches), "clocks": clk, "headroom": head}
     ctx.close()
     return res
+
+
+def batched_headroom(api, bakes, outs, stream, timed, target_paths: int = 1 << 24):
+    """How much any batching can gain on this mix.  Each bake is timed alone
+    through the plain path, and again with its sample count multiplied
+    until it traces at least `target_paths` paths: the same texels, scene,
+    bounces and per-path work, enough to fill the GPU, so its rate there is
+    the bake's saturated rate.  A bake's idle time is its plain time minus
+    its texel-samples at the saturated rate; no launch structure can beat
+    the sum of the saturated times, which bounds the batched speed-up."""
+    import torch
+    plain_ms = sat_ms = 0.0
+    per = []
+    for b, (sh, env) in zip(bakes, outs):
+        ms, st = timed(lambda: api.bake_plain_device(b, sh, env))
+        n = st.texel_samples
+        m = max(1, -(-target_paths // max(n, 1)))
+        cfg = api.BakeConfig(samples=b.config.samples * m, bounces=b.config.bounces, seed=b.config.seed)
+        big = api.BatchBake(b.scene, b.gbuffer, b.raster, cfg)
+        ms_big, st_big = timed(lambda: api.bake_plain_device(big, sh, env))
+        sat = n / (st_big.texel_samples / ms_big)  # ms at the saturated rate
+        plain_ms += ms
+        sat_ms += sat
+        per.append((n, ms, sat))
+    torch.cuda.synchronize()
+    small = [x for x in per if x[0] < 5_000_000]
+    return {"plain_ms": plain_ms, "saturated_ms": sat_ms, "idle_ms": plain_ms - sat_ms,
+            "max_speedup": plain_ms / sat_ms,
+            "bakes_under_5M_texel_samples": {"count": len(small), "plain_ms": sum(x[1] for x in small),
+                                             "saturated_ms": sum(x[2] for x in small)},
+            "method": "per bake: plain time vs its texel-samples at the rate of the same bake with samples "
+                      f"multiplied to >= {target_paths} paths"}
 
 
 def run_batched(args):
@@ -313,7 +346,8 @@ def run_batched(args):
             "config": {"workload": r["workload"], "bakes": r["bakes"], "triangles_total": r["triangles_total"],
                        "texel_samples_per_step": r["texel_samples_per_step"]},
             "sequential": r["sequential"], "speedup_vs_sequential": r["speedup_vs_sequential"],
-            "autotuned": r["autotuned"], "gpu_launches": r["gpu_launches"], "clocks": r["clocks"]}
+            "autotuned": r["autotuned"], "headroom": r["headroom"], "gpu_launches": r["gpu_launches"],
+            "clocks": r["clocks"]}
     print(json.dumps(line), flush=True)
 
 

@@ -46,10 +46,14 @@ def _newer(out: Path, deps) -> bool:
     return any(Path(d).stat().st_mtime > t for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False, variant: str | None = None, defines=()) -> Path:
+def build(verbose: bool = False, force: bool = False, variant: str | None = None, defines=(),
+          file_flags=None) -> Path:
     """Builds libshb.so.  A `variant` builds the same sources with extra
     preprocessor `defines` (tuning options such as SHB_NEE_BLOCKS_PER_SM=2)
-    into _build_<variant>/libshb.so, loaded through $SHB_LIBRARY."""
+    and per-file nvcc flags (`file_flags`, e.g. {"shade.cu": ["-fmad=true"]},
+    appended after the file's own) into _build_<variant>/libshb.so, loaded
+    through $SHB_LIBRARY."""
+    file_flags = file_flags or {}
     build_dir = BUILD if variant is None else PKG / f"_build_{variant}"
     lib = LIB if variant is None else build_dir / "libshb.so"
     build_dir.mkdir(exist_ok=True)
@@ -61,7 +65,7 @@ def build(verbose: bool = False, force: bool = False, variant: str | None = None
         o = build_dir / (src + ".o")
         objs.append(o)
         if force or _newer(o, [s, *headers, Path(__file__)]):
-            cmds.append([nvcc(), *ARCH, *COMMON, *flags, *dflags, "-c", str(s), "-o", str(o)])
+            cmds.append([nvcc(), *ARCH, *COMMON, *flags, *file_flags.get(src, []), *dflags, "-c", str(s), "-o", str(o)])
     if cmds:
         from concurrent.futures import ThreadPoolExecutor
 

@@ -1,5 +1,13 @@
-// batch.cu - shb_bake_batch: many bakes in one persistent launch, and the
-// autotuner that picks its launch structure per shape class.
+// batch.cu - shb_bake_batch: many bakes run through one shared sequence of
+// wavefront launches, and the autotuner that picks its launch structure per
+// shape class.
+//
+// The bakes' valid texels are cut into work tiles of whole texels, and the
+// tiles packed into waves of paths on the host (shade.cu plan_waves): a
+// bake large enough to fill waves gets waves of its own, smaller bakes share
+// waves, so the per-depth traversal and shading launches of one wave carry
+// paths of several bakes.  The whole sequence can be captured in one CUDA
+// graph.
 //
 // The tuned parameters are the queue depth (paths per wave), the size below
 // which bakes share waves (larger bakes get waves of their own), the

@@ -189,7 +189,7 @@ struct LightEval {
 template <bool HIT, bool BWD = false>
 __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint32_t li, f3 P, f3 N, Event& ev, f3 wo,
                                 f3 aop) {
-  DLight L = lights[li];
+  const DLight& L = lights[li];
   LightEval e;
   e.apdf = 1.0f;
   if (BWD) {
@@ -689,18 +689,26 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
 // weights, NLS picks and one shadow-queue entry per visible candidate.  All
 // lanes of the warp call it (queue pushes are warp-aggregated); lanes with
 // opaque_hit false take part without work.  BWD adds the gradient packets.
-template <bool BWD>
+// `late(beta, alpha, path)` runs after the light weights are summed and may
+// supply those three values then (k_nee reads them back from its record, so
+// that they are not held in registers through the light loop).
+struct NoLate {
+  __device__ __forceinline__ void operator()(f3&, float&, uint32_t&) const {}
+};
+
+template <bool BWD, class Late = NoLate>
 __device__ __forceinline__ void nee_hit(const WaveArgs& a, const BakeItem* B, uint32_t b, f3 hit_pos, f3 N, f3 wo,
                                         f3 aop, f3 beta, float alpha, uint32_t path, uint32_t vertex,
                                         uint32_t texel, uint32_t sample, int depth, bool opaque_hit, uint32_t ntan,
                                         f3 adj, bool param, int mat_id, int cur, int i, const DLight* lights,
-                                        float* wshared, int ws) {
+                                        float* wshared, int ws, Late late = Late()) {
   Event ev;
   ev.init(opaque_hit ? B->seed : 0u, texel, sample, vertex, EV_NEE);
   float wlocal[SHB_SMEM_WCACHE && !BWD ? 1 : kWeightCache];
   float* wcache = wshared ? wshared : wlocal;
   if (!wshared) ws = 1;
   float sum = opaque_hit ? light_weight_sum<true>(B->sc, lights, hit_pos, N, ev, wo, aop, wcache, ws) : 0.f;
+  late(beta, alpha, path);
   bool any_light = opaque_hit && !(sum < 1e-6f);
   const int nls = opaque_hit ? B->nls : 0;
   for (int j = 0; j < a.NLS; ++j) {
@@ -967,6 +975,9 @@ __global__ void SHB_SHADE_BOUNDS k_shade(WaveArgs a, int cur, int depth) {
 #ifndef SHB_NEE_BLOCKS_PER_SM
 #define SHB_NEE_BLOCKS_PER_SM 4
 #endif
+#ifndef SHB_NEE_LATE
+#define SHB_NEE_LATE 0
+#endif
 #if SHB_NEE_BLOCKS_PER_SM > 0
 #define SHB_NEE_BOUNDS __launch_bounds__(kThreads, SHB_NEE_BLOCKS_PER_SM)
 #else
@@ -991,15 +1002,18 @@ __global__ void SHB_NEE_BOUNDS k_nee(WaveArgs a, int cur, int depth) {
     const BakeItem* B = a.bakes;
     if (active) {
       const float4 r0 = a.nee_rec[i], r1 = a.nee_rec[C + i], r2 = a.nee_rec[2 * C + i],
-                   r3 = a.nee_rec[3 * C + i], r4 = a.nee_rec[4 * C + i];
+                   r3 = a.nee_rec[3 * C + i];
       hit_pos = {r0.x, r0.y, r0.z};
       path = __float_as_uint(r0.w);
       N = {r1.x, r1.y, r1.z};
       vertex = __float_as_uint(r1.w);
       d = {r2.x, r2.y, r2.z};
-      alpha = r2.w;
       aop = {r3.x, r3.y, r3.z};
-      beta = {r3.w, r4.x, r4.y};
+      if (!SHB_NEE_LATE) {
+        const float4 r4 = a.nee_rec[4 * C + i];
+        alpha = r2.w;
+        beta = {r3.w, r4.x, r4.y};
+      }
       const PathInfo pi = a.info[path];
       b = pi.x;
       B = a.bakes + b;
@@ -1007,9 +1021,19 @@ __global__ void SHB_NEE_BOUNDS k_nee(WaveArgs a, int cur, int depth) {
       sample = pi.z;
     }
     const f3 wo = -d;
+    // with SHB_NEE_LATE the throughput, alpha and path are read back after the light loop
+    auto late = [&](f3& bt, float& al, uint32_t& pa) {
+      if (SHB_NEE_LATE && active) {
+        const float4 r0 = a.nee_rec[i], r2 = a.nee_rec[2 * C + i], r3 = a.nee_rec[3 * C + i],
+                     r4 = a.nee_rec[4 * C + i];
+        pa = __float_as_uint(r0.w);
+        al = r2.w;
+        bt = {r3.w, r4.x, r4.y};
+      }
+    };
     nee_hit<false>(a, B, b, hit_pos, N, wo, aop, beta, alpha, path, vertex, texel, sample, depth, active, 0u,
                    f3{0.f, 0.f, 0.f}, false, -1, cur, i, wave_lights ? wave_lights : B->sc.lights,
-                   SHB_SMEM_WCACHE ? sm.wc : nullptr, sm.ws);
+                   SHB_SMEM_WCACHE ? sm.wc : nullptr, sm.ws, late);
   }
 }
 

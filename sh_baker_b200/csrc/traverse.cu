@@ -122,10 +122,12 @@ __device__ __forceinline__ float byte_f(uint32_t w, int k) {
   return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | (uint32_t)k)) - 8388608.0f;
 }
 
+#if SHB_TRAV_FOLD
 // Byte k of w as the float 2^23 + byte (one byte permute).
 __device__ __forceinline__ float byte_raw(uint32_t w, int k) {
   return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | (uint32_t)k));
 }
+#endif
 
 // Traversal state of one ray.  Groups are (base, bits): a node group has
 // kNodeGroup set, the internal-child mask in bits 8..15 and the remaining

@@ -35,3 +35,31 @@ def test_reference_arm_line():
 
 def test_reference_arm_other_ranks_are_silent():
     assert run_ref({"RANK": "1", "WORLD_SIZE": "2", "LOCAL_RANK": "1"}) == []
+
+
+def test_default_workload_is_the_atrium():
+    import argparse
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", ROOT / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    w = bench.WORKLOADS["atrium"]
+    assert (w["width"], w["height"], w["ss"], w["spp"], w["bounces"], w["dilation"]) == (2048, 2048, 3, 256, 4, 4)
+    src = (ROOT / "bench.py").read_text()
+    assert 'ap.add_argument("--workload", default="atrium"' in src
+    del argparse
+
+
+def test_traversal_profile_rows_parse(tmp_path, monkeypatch):
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod2", ROOT / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    (tmp_path / "profiles").mkdir()
+    (tmp_path / "profiles" / "traversal_demo_small.md").write_text(
+        "| kernel | rays | DRAM B/ray | L2 B/ray | warp inst/ray | lanes |\n|---|---|---|---|---|---|\n"
+        "| closest_hit | 1000 | 49.6 | 812.5 | 210.0 | 13.5 |\n")
+    monkeypatch.setattr(bench, "ROOT", tmp_path)
+    got = bench.traversal_profile("demo", "closest_hit")
+    assert got["warp_inst_per_ray"] == 210.0 and got["l2_bytes_per_ray"] == 812.5 and got["profiled_rays"] == 1000
+    assert bench.traversal_profile("demo", "any_hit") is None
