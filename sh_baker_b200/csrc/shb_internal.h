@@ -280,8 +280,11 @@ struct BakeSpec {
 };
 
 // Launch-structure parameters (chosen by the autotuner for batches).
+#ifndef SHB_WAVE_LOG2
+#define SHB_WAVE_LOG2 23
+#endif
 struct BatchParams {
-  int64_t wave_paths = int64_t(1) << 23;  // paths in flight per wave (queue depth)
+  int64_t wave_paths = int64_t(1) << SHB_WAVE_LOG2;  // paths in flight per wave (queue depth)
   int64_t tile_texels = int64_t(1) << 30; // texels per work tile
   int grid_scale = 1;                     // traversal grid = grid_scale x SMs x occupancy
   int64_t share_paths = -1;               // bakes of fewer paths share waves (-1: wave_paths / 2)
