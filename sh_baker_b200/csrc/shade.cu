@@ -315,10 +315,29 @@ __device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N
   return true;
 }
 
+// SHB_NEE_PREFETCH: before the weight loop, the triangle every area light
+// will sample is drawn (a separate cursor over the same counter stream, so
+// the values are the loop's) and its record prefetched into L1, so the
+// loop's dependent record loads no longer wait on L2 one after another.
+#ifndef SHB_NEE_PREFETCH
+#define SHB_NEE_PREFETCH 0
+#endif
+
 template <bool HIT>
 __device__ float light_weight_sum(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, f3 wo, f3 aop,
                                   float* wcache, int ws) {
   float sum = 0.0f;
+  if (SHB_NEE_PREFETCH) {
+    Event ep = ev;
+    ep.block = -1;
+    for (uint32_t k = 0; k < sc.area_light_count; ++k) {
+      const uint2 info = sc.area_info[k];
+      const uint32_t n = info.y & ~kAreaHasUv;
+      if (n == 0) continue;
+      const float4* r = sc.area_tris + 4 * ((size_t)info.x + ep.tri(3 * (int)k, n));
+      asm volatile("prefetch.global.L1 [%0];" ::"l"(r));
+    }
+  }
   const bool cached = sc.light_count <= kWeightCache;
   for (uint32_t i = 0; i < sc.light_count; ++i) {
     float w = eval_light<HIT>(sc, lights, i, P, N, ev, wo, aop).w;
