@@ -28,6 +28,7 @@ SOURCES = {
     "batch.cu": ["-fmad=false"],
     "exr.cu": ["-fmad=false"],
     "gltf.cpp": [],
+    "jpeg.cpp": [],
     "atlas.cpp": [],
     "preview.cu": ["-fmad=false"],
 }

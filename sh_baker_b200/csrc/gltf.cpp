@@ -5,7 +5,7 @@
 // hierarchies with matrix or TRS transforms, triangle primitives with
 // POSITION / NORMAL / TEXCOORD_0 (required, as the reference requires them)
 // and optional TEXCOORD_1 / TANGENT, materials with
-// KHR_materials_emissive_strength and a PNG base-colour texture or the
+// KHR_materials_emissive_strength and a PNG or JPEG base-colour texture or the
 // baseColorFactor, and KHR_lights_punctual lights.  Behaviour follows the
 // reference loader:
 //   - a primitive without material, POSITION, NORMAL or TEXCOORD_0 fails the
@@ -23,7 +23,8 @@
 // derivatives (MikkTSpace, a third-party library, is not vendored); the
 // bake's hemisphere sampling is invariant to the tangent's rotation about the
 // normal, so only the random stream's orientation differs.  JPEG textures
-// are rejected.  The sky environment (:705-797) is not read: the bake never
+// are decoded by jpeg.cpp (sequential files only; progressive ones are
+// rejected).  The sky environment (:705-797) is not read: the bake never
 // samples it.
 #include <zlib.h>
 
@@ -40,6 +41,12 @@
 
 #include "host_scene.h"
 #include "shb_internal.h"
+
+namespace shb {
+// jpeg.cpp: sequential JPEG -> 8-bit RGB.
+bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint32_t& W, uint32_t& H, uint32_t& C,
+                 std::string& err);
+}  // namespace shb
 
 namespace shb {
 namespace {
@@ -243,7 +250,7 @@ bool decode_png(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint32
                 std::string& err) {
   static const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
   if (f.size() < 8 || std::memcmp(f.data(), sig, 8) != 0) {
-    err = "not a PNG (only PNG textures are supported)";
+    err = "not a PNG or JPEG (only PNG and JPEG textures are supported)";
     return false;
   }
   size_t i = 8;
@@ -806,6 +813,7 @@ struct Loader {
     } else {
       return true;
     }
+    if (bytes.size() >= 2 && bytes[0] == 0xFF && bytes[1] == 0xD8) return shb::decode_jpeg(bytes, M.px, M.w, M.h, M.c, err);
     return decode_png(bytes, M.px, M.w, M.h, M.c, err);
   }
 

@@ -1,6 +1,7 @@
 """LoadScene (shb_load_gltf, src/loader.cpp:144-844) on glTF files written
 by tests/gltf_fixture.py; host code only, no GPU."""
 import math
+from pathlib import Path
 
 import numpy as np
 import pytest
@@ -144,6 +145,41 @@ def test_png_colour_types(tmp_path):
     np.testing.assert_array_equal(mp.albedo.pixel_data.reshape(2, 2, 4), exp)
 
 
+def test_jpeg_textures_match_libjpeg(tmp_path):
+    """JPEG base-colour textures (the reference decodes them with stb_image)
+    against Pillow's libjpeg decode of the same files
+    (tests/golden/make_jpeg_golden.py): 4:4:4 / 4:2:2 / 4:2:0 sampling,
+    restart markers, greyscale, partial MCUs.  Both use exact-enough inverse
+    DCTs and the same chroma filter, so pixels differ by at most 2 levels."""
+    ref = np.load(Path(__file__).parent / "golden" / "jpeg_reference.npz")
+    names = sorted({k[:-5] for k in ref.files if k.endswith("_jpeg")})
+    assert len(names) == 8
+    pos, nrm, uv, idx = quad()
+    for n in names:
+        b = GltfBuilder()
+        m = b.material(texture_png=ref[n + "_jpeg"].tobytes())
+        b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=m)]))
+        err = []
+        sc = api.LoadScene(b.write(tmp_path / f"{n}.gltf"), err)
+        assert sc is not None, (n, err)
+        a = sc.materials[0].albedo
+        want = ref[n + "_rgb"]
+        assert (a.height, a.width, a.channels) == (*want.shape[:2], 3), n
+        diff = np.abs(a.pixel_data.reshape(want.shape).astype(int) - want.astype(int))
+        assert diff.max() <= 2 and diff.mean() <= 0.5, (n, diff.max(), diff.mean())
+
+
+def test_progressive_jpeg_is_rejected(tmp_path):
+    # SOF2 marker right after SOI: the loader names the unsupported coding
+    data = bytes([0xFF, 0xD8, 0xFF, 0xC2, 0x00, 0x0B, 8, 0, 1, 0, 1, 1, 1, 0x11, 0, 0xFF, 0xD9])
+    pos, nrm, uv, idx = quad()
+    b = GltfBuilder()
+    b.material(texture_png=data)
+    b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=0)]))
+    err = []
+    assert api.LoadScene(b.write(tmp_path / "p.gltf"), err) is None and "sequential" in err[0]
+
+
 def test_defaults_and_errors(tmp_path):
     pos, nrm, uv, idx = quad()
     # no materials: a white default (a primitive must still name material 0)
@@ -169,10 +205,15 @@ def test_defaults_and_errors(tmp_path):
     err = []
     assert api.LoadScene(tmp_path / "missing.gltf", err) is None and "cannot read" in err[0]
     b = GltfBuilder()
-    b.material(texture_png=b"\xff\xd8\xff\xe0 not a png")
+    b.material(texture_png=b"\xff\xd8\xff\xe0 a damaged jpeg")
     b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=0)]))
     err = []
-    assert api.LoadScene(b.write(tmp_path / "j.gltf"), err) is None and "PNG" in err[0]
+    assert api.LoadScene(b.write(tmp_path / "j.gltf"), err) is None and "JPEG" in err[0]
+    b = GltfBuilder()
+    b.material(texture_png=b"GIF89a neither")
+    b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=0)]))
+    err = []
+    assert api.LoadScene(b.write(tmp_path / "g.gltf"), err) is None and "PNG or JPEG" in err[0]
 
 
 def test_save_scene_round_trip(tmp_path):
