@@ -468,25 +468,13 @@ __global__ void k_emit(int n_level, int wide_base, int child_wide_base, int tri_
     uint32_t ebits = 0;
     for (int a = 0; a < 3; ++a) {
       float ext = __fsub_ru(root.hi[a], root.lo[a]);
-      // with SHB_TRAV_FOLD: a step more below and above the node (253 + 2)
-      float sv = __fdiv_ru(ext, SHB_TRAV_FOLD ? 253.0f : 255.0f);
+      float sv = __fdiv_ru(ext, 255.0f);
       int e = 0;
       frexpf(sv, &e);
       if (!(sv > 0.f)) e = -126;
-      if (SHB_TRAV_FOLD) {
-        // the step must be representable next to the box's coordinates, so
-        // that the origin one step below the node is exact
-        const float mag = fmaxf(fabsf(root.lo[a]), fabsf(root.hi[a]));
-        if (mag > 0.f) e = max(e, ilogbf(mag) - 22);
-      }
       e = e < -126 ? -126 : (e > 127 ? 127 : e);
       ebits |= (uint32_t)(e + 127) << (8 * a);
       scale[a] = __int_as_float((e + 127) << 23);
-    }
-    if (SHB_TRAV_FOLD) {  // origin one step below the node
-      nd.px = __fsub_rd(root.lo[0], scale[0]);
-      nd.py = __fsub_rd(root.lo[1], scale[1]);
-      nd.pz = __fsub_rd(root.lo[2], scale[2]);
     }
     uint32_t imask = 0, meta_lo = 0, meta_hi = 0;
     uint32_t qlo[6] = {0, 0, 0, 0, 0, 0}, qhi[6] = {0, 0, 0, 0, 0, 0};
@@ -526,10 +514,6 @@ __global__ void k_emit(int n_level, int wide_base, int child_wide_base, int tri_
         int qh = h < 0.f ? 0 : (h > 255.f ? 255 : (int)h);
         while (ql > 0 && __fadd_rn(p[a], __fmul_rn((float)ql, scale[a])) > ch.lo[a]) ql--;
         while (qh < 255 && __fadd_rn(p[a], __fmul_rn((float)qh, scale[a])) < ch.hi[a]) qh++;
-        if (SHB_TRAV_FOLD) {  // one step of margin on each side
-          ql = ql > 0 ? ql - 1 : 0;
-          qh = qh < 255 ? qh + 1 : 255;
-        }
         int word = a * 2 + (s >> 2);
         qlo[word] = set_byte(qlo[word], s & 3, (uint32_t)ql);
         qhi[word] = set_byte(qhi[word], s & 3, (uint32_t)qh);

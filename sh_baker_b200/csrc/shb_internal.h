@@ -155,15 +155,6 @@ static_assert(sizeof(WideNode) == 80, "WideNode must be 80 bytes");
 // Internal child in slot s: count 1, position 24 + s (the traversal XORs s
 // with the ray octant, so the hit mask's bits 24..31 are in visiting order).
 
-// SHB_TRAV_FOLD: the builder leaves one quantisation step of margin on
-// every side of every child box, which lets the traversal fold the byte ->
-// float conversion of a plane into its FMA (t = (2^23 + q) s + (a - 2^23 s),
-// off by at most half a step, so the box test stays conservative).  Builder
-// and traversal read the same setting.
-#ifndef SHB_TRAV_FOLD
-#define SHB_TRAV_FOLD 0
-#endif
-
 struct BvhView {
   const WideNode* nodes;
   const float4* tris;   // 3 float4 per triangle in leaf order, v0.w = prim id
@@ -281,7 +272,7 @@ struct BakeSpec {
 
 // Launch-structure parameters (chosen by the autotuner for batches).
 #ifndef SHB_WAVE_LOG2
-#define SHB_WAVE_LOG2 23
+#define SHB_WAVE_LOG2 25
 #endif
 struct BatchParams {
   int64_t wave_paths = int64_t(1) << SHB_WAVE_LOG2;  // paths in flight per wave (queue depth)

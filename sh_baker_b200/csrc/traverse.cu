@@ -122,12 +122,6 @@ __device__ __forceinline__ float byte_f(uint32_t w, int k) {
   return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | (uint32_t)k)) - 8388608.0f;
 }
 
-#if SHB_TRAV_FOLD
-// Byte k of w as the float 2^23 + byte (one byte permute).
-__device__ __forceinline__ float byte_raw(uint32_t w, int k) {
-  return __uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u | (uint32_t)k));
-}
-#endif
 
 // Traversal state of one ray.  Groups are (base, bits): a node group has
 // kNodeGroup set, the internal-child mask in bits 8..15 and the remaining
@@ -214,15 +208,6 @@ __device__ __forceinline__ void intersect_node(const BvhView& bvh, const Walk& w
   if (oct & 4u) { uint32_t t0 = lz0, t1 = lz1; lz0 = hz0; lz1 = hz1; hz0 = t0; hz1 = t1; }
   const float tlim = w.tmax * 1.0000004f;
 #if SHB_TRAV_V2
-#if SHB_TRAV_FOLD
-  // planes decode to 2^23 + q; the 2^23 s goes into the offset
-  ax = fmaf(-8388608.0f, sx, ax);
-  ay = fmaf(-8388608.0f, sy, ay);
-  az = fmaf(-8388608.0f, sz, az);
-#define SHB_PLANE(w, k) byte_raw(w, k)
-#else
-#define SHB_PLANE(w, k) byte_f(w, k)
-#endif
   const uint32_t oct4 = oct * 0x01010101u;
   // internal children have position bits 3 and 4 both set (24..31)
   const uint32_t m_lo = n1.z ^ (__vcmpeq4(n1.z & 0x18181818u, 0x18181818u) & oct4);
@@ -232,19 +217,17 @@ __device__ __forceinline__ void intersect_node(const BvhView& bvh, const Walk& w
   for (int j = 0; j < 8; ++j) {
     const int k = j & 3;
     const uint32_t mw = j < 4 ? m_lo : m_hi;
-    float t0x = fmaf(SHB_PLANE(j < 4 ? lx0 : lx1, k), sx, ax), t1x = fmaf(SHB_PLANE(j < 4 ? hx0 : hx1, k), sx, ax);
-    float t0y = fmaf(SHB_PLANE(j < 4 ? ly0 : ly1, k), sy, ay), t1y = fmaf(SHB_PLANE(j < 4 ? hy0 : hy1, k), sy, ay);
-    float t0z = fmaf(SHB_PLANE(j < 4 ? lz0 : lz1, k), sz, az), t1z = fmaf(SHB_PLANE(j < 4 ? hz0 : hz1, k), sz, az);
+    float t0x = fmaf(byte_f(j < 4 ? lx0 : lx1, k), sx, ax), t1x = fmaf(byte_f(j < 4 ? hx0 : hx1, k), sx, ax);
+    float t0y = fmaf(byte_f(j < 4 ? ly0 : ly1, k), sy, ay), t1y = fmaf(byte_f(j < 4 ? hy0 : hy1, k), sy, ay);
+    float t0z = fmaf(byte_f(j < 4 ? lz0 : lz1, k), sz, az), t1z = fmaf(byte_f(j < 4 ? hz0 : hz1, k), sz, az);
     const float tmin_c = fmaxf(max3f(t0x, t0y, t0z), w.tnear);
     const float tmax_c = fminf(min3f(t1x, t1y, t1z), tlim);
     const uint32_t bits = bit_mask(bfe(mw, 8 * k, 5), bfe(mw, 8 * k + 5, 3));
     if (tmin_c <= tmax_c) hm |= bits;
   }
-#undef SHB_PLANE
   Gn = make_uint2(n1.x, kNodeGroup | (imask << 8) | (hm >> 24));
   Tn = make_uint2(n1.y, hm & 0x00FFFFFFu);
 #else
-  static_assert(!SHB_TRAV_FOLD, "the folded plane decode needs SHB_TRAV_V2");
   uint32_t hits_int = 0, hits_tri = 0;
 #pragma unroll
   for (int j = 0; j < 8; ++j) {
