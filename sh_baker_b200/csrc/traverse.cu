@@ -34,11 +34,6 @@ constexpr int kTravThreads = 128;
 #ifndef SHB_POSTPONE
 #define SHB_POSTPONE 0
 #endif
-// SHB_TRAV_TRI1: a step tests one triangle or visits one node (else a node
-// and all the triangles it yields)
-#ifndef SHB_TRAV_TRI1
-#define SHB_TRAV_TRI1 0
-#endif
 constexpr int kPostpone = SHB_POSTPONE;  // fewer lanes than this on triangles: postpone them
 constexpr uint32_t kNodeGroup = 0x80000000u;
 constexpr uint32_t kMaxIters = 1u << 22;  // default bound of one ray's traversal steps
@@ -261,53 +256,6 @@ __device__ __forceinline__ bool walk_step(const BvhView& bvh, Walk& w, uint2* st
     atomicOr(err, ERR_ITER);
     return true;
   }
-#if SHB_TRAV_TRI1
-  // one triangle or one node per step: a lane with a long triangle group
-  // does not hold the warp's other lanes through all of it
-  if (w.T.y) {
-    const int k = __ffs(w.T.y) - 1;
-    w.T.y &= w.T.y - 1;
-    const float4* tp = bvh.tris + 3 * (size_t)(w.T.x + k);
-    const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-    float t, u, v;
-    if (tri_test(w.r, a, b, c, w.tnear, w.tmax, t, u, v)) {
-      w.hit = true;
-      w.tmax = t;
-      w.u = u;
-      w.v = v;
-      w.prim = __float_as_uint(a.w);
-      if (ANY) return true;
-    }
-    if (w.T.y) return false;
-  } else if ((w.G.y & kNodeGroup) && (w.G.y & 0xFFu)) {
-    uint32_t hits = w.G.y & 0xFFu;
-    const uint32_t imask = (w.G.y >> 8) & 0xFFu;
-    const int bpos = __ffs(hits) - 1;
-    hits &= hits - 1;
-    const uint32_t slot = (uint32_t)bpos ^ w.r.oct;
-    const uint32_t node = w.G.x + __popc(imask & ((1u << slot) - 1u));
-    if (hits) {
-      if (w.sp < kStack) stack[w.sp++] = make_uint2(w.G.x, kNodeGroup | (imask << 8) | hits);
-      else atomicOr(err, ERR_STACK);
-    }
-    uint2 Tn;
-    intersect_node(bvh, w, node, w.G, Tn);
-    w.T = Tn;
-    if (w.T.y) return false;
-  } else if (!(w.G.y & kNodeGroup)) {
-    w.T = w.G;  // a popped triangle group, tested from the next step on
-    w.G = make_uint2(0u, 0u);
-    return false;
-  } else {
-    w.G = make_uint2(0u, 0u);
-  }
-  const bool g_empty1 = !((w.G.y & kNodeGroup) ? (w.G.y & 0xFFu) : w.G.y);
-  if (g_empty1) {
-    if (w.sp == 0) return true;
-    w.G = stack[--w.sp];
-  }
-  return false;
-#else
   bool descended = false;
   if ((w.G.y & kNodeGroup) && (w.G.y & 0xFFu)) {
     uint32_t hits = w.G.y & 0xFFu;
@@ -359,7 +307,6 @@ __device__ __forceinline__ bool walk_step(const BvhView& bvh, Walk& w, uint2* st
     w.G = stack[--w.sp];
   }
   return false;
-#endif
 }
 
 __device__ __forceinline__ void load_ray(TravRay& r, float4 o, float4 d) {
