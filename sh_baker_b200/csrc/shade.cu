@@ -286,12 +286,6 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
 // `lights` is the bake's light table in global memory or the block's copy
 // of it in shared memory.
 constexpr uint32_t kWeightCache = 32;
-// Light counts up to which the hit next-event loop keeps the weights
-// (SHB_HIT_WCACHE_MAX, at most kWeightCache); above it the pick re-evaluates
-// the lights in order until the chosen one (no per-thread array).
-#ifndef SHB_HIT_WCACHE_MAX
-#define SHB_HIT_WCACHE_MAX 32
-#endif
 
 template <bool HIT, bool BWD = false>
 __device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, f3 wo, f3 aop, float sum,
@@ -299,7 +293,7 @@ __device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N
   float target = u * sum;
   float cum = 0.f;
   int last = -1;
-  const bool cached = sc.light_count <= (HIT ? (uint32_t)SHB_HIT_WCACHE_MAX : kWeightCache);
+  const bool cached = sc.light_count <= kWeightCache;
   for (uint32_t i = 0; i < sc.light_count; ++i) {
     float w;
     LightEval e;
@@ -325,7 +319,7 @@ template <bool HIT>
 __device__ float light_weight_sum(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, f3 wo, f3 aop,
                                   float* wcache, int ws) {
   float sum = 0.0f;
-  const bool cached = sc.light_count <= (HIT ? (uint32_t)SHB_HIT_WCACHE_MAX : kWeightCache);
+  const bool cached = sc.light_count <= kWeightCache;
   for (uint32_t i = 0; i < sc.light_count; ++i) {
     float w = eval_light<HIT>(sc, lights, i, P, N, ev, wo, aop).w;
     if (cached) wcache[i * ws] = w;
@@ -679,7 +673,7 @@ __device__ __forceinline__ void nee_hit(const WaveArgs& a, const BakeItem* B, ui
                                         f3 adj, bool param, int mat_id, int cur, int i, const DLight* lights) {
   Event ev;
   ev.init(opaque_hit ? B->seed : 0u, texel, sample, vertex, EV_NEE);
-  float wcache[SHB_HIT_WCACHE_MAX > 0 ? SHB_HIT_WCACHE_MAX : 1];
+  float wcache[kWeightCache];
   const int ws = 1;
   float sum = opaque_hit ? light_weight_sum<true>(B->sc, lights, hit_pos, N, ev, wo, aop, wcache, ws) : 0.f;
   bool any_light = opaque_hit && !(sum < 1e-6f);
