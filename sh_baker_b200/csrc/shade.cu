@@ -41,10 +41,6 @@ constexpr int kThreads = 256;
 // wave is shrunk by 2^min(bounces, kMaxBranchLog).  Branch slots beyond that
 // (more than six transmissive bounces) fall back to atomic accumulation.
 constexpr int kMaxBranchLog = 6;
-#ifndef SHB_PLANE_PAD
-#define SHB_PLANE_PAD 0
-#endif
-constexpr int64_t kPlanePad = SHB_PLANE_PAD;
 // Light-loop cost from which the forward bake runs next-event estimation as
 // a kernel of its own (k_nee): punctual lights count 1, area lights 4 (each
 // samples a triangle and a point and looks up its emission).
@@ -1398,10 +1394,8 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   plan_waves(specs, n_valid, wave_paths, prm.tile_texels, share, tiles, waves);
   int64_t Pmax = 0;
   for (const Wave& w : waves) Pmax = std::max(Pmax, w.P);
-  // Queue planes (structure of arrays) are ext_cap / sh_cap entries apart;
-  // SHB_PLANE_PAD extra entries keep those strides off powers of two.
-  int64_t ext_cap = std::max<int64_t>(Pmax * mult, 1) + kPlanePad;
-  int64_t sh_cap = (Pmax + ext_cap) * NLS + kPlanePad;
+  int64_t ext_cap = std::max<int64_t>(Pmax * mult, 1);
+  int64_t sh_cap = (Pmax + ext_cap) * NLS;
   if (prm.queue_cap > 0) {  // a smaller queue drops what does not fit (ERR_QUEUE)
     ext_cap = std::min(ext_cap, prm.queue_cap);
     sh_cap = std::min(sh_cap, prm.queue_cap);
@@ -1415,7 +1409,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   SHB_TRY(c->scratch[14].reserve(sizeof(float4) * (size_t)ext_cap));
   SHB_TRY(c->scratch[15].reserve(sizeof(float4) * 3 * (size_t)sh_cap));
   SHB_TRY(c->scratch[16].reserve(sizeof(float4) * (size_t)std::max<int64_t>(Pmax, 1)));
-  SHB_TRY(c->scratch[17].reserve(sizeof(float4) * (2 * (size_t)std::max<int64_t>(Pmax, 1) * NLS + kPlanePad)));
+  SHB_TRY(c->scratch[17].reserve(sizeof(float4) * 2 * (size_t)std::max<int64_t>(Pmax, 1) * NLS));
   SHB_TRY(c->scratch[18].reserve(sizeof(PathInfo) * (size_t)std::max<int64_t>(Pmax, 1)));
   if (det) SHB_TRY(c->scratch[24].reserve(sizeof(float4) * (size_t)std::max<int64_t>(Pmax, 1) * slots * NLS));
   const int ntan = bwd ? std::max(max_b, 1) : 0, npk = ntan + 2;
@@ -1443,7 +1437,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   }
   a.path_L = c->scratch[16].as<float4>();
   a.nee_li = c->scratch[17].as<float4>();
-  a.nee_dir = a.nee_li + std::max<int64_t>(Pmax, 1) * NLS + kPlanePad;
+  a.nee_dir = a.nee_li + std::max<int64_t>(Pmax, 1) * NLS;
   a.info = c->scratch[18].as<PathInfo>();
   a.cnt = cnt;
   a.ext_cap = (int)ext_cap;
