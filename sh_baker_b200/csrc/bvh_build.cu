@@ -368,18 +368,129 @@ struct Collapse {
   int n;
   int n_int;
   int n_tri;
+  int leaf_mask;  // bit k: child k is a leaf slot (a binary leaf, or a small subtree merged into one)
+};
+
+// SAH-optimal collapse (Ylitie, Karras and Laine 2017, section 4.1): for
+// every binary node n and i = 1..7, C(n, i) is the least SAH cost of the
+// subtree at n spread over at most i child slots of its wide parent:
+//   C(n, 1) = min(leaf(n), A(n) c_node + D(n, 8)),
+//   C(n, i) = min(C(n, i - 1), D(n, i)),
+//   D(n, j) = min over 0 < k < j of C(left, k) + C(right, j - k),
+// leaf(n) = A(n) |n| for |n| <= kMaxLeaf triangles.  dec[n][i] records the
+// choice (kDecLeaf, kDecNode, kDecFewer or the split k), dec[n][8] the split
+// of D(n, 8); the collapse then reads the wide nodes off the decisions.
+#ifndef SHB_BVH_SAH_COLLAPSE
+#define SHB_BVH_SAH_COLLAPSE 1
+#endif
+constexpr int8_t kDecLeaf = -1, kDecNode = -2, kDecFewer = -3;
+struct DpCost {
+  float c[8];  // c[i] = C(n, i), i = 1..7
+};
+struct DpDec {
+  int8_t d[9];  // d[i], i = 1..8
 };
 
 __device__ __forceinline__ float node_area(const BNode& n) { return half_area(n.lo, n.hi); }
 
+// One level of binary nodes [begin, end), after all deeper levels.
+__global__ void k_dp(int begin, int end, const BNode* __restrict__ nodes, DpCost* __restrict__ cost,
+                     DpDec* __restrict__ dec) {
+  for (int n = begin + blockIdx.x * blockDim.x + threadIdx.x; n < end; n += gridDim.x * blockDim.x) {
+    const BNode& nd = nodes[n];
+    const float A = half_area(nd.lo, nd.hi);
+    DpCost C;
+    DpDec D;
+    C.c[0] = 0.f;
+    D.d[0] = 0;
+    if (nd.left < 0) {
+      const float leaf = A * (float)nd.count;
+      for (int i = 1; i < 8; ++i) {
+        C.c[i] = leaf;
+        D.d[i] = kDecLeaf;
+      }
+      D.d[8] = 0;
+    } else {
+      const DpCost L = cost[nd.left], R = cost[nd.right];
+      float dist[9];
+      int8_t arg[9];
+      for (int j = 2; j <= 8; ++j) {
+        float best = INFINITY;
+        int8_t bk = 1;
+        for (int k = 1; k < j; ++k) {
+          const float v = L.c[k] + R.c[j - k];
+          if (v < best) {
+            best = v;
+            bk = (int8_t)k;
+          }
+        }
+        dist[j] = best;
+        arg[j] = bk;
+      }
+      const float internal = A * SHB_BVH_NODE_COST + dist[8];
+      const float leaf = nd.count <= kMaxLeaf ? A * (float)nd.count : INFINITY;
+      C.c[1] = leaf <= internal ? leaf : internal;
+      D.d[1] = leaf <= internal ? kDecLeaf : kDecNode;
+      for (int i = 2; i < 8; ++i) {
+        if (C.c[i - 1] <= dist[i]) {
+          C.c[i] = C.c[i - 1];
+          D.d[i] = kDecFewer;
+        } else {
+          C.c[i] = dist[i];
+          D.d[i] = arg[i];
+        }
+      }
+      D.d[8] = arg[8];
+    }
+    cost[n] = C;
+    dec[n] = D;
+  }
+}
+
+// Children of the wide node rooted at binary node r: the 8 slots of D(r, 8)
+// spread down the recorded decisions.
+__device__ void sah_children(int r, const BNode* __restrict__ nodes, const DpDec* __restrict__ dec, Collapse& c) {
+  int st_n[16], st_i[16], sp = 0;
+  const BNode& root = nodes[r];
+  const int k8 = dec[r].d[8];
+  st_n[sp] = root.left;
+  st_i[sp++] = k8;
+  st_n[sp] = root.right;
+  st_i[sp++] = 8 - k8;
+  c.n = 0;
+  c.leaf_mask = 0;
+  while (sp > 0) {
+    const int n = st_n[--sp];
+    int i = st_i[sp];
+    const BNode& nd = nodes[n];
+    const DpDec& D = dec[n];
+    while (i > 1 && D.d[i] == kDecFewer) --i;
+    if (i == 1 || nd.left < 0 || D.d[i] == kDecLeaf) {
+      if (nd.left < 0 || D.d[1] == kDecLeaf) c.leaf_mask |= 1 << c.n;
+      c.child[c.n++] = n;
+    } else {
+      const int k = D.d[i];
+      st_n[sp] = nd.left;
+      st_i[sp++] = k;
+      st_n[sp] = nd.right;
+      st_i[sp++] = i - k;
+    }
+  }
+}
+
 __global__ void k_collapse(int n_level, const int* __restrict__ level, const BNode* __restrict__ nodes,
-                           Collapse* __restrict__ out, int* __restrict__ n_int, int* __restrict__ n_tri) {
+                           const DpDec* __restrict__ dec, Collapse* __restrict__ out, int* __restrict__ n_int,
+                           int* __restrict__ n_tri) {
   for (int w = blockIdx.x * blockDim.x + threadIdx.x; w < n_level; w += gridDim.x * blockDim.x) {
     const BNode& root = nodes[level[w]];
     Collapse c;
+    c.leaf_mask = 0;
     if (root.left < 0) {
       c.n = 1;
       c.child[0] = level[w];
+      c.leaf_mask = 1;
+    } else if (SHB_BVH_SAH_COLLAPSE) {
+      sah_children(level[w], nodes, dec, c);
     } else {
       c.n = 2;
       c.child[0] = root.left;
@@ -401,6 +512,8 @@ __global__ void k_collapse(int n_level, const int* __restrict__ level, const BNo
         c.child[best] = ch.left;
         c.child[c.n++] = ch.right;
       }
+      for (int k = 0; k < c.n; ++k)
+        if (nodes[c.child[k]].left < 0) c.leaf_mask |= 1 << k;
     }
     // octant slot assignment (greedy on centroid offsets)
     float pc[3];
@@ -436,7 +549,7 @@ __global__ void k_collapse(int n_level, const int* __restrict__ level, const BNo
     c.n_tri = 0;
     for (int k = 0; k < c.n; ++k) {
       const BNode& ch = nodes[c.child[k]];
-      if (ch.left >= 0) c.n_int++;
+      if (!((c.leaf_mask >> k) & 1)) c.n_int++;
       else c.n_tri += ch.count;
     }
     out[w] = c;
@@ -458,8 +571,12 @@ __global__ void k_emit(int n_level, int wide_base, int child_wide_base, int tri_
     const Collapse& c = col[w];
     const BNode& root = nodes[level[w]];
     int by_slot[8];
+    unsigned leaf_slots = 0;
     for (int s = 0; s < 8; ++s) by_slot[s] = -1;
-    for (int k = 0; k < c.n; ++k) by_slot[c.slot[k]] = c.child[k];
+    for (int k = 0; k < c.n; ++k) {
+      by_slot[c.slot[k]] = c.child[k];
+      if ((c.leaf_mask >> k) & 1) leaf_slots |= 1u << c.slot[k];
+    }
     WideNode nd;
     nd.px = root.lo[0];
     nd.py = root.lo[1];
@@ -487,7 +604,7 @@ __global__ void k_emit(int n_level, int wide_base, int child_wide_base, int tri_
       if (b < 0) continue;
       const BNode& ch = nodes[b];
       uint32_t meta;
-      if (ch.left >= 0) {
+      if (!((leaf_slots >> s) & 1u)) {
         imask |= 1u << s;
         meta = (1u << 5) | (24u + (uint32_t)s);  // one bit at 24 + slot (see WideNode)
         next_level[int_off[w] + r_int] = b;
@@ -589,6 +706,7 @@ shb_status build_bvh(shb_scene* s) {
     SHB_CUDA(cudaStreamSynchronize(st));
   }
   int n_act = 1, node_count = 1, depth = 0;
+  std::vector<int> level_begin = {0};  // binary nodes of depth d: [level_begin[d], level_begin[d + 1])
   size_t slot_cap = 0;
   while (n_act > 0) {
     if ((size_t)n_act > slot_cap) {
@@ -630,9 +748,24 @@ shb_status build_bvh(shb_scene* s) {
       pslot.swap(pslot2);
     }
     act.swap(act2);
+    level_begin.push_back(node_count);
     node_count += 2 * n_split;
     n_act = 2 * n_split;
     depth++;
+  }
+  level_begin.push_back(node_count);
+  // ---- SAH costs of spreading each subtree over 1..7 wide-node slots, bottom up
+  DevBuf dp_cost, dp_dec;
+  SHB_TRY(dp_cost.reserve(sizeof(DpCost) * (size_t)node_count));
+  SHB_TRY(dp_dec.reserve(sizeof(DpDec) * (size_t)node_count));
+  if (SHB_BVH_SAH_COLLAPSE) {
+    for (int d = (int)level_begin.size() - 2; d >= 0; --d) {
+      const int b0 = level_begin[(size_t)d], b1 = level_begin[(size_t)d + 1];
+      if (b1 <= b0) continue;
+      k_dp<<<grid_for(b1 - b0), kThreads, 0, st>>>(b0, b1, nodes.as<BNode>(), dp_cost.as<DpCost>(),
+                                                    dp_dec.as<DpDec>());
+      count_launch(c);
+    }
   }
   // ---- collapse into 8-wide nodes
   DevBuf col, nint, ntri, ioff, toff, lev, lev2;
@@ -657,7 +790,8 @@ shb_status build_bvh(shb_scene* s) {
   int n_level = 1, wide_count = 1, tri_count = 0, wdepth = 0;
   while (n_level > 0) {
     k_collapse<<<grid_for(n_level), kThreads, 0, st>>>(n_level, lev.as<int>(), nodes.as<BNode>(),
-                                                       col.as<Collapse>(), nint.as<int>(), ntri.as<int>());
+                                                       dp_dec.as<DpDec>(), col.as<Collapse>(), nint.as<int>(),
+                                                       ntri.as<int>());
     SHB_CUDA(cudaMemsetAsync(nint.as<int>() + n_level, 0, sizeof(int), st));
     SHB_CUDA(cudaMemsetAsync(ntri.as<int>() + n_level, 0, sizeof(int), st));
     size_t tb = tmp_all;
