@@ -465,7 +465,10 @@ __device__ void sah_children(int r, const BNode* __restrict__ nodes, const DpDec
     const BNode& nd = nodes[n];
     const DpDec& D = dec[n];
     while (i > 1 && D.d[i] == kDecFewer) --i;
-    if (i == 1 || nd.left < 0 || D.d[i] == kDecLeaf) {
+    // a split k outside 1..i-1 cannot occur; such an entry (or a full child
+    // list or stack) would end the spreading at n rather than overrun
+    const bool stop = i <= 1 || nd.left < 0 || D.d[i] < 1 || D.d[i] >= i || sp + 2 > 16 || c.n + sp + 2 > 8;
+    if (stop) {
       if (nd.left < 0 || D.d[1] == kDecLeaf) c.leaf_mask |= 1 << c.n;
       c.child[c.n++] = n;
     } else {
