@@ -175,10 +175,6 @@ __device__ __forceinline__ uint32_t bfe(uint32_t x, uint32_t pos, uint32_t len) 
   return r;
 }
 
-#ifndef SHB_TRAV_V2
-#define SHB_TRAV_V2 1
-#endif
-
 // Tests the 8 children of `node`; returns the internal children as a node
 // group and the hit leaf triangles as a triangle group.
 //
@@ -207,7 +203,6 @@ __device__ __forceinline__ void intersect_node(const BvhView& bvh, const Walk& w
   if (oct & 2u) { uint32_t t0 = ly0, t1 = ly1; ly0 = hy0; ly1 = hy1; hy0 = t0; hy1 = t1; }
   if (oct & 4u) { uint32_t t0 = lz0, t1 = lz1; lz0 = hz0; lz1 = hz1; hz0 = t0; hz1 = t1; }
   const float tlim = w.tmax * 1.0000004f;
-#if SHB_TRAV_V2
   const uint32_t oct4 = oct * 0x01010101u;
   // internal children have position bits 3 and 4 both set (24..31)
   const uint32_t m_lo = n1.z ^ (__vcmpeq4(n1.z & 0x18181818u, 0x18181818u) & oct4);
@@ -227,25 +222,6 @@ __device__ __forceinline__ void intersect_node(const BvhView& bvh, const Walk& w
   }
   Gn = make_uint2(n1.x, kNodeGroup | (imask << 8) | (hm >> 24));
   Tn = make_uint2(n1.y, hm & 0x00FFFFFFu);
-#else
-  uint32_t hits_int = 0, hits_tri = 0;
-#pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    uint32_t meta = ((j < 4 ? n1.z : n1.w) >> (8 * (j & 3))) & 0xFFu;
-    int k = j & 3;
-    float t0x = fmaf(byte_f(j < 4 ? lx0 : lx1, k), sx, ax), t1x = fmaf(byte_f(j < 4 ? hx0 : hx1, k), sx, ax);
-    float t0y = fmaf(byte_f(j < 4 ? ly0 : ly1, k), sy, ay), t1y = fmaf(byte_f(j < 4 ? hy0 : hy1, k), sy, ay);
-    float t0z = fmaf(byte_f(j < 4 ? lz0 : lz1, k), sz, az), t1z = fmaf(byte_f(j < 4 ? hz0 : hz1, k), sz, az);
-    float tmin_c = fmaxf(fmaxf(t0x, t0y), fmaxf(t0z, w.tnear));
-    float tmax_c = fminf(fminf(t1x, t1y), fminf(t1z, tlim));
-    if (meta != 0u && tmin_c <= tmax_c) {
-      if (imask & (1u << j)) hits_int |= 1u << ((uint32_t)j ^ oct);
-      else hits_tri |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
-    }
-  }
-  Gn = make_uint2(n1.x, kNodeGroup | (imask << 8) | hits_int);
-  Tn = make_uint2(n1.y, hits_tri);
-#endif
 }
 
 // One step: visit one node (or take a popped triangle group) and test the
