@@ -516,7 +516,7 @@ def l2_note(w):
     return "%s: G-buffer %.0f MB + outputs %.0f MB per step" % (kind, gb, out)
 
 
-def run_exr(args):
+def exr_result(steps: int, warmup: int, reference: bool = True, ref_runs: int = 1):
     """SaveSHLightMap of a 2048^2 lightmap (the atrium's output size) in the
     three save modes from host buffers: the library (channel packing,
     float->half and the ZIP pre-pass on the GPU, zlib on all host threads)
@@ -524,17 +524,15 @@ def run_exr(args):
     from the reference tree into oracle/_ref, one host thread; the
     cpu_baseline leg).  The texture is a seeded smooth field with 1 %
     sample noise, like a converged bake.  Wall clock per save, files to a
-    temporary directory, W warm-up saves then K timed ones per mode."""
+    temporary directory: `warmup` untimed then `steps` timed saves per mode
+    (the median), and `ref_runs` timed reference saves after one untimed."""
     import ctypes as C
     import tempfile
-    import time
 
     import numpy as np
 
     from sh_baker_b200 import _capi as A
     from sh_baker_b200 import api
-    from sh_baker_b200 import build as B
-    B.build()
     W = H = 2048
     rng = np.random.default_rng(11)
     y, x = np.mgrid[0:H, 0:W].astype(np.float32) / np.float32(W)
@@ -552,7 +550,7 @@ def run_exr(args):
     tmp = Path(tempfile.mkdtemp())
     ours, ref, files = {}, {}, {}
     ref_lib = None
-    if not args.no_cpu_baseline:
+    if reference:
         try:
             from oracle import build as OB
             path = OB.REF_LIB if OB.REF_LIB.exists() else OB.build_ref()
@@ -566,17 +564,17 @@ def run_exr(args):
     for name, m in modes.items():
         out = tmp / f"ours_{name}.exr"
         ts = []
-        for i in range(args.warmup + args.steps):
+        for i in range(warmup + steps):
             t0 = time.perf_counter()
             A.check(ctx.lib.shb_save_sh_lightmap(ctx.h, sh.ctypes.data, env.ctypes.data, W, H, 0, str(out).encode(), m))
-            if i >= args.warmup:
+            if i >= warmup:
                 ts.append(time.perf_counter() - t0)
         ours[name] = float(np.median(ts))
         files[name] = sum(p.stat().st_size for p in tmp.glob(f"ours_{name}*.exr"))
         if ref_lib is not None:
             rout = tmp / f"ref_{name}.exr"
             rts = []
-            for i in range(1 + max(1, args.steps // 2)):
+            for i in range(1 + max(1, ref_runs)):
                 t0 = time.perf_counter()
                 assert ref_lib.ref_exr_save(sh.ctypes.data, env.ctypes.data, W, H, str(rout).encode(), m) == 0
                 if i >= 1:
@@ -585,21 +583,34 @@ def run_exr(args):
     clk = clocks.stop()
     ctx.close()
     texels = W * H
-    line = {"metric": "lightmap texels saved/s (SaveSHLightMap, host buffers, median over saves)",
-            "value": texels / ours["combined"], "unit": "texels/s", "n_gpus": 1, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ours["combined"] * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32->f16", "data": "synthetic",
-            "config": {"workload": "SaveSHLightMap 2048x2048 SH9 + env visibility, three save modes",
-                       "width": W, "height": H, "host_threads": os.cpu_count()},
+    return {"value": texels / ours["combined"], "unit": "texels/s", "ms_per_save": ours["combined"] * 1e3,
+            "steps": steps, "warmup": warmup,
+            "workload": "SaveSHLightMap 2048x2048 SH9 + env visibility from host buffers, three save modes",
+            "width": W, "height": H, "host_threads": os.cpu_count(),
             "modes": {n: {"ms": ours[n] * 1e3, "bytes": files[n],
                           "reference_ms": ref[n] * 1e3 if n in ref else None,
                           "speedup": ref[n] / ours[n] if n in ref else None} for n in modes},
-            "cpu_baseline": ({"value": texels / ref["combined"], "unit": "texels/s", "cores": 1, "kind": "reference",
-                              "sample": "the whole 2048x2048 texture, reference tinyexr + miniz saver"}
-                             if "combined" in ref else None),
-            "e2e": {"value": texels / ours["combined"], "unit": "texels/s",
-                    "h2d_bytes_per_step": int(sh.nbytes + env.nbytes), "d2h_bytes_per_step": 0},
-            "clocks": clk}
+            "reference_saver": ({"value": texels / ref["combined"], "unit": "texels/s", "cores": 1,
+                                 "kind": "reference",
+                                 "sample": "the whole 2048x2048 texture, the reference's tinyexr + miniz saver"}
+                                if "combined" in ref else None),
+            "h2d_bytes_per_save": int(sh.nbytes + env.nbytes), "clocks": clk}
+
+
+def run_exr(args):
+    from sh_baker_b200 import build as B
+    B.build()
+    r = exr_result(args.steps, args.warmup, reference=not args.no_cpu_baseline, ref_runs=max(1, args.steps // 2))
+    line = {"metric": "lightmap texels saved/s (SaveSHLightMap, host buffers, median over saves)",
+            "value": r["value"], "unit": "texels/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r["ms_per_save"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32->f16", "data": "synthetic",
+            "config": {"workload": r["workload"], "width": r["width"], "height": r["height"],
+                       "host_threads": r["host_threads"]},
+            "modes": r["modes"], "cpu_baseline": r["reference_saver"],
+            "e2e": {"value": r["value"], "unit": "texels/s", "h2d_bytes_per_step": r["h2d_bytes_per_save"],
+                    "d2h_bytes_per_step": 0},
+            "clocks": r["clocks"]}
     print(json.dumps(line), flush=True)
 
 
@@ -705,7 +716,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3, help="timed end-to-end steps (after one warm-up)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--no-sub", action="store_true", help="skip the batched and adjoint sub-results")
+    ap.add_argument("--no-sub", action="store_true", help="skip the batched, adjoint and EXR sub-results")
     args = ap.parse_args()
     if args.workload in ("batched", "adjoint", "exr"):
         if args.impl == "ours" and int(os.environ.get("RANK", "0")) == 0:
@@ -847,6 +858,7 @@ def main():
             # the metric's other two parts, shortened: batched vs sequential and adjoint vs forward
             line["batched"] = batched_result(steps=2, warmup=1)
             line["adjoint"] = adjoint_result(steps=2, warmup=1)
+            line["exr"] = exr_result(steps=3, warmup=1, reference=not args.no_cpu_baseline, ref_runs=1)
     elif rank == 0:
         line["accuracy"] = None
     if rank == 0:
