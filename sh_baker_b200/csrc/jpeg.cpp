@@ -191,6 +191,12 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
       return false;
     }
     const size_t s = i + 4, e = i + 2 + len;
+    // the fixed part each segment reads before its own checks
+    const size_t need = mk == 0xC0 || mk == 0xC1 ? 6 : (mk == 0xDD ? 2 : (mk == 0xDA ? 1 : 0));
+    if (s + need > e) {
+      err = "JPEG: truncated segment";
+      return false;
+    }
     if (mk == 0xDB) {  // DQT
       size_t k = s;
       while (k < e) {
@@ -276,6 +282,10 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
         return false;
       }
       const int ns = f[s];
+      if (ns < 1 || ns > (int)comps.size() || s + 1 + 2 * (size_t)ns + 3 > e) {
+        err = "JPEG: bad scan header";
+        return false;
+      }
       std::vector<Comp*> sc;
       for (int c = 0; c < ns; ++c) {
         const int id = f[s + 1 + 2 * c], t = f[s + 2 + 2 * c];

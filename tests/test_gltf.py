@@ -263,3 +263,26 @@ def test_srgb_bytes_round_trip_through_factor(tmp_path):
     back = api.LoadScene(tmp_path / "s.gltf")
     for a, c in zip(mats, back.materials):
         np.testing.assert_array_equal(a.albedo.pixel_data, c.albedo.pixel_data)
+
+
+def test_damaged_jpeg_files_fail_cleanly(tmp_path):
+    """Truncated and bit-flipped copies of the JPEG fixtures: the loader
+    either decodes them or reports an error, without crashing."""
+    ref = np.load(Path(__file__).parent / "golden" / "jpeg_reference.npz")
+    rng = np.random.default_rng(0)
+    pos, nrm, uv, idx = quad()
+    for n in ("s420_restart", "s444_q90", "grey"):
+        good = ref[n + "_jpeg"].tobytes()
+        for t in range(40):
+            data = bytearray(good)
+            if t % 2:
+                data = data[: int(rng.integers(2, len(data)))]
+            else:
+                for _ in range(int(rng.integers(1, 6))):
+                    data[int(rng.integers(2, len(data)))] = int(rng.integers(0, 256))
+            b = GltfBuilder()
+            b.material(texture_png=bytes(data))
+            b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=0)]))
+            err = []
+            sc = api.LoadScene(b.write(tmp_path / f"{n}_{t}.gltf"), err)
+            assert sc is not None or "JPEG" in err[0], err
