@@ -1,6 +1,6 @@
 """Global relative RMSE of the GPU bake against the 4096-spp FP64 CPU oracle
 (tests/golden/fp64_<workload>.npz, made by tests/golden/make_fp64_reference.py)
-on a crop of the output lightmap (room 64x64, atrium 128x128), at the
+on a crop of the output lightmap (room 64x64, atrium 256x256), at the
 workload's own spp.
 
 The reference estimator samples primary directions uniformly over the
@@ -11,7 +11,9 @@ per-texel standard errors predict: ||se|| sqrt(4096 / spp + 1) / ||ref||
 (the bake's noise plus the fixture's own).  The GPU must reach 1 % or stay
 within 25 % of that prediction.  The reference algorithm itself (the oracle
 on the reference's mt19937 stream) is held to the same gate, which checks
-the prediction; both errors are printed.
+the prediction; both errors are printed.  To keep the CPU run to about a
+minute, the reference algorithm bakes the central 128x128 of a larger crop
+and is held to that region's own prediction.
 """
 from pathlib import Path
 
@@ -42,16 +44,30 @@ def test_relative_rmse_vs_fp64_oracle(gpu_ctx, name, spp):
     rc = api.RasterConfig(size, size, ss)
     got = api.BakeSHLightMap(sc, crop, rc, api.BakeConfig(samples=spp, bounces=bounces, seed=2024), ctx=gpu_ctx)
     g = api.DownsampleSHTexture(got.sh_texture, ss, ctx=gpu_ctx).reshape(size, size, 27)
-    osc = O.OracleScene(sc)
-    cpu = osc.bake(crop, size, size, ss, samples=spp, bounces=bounces, rng=O.RNG_MT19937)
-    c = O.downsample(cpu["sh"], size * ss, size * ss, 27, ss).reshape(size, size, 27)
     valid = ref["valid"]
     r = ref["sh"]
+
+    def predicted(v):
+        floor = float(np.linalg.norm(ref["se"][v]) / np.linalg.norm(r[v]))
+        return floor, floor * float(np.sqrt(int(ref["spp"]) / spp + 1.0))
+
     e_gpu = rel_rmse(g, r, valid)
-    e_cpu = rel_rmse(c, r, valid)
-    floor = float(np.linalg.norm(ref["se"][valid]) / np.linalg.norm(r[valid]))
-    expected = floor * float(np.sqrt(int(ref["spp"]) / spp + 1.0))
-    print(f"{name}: rel. RMSE vs FP64@{int(ref['spp'])}: GPU {e_gpu:.4f}, reference algorithm {e_cpu:.4f}, "
-          f"unbiased estimator predicted {expected:.4f} (FP64 reference's own error {floor:.4f}) at {spp} spp")
-    assert e_cpu <= max(0.01, 1.25 * expected), (e_cpu, expected)
+    floor, expected = predicted(valid)
+    # the reference algorithm on the central (at most) 128x128 of the crop
+    sub = min(size, 128)
+    o = (size - sub) // 2
+    cpts = np.ascontiguousarray(crop.reshape(size * ss, size * ss)[o * ss:(o + sub) * ss, o * ss:(o + sub) * ss])
+    osc = O.OracleScene(sc)
+    cpu = osc.bake(cpts.reshape(-1), sub, sub, ss, samples=spp, bounces=bounces, rng=O.RNG_MT19937)
+    c = O.downsample(cpu["sh"], sub * ss, sub * ss, 27, ss).reshape(sub, sub, 27)
+    vsub = np.zeros_like(valid)
+    vsub[o:o + sub, o:o + sub] = valid[o:o + sub, o:o + sub]
+    cfull = np.zeros_like(r)
+    cfull[o:o + sub, o:o + sub] = c
+    e_cpu = rel_rmse(cfull, r, vsub)
+    _, expected_cpu = predicted(vsub)
+    print(f"{name}: rel. RMSE vs FP64@{int(ref['spp'])}: GPU {e_gpu:.4f} (predicted {expected:.4f}, "
+          f"{size}x{size}), reference algorithm {e_cpu:.4f} (predicted {expected_cpu:.4f}, {sub}x{sub}); "
+          f"FP64 reference's own error {floor:.4f}; {spp} spp")
+    assert e_cpu <= max(0.01, 1.25 * expected_cpu), (e_cpu, expected_cpu)
     assert e_gpu <= max(0.01, 1.25 * expected), (e_gpu, expected)
