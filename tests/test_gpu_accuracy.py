@@ -71,3 +71,33 @@ def test_relative_rmse_vs_fp64_oracle(gpu_ctx, name, spp):
           f"FP64 reference's own error {floor:.4f}; {spp} spp")
     assert e_cpu <= max(0.01, 1.25 * expected_cpu), (e_cpu, expected_cpu)
     assert e_gpu <= max(0.01, 1.25 * expected), (e_gpu, expected)
+
+
+@pytest.mark.parametrize("name", ["room", "atrium"])
+def test_systematic_error_below_one_percent(gpu_ctx, name):
+    """The GPU bake at the fixture's own 4096 spp against the FP64 fixture:
+    two independent 4096-spp estimates differ by their noise (sqrt 2 times
+    the fixture's own error, from its per-texel standard errors) plus any
+    systematic error.  What is left of ||x - o||^2 after the noise is taken
+    out, relative to ||o||, must stay under 1 %: the bake converges to the
+    FP64 oracle's value within 1 %.  (The noise estimate itself is good to
+    a few tenths of a percent over the crop's ~10^5 coefficients.)"""
+    ref = np.load(GOLDEN / f"fp64_{name}.npz")
+    w, h, ss, size, x0, y0 = (int(ref[k]) for k in ("width", "height", "ss", "size", "x0", "y0"))
+    sc = FACTORY[name]()
+    pts = api.RasterizeScene(sc, api.RasterConfig(w, h, ss), ctx=gpu_ctx).reshape(h * ss, w * ss)
+    crop = np.ascontiguousarray(pts[y0 * ss:(y0 + size) * ss, x0 * ss:(x0 + size) * ss]).reshape(-1)
+    rc = api.RasterConfig(size, size, ss)
+    got = api.BakeSHLightMap(sc, crop, rc, api.BakeConfig(samples=int(ref["spp"]), bounces=int(ref["bounces"]),
+                                                          seed=777), ctx=gpu_ctx)
+    g = api.DownsampleSHTexture(got.sh_texture, ss, ctx=gpu_ctx).reshape(size, size, 27).astype(np.float64)
+    valid = ref["valid"]
+    r = ref["sh"].astype(np.float64)
+    d2 = float(np.sum((g - r)[valid] ** 2))
+    o2 = float(np.sum(r[valid] ** 2))
+    se2 = float(np.sum(ref["se"].astype(np.float64)[valid] ** 2))
+    total = (d2 / o2) ** 0.5
+    noise = (2 * se2 / o2) ** 0.5
+    systematic = max(0.0, d2 - 2 * se2) ** 0.5 / o2 ** 0.5
+    print(f"{name}: at {int(ref['spp'])} spp rel. RMSE {total:.4f}, noise {noise:.4f}, systematic {systematic:.4f}")
+    assert systematic < 0.01, (total, noise, systematic)
