@@ -663,8 +663,8 @@ def accuracy_at_fixture_spp(w, scene, ctx):
     """The bake of the FP64 fixture's crop at the fixture's own spp (4096):
     relative RMSE against the fixture, the noise floor two independent
     4096-spp estimates have (sqrt 2 x the fixture's own error), the
-    systematic part left after that noise is taken out, and the GPU rate of
-    that bake (CUDA events, BVH already built)."""
+    systematic part as the per-channel relative bias of the summed
+    difference (with its standard error), and the rate of that bake."""
     import numpy as np
     import torch
 
@@ -696,11 +696,19 @@ def accuracy_at_fixture_spp(w, scene, ctx):
     valid, r = ref["valid"], ref["sh"].astype(np.float64)
     d2 = float(np.sum((got - r)[valid] ** 2))
     o2 = float(np.sum(r[valid] ** 2))
-    se2 = float(np.sum(ref["se"].astype(np.float64)[valid] ** 2))
+    se = ref["se"].astype(np.float64)
+    se2 = float(np.sum(se[valid] ** 2))
+    # systematic part: per SH channel, the summed difference over the crop
+    # relative to the summed magnitude (the noise averages down)
+    mag = np.abs(r[valid]).sum(axis=0)
+    bias = (got - r)[valid].sum(axis=0) / mag
+    bias_se = np.sqrt(2.0 * (se[valid] ** 2).sum(axis=0)) / mag
     g.close()
     ds.close()
     return {"spp": spp, "rel_rmse_vs_fp64": (d2 / o2) ** 0.5, "noise_floor": (2 * se2 / o2) ** 0.5,
-            "systematic_est": max(0.0, d2 - 2 * se2) ** 0.5 / o2 ** 0.5,
+            "channel_bias": {"l0_rgb": [float(v) for v in bias[:3]], "max_abs": float(np.abs(bias).max()),
+                             "max_abs_over_se": float(np.max(np.abs(bias) / bias_se)),
+                             "se_of_max": float(bias_se[int(np.argmax(np.abs(bias)))])},
             "texel_samples_per_s": st.texel_samples / dt, "seconds": dt}
 
 

@@ -73,15 +73,27 @@ def test_relative_rmse_vs_fp64_oracle(gpu_ctx, name, spp):
     assert e_gpu <= max(0.01, 1.25 * expected), (e_gpu, expected)
 
 
+def channel_bias(x, o, se, valid):
+    """Per SH coefficient channel c: the relative bias sum(x_c - o_c) /
+    sum |o_c| over the valid texels, and its standard error when x and o
+    are independent estimates with the fixture's per-texel standard errors."""
+    d = (x - o)[valid].astype(np.float64)
+    a = np.abs(o[valid].astype(np.float64)).sum(axis=0)
+    se_sum = np.sqrt(2.0 * (se[valid].astype(np.float64) ** 2).sum(axis=0))
+    return d.sum(axis=0) / a, se_sum / a
+
+
 @pytest.mark.parametrize("name", ["room", "atrium"])
 def test_systematic_error_below_one_percent(gpu_ctx, name):
-    """The GPU bake at the fixture's own 4096 spp against the FP64 fixture:
-    two independent 4096-spp estimates differ by their noise (sqrt 2 times
-    the fixture's own error, from its per-texel standard errors) plus any
-    systematic error.  What is left of ||x - o||^2 after the noise is taken
-    out, relative to ||o||, must stay under 1 %: the bake converges to the
-    FP64 oracle's value within 1 %.  (The noise estimate itself is good to
-    a few tenths of a percent over the crop's ~10^5 coefficients.)"""
+    """The GPU bake at the fixture's own 4096 spp against the FP64 fixture.
+    Two independent 4096-spp estimates differ by their noise, which the
+    fixture's per-texel standard errors give.  (1) The relative RMSE stays
+    within 25 % of that noise floor (sqrt 2 times the fixture's own error).
+    (2) The 1 % gate on what is systematic: in every one of the 27 SH
+    channels the summed difference over the crop, relative to the summed
+    magnitude, is at most 1 % plus 3 of its standard errors.  Summing over
+    the crop's texels averages the noise down, so the bias is resolved far
+    below 1 %, where the RMSE itself is dominated by noise."""
     ref = np.load(GOLDEN / f"fp64_{name}.npz")
     w, h, ss, size, x0, y0 = (int(ref[k]) for k in ("width", "height", "ss", "size", "x0", "y0"))
     sc = FACTORY[name]()
@@ -93,11 +105,12 @@ def test_systematic_error_below_one_percent(gpu_ctx, name):
     g = api.DownsampleSHTexture(got.sh_texture, ss, ctx=gpu_ctx).reshape(size, size, 27).astype(np.float64)
     valid = ref["valid"]
     r = ref["sh"].astype(np.float64)
-    d2 = float(np.sum((g - r)[valid] ** 2))
-    o2 = float(np.sum(r[valid] ** 2))
-    se2 = float(np.sum(ref["se"].astype(np.float64)[valid] ** 2))
-    total = (d2 / o2) ** 0.5
-    noise = (2 * se2 / o2) ** 0.5
-    systematic = max(0.0, d2 - 2 * se2) ** 0.5 / o2 ** 0.5
-    print(f"{name}: at {int(ref['spp'])} spp rel. RMSE {total:.4f}, noise {noise:.4f}, systematic {systematic:.4f}")
-    assert systematic < 0.01, (total, noise, systematic)
+    total = rel_rmse(g, r, valid)
+    noise = float(np.sqrt(2.0) * np.linalg.norm(ref["se"][valid]) / np.linalg.norm(r[valid]))
+    bias, bias_se = channel_bias(g, r, ref["se"], valid)
+    worst = int(np.argmax(np.abs(bias) - 3 * bias_se))
+    print(f"{name}: at {int(ref['spp'])} spp rel. RMSE {total:.4f} (noise floor {noise:.4f}); channel bias "
+          f"|b| max {np.abs(bias).max():.4f}, L0 {bias[0]:+.4f} {bias[1]:+.4f} {bias[2]:+.4f}, "
+          f"worst channel {worst}: {bias[worst]:+.4f} +- {bias_se[worst]:.4f}")
+    assert total <= 1.25 * noise, (total, noise)
+    assert (np.abs(bias) <= 0.01 + 3 * bias_se).all(), (bias, bias_se)
