@@ -186,9 +186,13 @@ struct LightEval {
 
 // Incoming radiance without visibility (src/light.h:34-49,72-95,117-144,
 // 166-188); with HIT, times cos x BRDF (src/light.h:51-203).
-template <bool HIT, bool BWD = false>
-__device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint32_t li, f3 P, f3 N, Event& ev, f3 wo,
-                                f3 aop) {
+// ONLY: 0 any light, 1 the caller knows li is punctual (point, spot,
+// directional), 2 it knows li is an area light; the other branches are not
+// compiled, which keeps the loop bodies of a split weight pass small.
+template <bool HIT, bool BWD = false, int ONLY = 0>
+__device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint32_t li, f3 P, f3 N, Event& ev,
+                                bool wo_back, f3 aop) {
+  constexpr bool kPunct = ONLY != 2, kArea = ONLY != 1;
   const DLight& L = lights[li];
   LightEval e;
   e.apdf = 1.0f;
@@ -202,7 +206,7 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
   f3 color = {L.cr, L.cg, L.cb};
   float cos_n;
   f3 incident;
-  if (L.type == SHB_LIGHT_DIRECTIONAL) {
+  if (kPunct && L.type == SHB_LIGHT_DIRECTIONAL) {
     f3 dir = {L.dx, L.dy, L.dz};
     e.ray_d = -dir;
     e.tfar = 1.0e10f;
@@ -213,9 +217,10 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
       e.lpar = 1;
       e.dpar = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : color;
     }
-  } else if (L.type == SHB_LIGHT_POINT || L.type == SHB_LIGHT_SPOT || L.type == SHB_LIGHT_AREA) {
+  } else if ((kPunct && (L.type == SHB_LIGHT_POINT || L.type == SHB_LIGHT_SPOT)) ||
+             (kArea && L.type == SHB_LIGHT_AREA)) {
     f3 target, arad = {0.f, 0.f, 0.f};
-    if (L.type == SHB_LIGHT_AREA) sample_area(sc, L, ev, 3 * L.area_ord, target, arad, e.apdf);
+    if (kArea && (!kPunct || L.type == SHB_LIGHT_AREA)) sample_area(sc, L, ev, 3 * L.area_ord, target, arad, e.apdf);
     else target = {L.px, L.py, L.pz};
     f3 Lv = target - P;
     float dist_sq = sqnorm(Lv);
@@ -225,13 +230,13 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
     Lv = Lv / dist;
     incident = Lv;
     cos_n = dot(N, Lv);
-    if (L.type == SHB_LIGHT_POINT) {
+    if (kPunct && L.type == SHB_LIGHT_POINT) {
       e.rad = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : L.intensity * color / (dist * dist);
       if (BWD) {
         e.lpar = 1;
         e.dpar = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : color / (dist * dist);
       }
-    } else if (L.type == SHB_LIGHT_SPOT) {
+    } else if (kPunct && L.type == SHB_LIGHT_SPOT) {
       float cos_l = dot(f3{L.dx, L.dy, L.dz}, -Lv);
       float falloff = (cos_l - L.cos_outer) / (L.cos_inner - L.cos_outer);
       falloff = fminf(fmaxf(falloff, 0.0f), 1.0f);
@@ -262,7 +267,7 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
       e.rad = {0.f, 0.f, 0.f};
       if (BWD) e.dpar = {0.f, 0.f, 0.f};
     } else {
-      bool zero = dot(N, wo) <= 0.0f || dot(N, incident) <= 0.0f;
+      bool zero = wo_back || dot(N, incident) <= 0.0f;
       f3 brdf = zero ? f3{0.f, 0.f, 0.f} : aop;
       if (BWD) {
         e.dpar = cmul(e.dpar, cos_n * brdf);
@@ -288,7 +293,8 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
 constexpr uint32_t kWeightCache = 32;
 
 template <bool HIT, bool BWD = false>
-__device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, f3 wo, f3 aop, float sum,
+__device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, bool wo_back, f3 aop,
+                           float sum,
                            float u, const float* wcache, int ws, LightEval& out) {
   float target = u * sum;
   float cum = 0.f;
@@ -300,28 +306,45 @@ __device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N
     if (cached) {
       w = wcache[i * ws];
     } else {
-      e = eval_light<HIT, BWD>(sc, lights, i, P, N, ev, wo, aop);
+      e = eval_light<HIT, BWD>(sc, lights, i, P, N, ev, wo_back, aop);
       w = e.w;
     }
     cum += w;
     if (w > 0.f) last = (int)i;
     if (target < cum) {
-      out = cached ? eval_light<HIT, BWD>(sc, lights, i, P, N, ev, wo, aop) : e;
+      out = cached ? eval_light<HIT, BWD>(sc, lights, i, P, N, ev, wo_back, aop) : e;
       return true;
     }
   }
   if (last < 0) return false;
-  out = eval_light<HIT, BWD>(sc, lights, (uint32_t)last, P, N, ev, wo, aop);
+  out = eval_light<HIT, BWD>(sc, lights, (uint32_t)last, P, N, ev, wo_back, aop);
   return true;
 }
 
+// SHB_NEE_SPLIT_TYPES: with the weights cached, the hit weight pass runs one
+// loop over the punctual lights and one over the area lights (smaller loop
+// bodies, fewer spilled registers), then sums the cached weights in light
+// order, so the sum is the same float sum.
+#ifndef SHB_NEE_SPLIT_TYPES
+#define SHB_NEE_SPLIT_TYPES 0
+#endif
+
 template <bool HIT>
-__device__ float light_weight_sum(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, f3 wo, f3 aop,
+__device__ float light_weight_sum(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, bool wo_back,
+                                  f3 aop,
                                   float* wcache, int ws) {
   float sum = 0.0f;
   const bool cached = sc.light_count <= kWeightCache;
+  if (SHB_NEE_SPLIT_TYPES && HIT && cached) {
+    for (uint32_t i = 0; i < sc.light_count; ++i)
+      if (lights[i].type != SHB_LIGHT_AREA) wcache[i * ws] = eval_light<HIT, false, 1>(sc, lights, i, P, N, ev, wo_back, aop).w;
+    for (uint32_t i = 0; i < sc.light_count; ++i)
+      if (lights[i].type == SHB_LIGHT_AREA) wcache[i * ws] = eval_light<HIT, false, 2>(sc, lights, i, P, N, ev, wo_back, aop).w;
+    for (uint32_t i = 0; i < sc.light_count; ++i) sum += wcache[i * ws];
+    return sum;
+  }
   for (uint32_t i = 0; i < sc.light_count; ++i) {
-    float w = eval_light<HIT>(sc, lights, i, P, N, ev, wo, aop).w;
+    float w = eval_light<HIT>(sc, lights, i, P, N, ev, wo_back, aop).w;
     if (cached) wcache[i * ws] = w;
     sum += w;
   }
@@ -596,7 +619,7 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
       const uint32_t nl = BL->sc.light_count;
       const DLight* ll = wave_lights ? wave_lights : BL->sc.lights;
       const float mine =
-          (uint32_t)lane < nl ? eval_light<false>(BL->sc, ll, (uint32_t)lane, Pl, Nl, ev, zero3, zero3).w : 0.f;
+          (uint32_t)lane < nl ? eval_light<false>(BL->sc, ll, (uint32_t)lane, Pl, Nl, ev, true, zero3).w : 0.f;
       for (uint32_t i = 0; i < nl; ++i) {
         const float w = __shfl_sync(0xFFFFFFFFu, mine, (int)i);
         wcache[i * ws] = w;
@@ -604,7 +627,7 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
       }
       if (!active) sum = 0.f;
     } else if (active) {
-      sum = light_weight_sum<false>(B->sc, lights, P0, N, ev, zero3, zero3, wcache, ws);
+      sum = light_weight_sum<false>(B->sc, lights, P0, N, ev, true, zero3, wcache, ws);
     }
     bool any_light = active && !(sum < 1e-6f);
     const int nls = active ? B->nls : 0;
@@ -613,7 +636,7 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
       bool ok = false;
       float joint = 1.f;
       if (any_light && j < nls) {
-        ok = pick_light<false, BWD>(B->sc, lights, P0, N, ev, zero3, zero3, sum,
+        ok = pick_light<false, BWD>(B->sc, lights, P0, N, ev, true, zero3, sum,
                                     ev.u(3 * (int)B->sc.area_light_count + j), wcache, ws, e);
         if (ok) {
           float pdf = e.w / sum;
@@ -675,7 +698,9 @@ __device__ __forceinline__ void nee_hit(const WaveArgs& a, const BakeItem* B, ui
   ev.init(opaque_hit ? B->seed : 0u, texel, sample, vertex, EV_NEE);
   float wcache[kWeightCache];
   const int ws = 1;
-  float sum = opaque_hit ? light_weight_sum<true>(B->sc, lights, hit_pos, N, ev, wo, aop, wcache, ws) : 0.f;
+  // dot(N, wo) <= 0 zeroes the BRDF of every light alike: evaluated once
+  const bool wo_back = dot(N, wo) <= 0.0f;
+  float sum = opaque_hit ? light_weight_sum<true>(B->sc, lights, hit_pos, N, ev, wo_back, aop, wcache, ws) : 0.f;
   bool any_light = opaque_hit && !(sum < 1e-6f);
   const int nls = opaque_hit ? B->nls : 0;
   for (int j = 0; j < a.NLS; ++j) {
@@ -684,7 +709,7 @@ __device__ __forceinline__ void nee_hit(const WaveArgs& a, const BakeItem* B, ui
     f3 c = {0.f, 0.f, 0.f};
     float scale = 0.f;
     if (any_light && j < nls) {
-      ok = pick_light<true, BWD>(B->sc, lights, hit_pos, N, ev, wo, aop, sum,
+      ok = pick_light<true, BWD>(B->sc, lights, hit_pos, N, ev, wo_back, aop, sum,
                                  ev.u(3 * (int)B->sc.area_light_count + j), wcache, ws, e);
       if (ok) {
         float pdf = e.w / sum;
