@@ -186,13 +186,9 @@ struct LightEval {
 
 // Incoming radiance without visibility (src/light.h:34-49,72-95,117-144,
 // 166-188); with HIT, times cos x BRDF (src/light.h:51-203).
-// ONLY: 0 any light, 1 the caller knows li is punctual (point, spot,
-// directional), 2 it knows li is an area light; the other branches are not
-// compiled, which keeps the loop bodies of a split weight pass small.
-template <bool HIT, bool BWD = false, int ONLY = 0>
+template <bool HIT, bool BWD = false>
 __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint32_t li, f3 P, f3 N, Event& ev,
                                 bool wo_back, f3 aop) {
-  constexpr bool kPunct = ONLY != 2, kArea = ONLY != 1;
   const DLight& L = lights[li];
   LightEval e;
   e.apdf = 1.0f;
@@ -206,7 +202,7 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
   f3 color = {L.cr, L.cg, L.cb};
   float cos_n;
   f3 incident;
-  if (kPunct && L.type == SHB_LIGHT_DIRECTIONAL) {
+  if (L.type == SHB_LIGHT_DIRECTIONAL) {
     f3 dir = {L.dx, L.dy, L.dz};
     e.ray_d = -dir;
     e.tfar = 1.0e10f;
@@ -217,10 +213,9 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
       e.lpar = 1;
       e.dpar = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : color;
     }
-  } else if ((kPunct && (L.type == SHB_LIGHT_POINT || L.type == SHB_LIGHT_SPOT)) ||
-             (kArea && L.type == SHB_LIGHT_AREA)) {
+  } else if (L.type == SHB_LIGHT_POINT || L.type == SHB_LIGHT_SPOT || L.type == SHB_LIGHT_AREA) {
     f3 target, arad = {0.f, 0.f, 0.f};
-    if (kArea && (!kPunct || L.type == SHB_LIGHT_AREA)) sample_area(sc, L, ev, 3 * L.area_ord, target, arad, e.apdf);
+    if (L.type == SHB_LIGHT_AREA) sample_area(sc, L, ev, 3 * L.area_ord, target, arad, e.apdf);
     else target = {L.px, L.py, L.pz};
     f3 Lv = target - P;
     float dist_sq = sqnorm(Lv);
@@ -230,13 +225,13 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
     Lv = Lv / dist;
     incident = Lv;
     cos_n = dot(N, Lv);
-    if (kPunct && L.type == SHB_LIGHT_POINT) {
+    if (L.type == SHB_LIGHT_POINT) {
       e.rad = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : L.intensity * color / (dist * dist);
       if (BWD) {
         e.lpar = 1;
         e.dpar = cos_n < 0.f ? f3{0.f, 0.f, 0.f} : color / (dist * dist);
       }
-    } else if (kPunct && L.type == SHB_LIGHT_SPOT) {
+    } else if (L.type == SHB_LIGHT_SPOT) {
       float cos_l = dot(f3{L.dx, L.dy, L.dz}, -Lv);
       float falloff = (cos_l - L.cos_outer) / (L.cos_inner - L.cos_outer);
       falloff = fminf(fmaxf(falloff, 0.0f), 1.0f);
@@ -321,28 +316,12 @@ __device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N
   return true;
 }
 
-// SHB_NEE_SPLIT_TYPES: with the weights cached, the hit weight pass runs one
-// loop over the punctual lights and one over the area lights (smaller loop
-// bodies, fewer spilled registers), then sums the cached weights in light
-// order, so the sum is the same float sum.
-#ifndef SHB_NEE_SPLIT_TYPES
-#define SHB_NEE_SPLIT_TYPES 0
-#endif
-
 template <bool HIT>
 __device__ float light_weight_sum(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, bool wo_back,
                                   f3 aop,
                                   float* wcache, int ws) {
   float sum = 0.0f;
   const bool cached = sc.light_count <= kWeightCache;
-  if (SHB_NEE_SPLIT_TYPES && HIT && cached) {
-    for (uint32_t i = 0; i < sc.light_count; ++i)
-      if (lights[i].type != SHB_LIGHT_AREA) wcache[i * ws] = eval_light<HIT, false, 1>(sc, lights, i, P, N, ev, wo_back, aop).w;
-    for (uint32_t i = 0; i < sc.light_count; ++i)
-      if (lights[i].type == SHB_LIGHT_AREA) wcache[i * ws] = eval_light<HIT, false, 2>(sc, lights, i, P, N, ev, wo_back, aop).w;
-    for (uint32_t i = 0; i < sc.light_count; ++i) sum += wcache[i * ws];
-    return sum;
-  }
   for (uint32_t i = 0; i < sc.light_count; ++i) {
     float w = eval_light<HIT>(sc, lights, i, P, N, ev, wo_back, aop).w;
     if (cached) wcache[i * ws] = w;
