@@ -107,8 +107,8 @@ __device__ __forceinline__ float max_coeff_std(f3 a) {
 // float4 {v0, pdf}, {v1, uv0.x}, {v2, uv0.y}, {uv1, uv2} with object-space
 // vertices and pdf = max(1e-6, 1 / (n * area)) computed by the expressions
 // of SampleAreaLight, so a sample reads one 64-byte record instead of the
-// index, vertex and uv gathers.  area_info[area light] = (first record,
-// triangle count | has-texture-uv << 31).
+// index, vertex and uv gathers.  The light record carries its first record
+// and its triangle count | has-texture-uv << 31.
 constexpr uint32_t kAreaHasUv = 0x80000000u;
 
 __device__ __forceinline__ float area_pdf(f3 v0, f3 v1, f3 v2, uint32_t n) {
@@ -124,11 +124,10 @@ __device__ void sample_area(const SceneView& sc, const DLight& L, Event& ev, int
   rad = {0.f, 0.f, 0.f};
   pdf = 0.f;
   if (L.geom < 0 || L.mat < 0) return;
-  const uint2 info = sc.area_info[L.area_ord];
-  const uint32_t n = info.y & ~kAreaHasUv;
+  const uint32_t n = L.area_count & ~kAreaHasUv;
   if (n == 0) return;
   uint32_t tri = ev.tri(ubase, n);
-  const float4* r = sc.area_tris + 4 * ((size_t)info.x + tri);
+  const float4* r = sc.area_tris + 4 * ((size_t)L.area_first + tri);
   const float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
   float u1 = ev.u(ubase + 1);
   float u2 = ev.u(ubase + 2);
@@ -143,7 +142,7 @@ __device__ void sample_area(const SceneView& sc, const DLight& L, Event& ev, int
     rad = {L.er, L.eg, L.eb};
   } else {
     f2 uv = {0.f, 0.f};
-    if (info.y & kAreaHasUv) uv = w * f2{b.w, c.w} + u1 * f2{d.x, d.y} + u2 * f2{d.z, d.w};
+    if (L.area_count & kAreaHasUv) uv = w * f2{b.w, c.w} + u1 * f2{d.x, d.y} + u2 * f2{d.z, d.w};
     rad = get_emission(sc, load_mat(sc, L.mat), uv);
   }
   pdf = a.w;
@@ -286,6 +285,11 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
 // `lights` is the bake's light table in global memory or the block's copy
 // of it in shared memory.
 constexpr uint32_t kWeightCache = 32;
+// Texel next-event estimation shares the punctual lights' weights across a
+// warp of one texel's samples also in scenes with area lights.
+#ifndef SHB_TEXEL_COOP_AREA
+#define SHB_TEXEL_COOP_AREA 1
+#endif
 
 template <bool HIT, bool BWD = false>
 __device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N, Event& ev, bool wo_back, f3 aop,
@@ -578,17 +582,19 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
     const int ws = 1;
     const DLight* lights = wave_lights ? wave_lights : B->sc.lights;
     float sum = 0.f;
-    // Without area lights the weights depend on the texel only.  When the
-    // warp's paths all belong to one texel (spp >= 32 mostly), lane j
-    // evaluates light j and the lanes share the weights by shuffle; each
-    // lane still sums them in light order, so the result is the same.
+    // The weights of point, spot and directional lights depend on the texel
+    // only.  When the warp's paths all belong to one texel (spp >= 32
+    // mostly), lane j evaluates light j if it is one of those and the lanes
+    // share the weights by shuffle; area lights, which sample a point per
+    // path, are evaluated by every lane for its own path.  Each lane still
+    // sums the weights in light order, so the result is the same.
     const unsigned act = __ballot_sync(0xFFFFFFFFu, active);
     const uint64_t key = active ? ((uint64_t)b << 32 | texel) : ~0ull;
     const int lead = act ? __ffs(act) - 1 : 0;
     const uint64_t key0 = __shfl_sync(0xFFFFFFFFu, key, lead);
-    const bool coop =
-        act && __all_sync(0xFFFFFFFFu, !active || (key == key0 && B->sc.area_light_count == 0 &&
-                                                   B->sc.light_count <= kWeightCache));
+    const bool coop = act && __all_sync(0xFFFFFFFFu, !active || (key == key0 &&
+                                                                 (SHB_TEXEL_COOP_AREA || B->sc.area_light_count == 0) &&
+                                                                 B->sc.light_count <= kWeightCache));
     if (coop) {
       const BakeItem* BL = a.bakes + (uint32_t)(key0 >> 32);
       const f3 Pl = {__shfl_sync(0xFFFFFFFFu, P0.x, lead), __shfl_sync(0xFFFFFFFFu, P0.y, lead),
@@ -597,10 +603,13 @@ __global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
                      __shfl_sync(0xFFFFFFFFu, N.z, lead)};
       const uint32_t nl = BL->sc.light_count;
       const DLight* ll = wave_lights ? wave_lights : BL->sc.lights;
-      const float mine =
-          (uint32_t)lane < nl ? eval_light<false>(BL->sc, ll, (uint32_t)lane, Pl, Nl, ev, true, zero3).w : 0.f;
+      const float mine = (uint32_t)lane < nl && ll[lane].type != SHB_LIGHT_AREA
+                             ? eval_light<false>(BL->sc, ll, (uint32_t)lane, Pl, Nl, ev, true, zero3).w
+                             : 0.f;
       for (uint32_t i = 0; i < nl; ++i) {
-        const float w = __shfl_sync(0xFFFFFFFFu, mine, (int)i);
+        float w;
+        if (ll[i].type != SHB_LIGHT_AREA) w = __shfl_sync(0xFFFFFFFFu, mine, (int)i);
+        else w = active ? eval_light<false>(BL->sc, ll, i, P0, N, ev, true, zero3).w : 0.f;
         wcache[i * ws] = w;
         sum += w;
       }
@@ -1175,19 +1184,22 @@ void srgb_upload(const float table[256]) { cudaMemcpyToSymbol(g_srgb, table, siz
 
 // Area-light triangle records of a scene (see sample_area).
 shb_status build_area_tris(shb_scene* s) {
-  std::vector<uint2> info(std::max<uint32_t>(s->area_light_count, 1), make_uint2(0u, 0u));
   std::vector<uint4> entries;
-  for (const DLight& L : s->h_lights) {
+  for (DLight& L : s->h_lights) {
+    L.area_first = 0;
+    L.area_count = 0;
     if (L.type != SHB_LIGHT_AREA || L.area_ord < 0) continue;
     if (L.geom < 0 || L.mat < 0 || (size_t)L.geom >= s->h_geoms.size()) continue;
     const DGeom& g = s->h_geoms[(size_t)L.geom];
     const uint32_t has_uv = (g.flags & GEOM_HAS_TEXUV) ? 1u : 0u;
-    info[(size_t)L.area_ord] = make_uint2((uint32_t)entries.size(), g.tri_count | (has_uv ? kAreaHasUv : 0u));
+    L.area_first = (uint32_t)entries.size();
+    L.area_count = g.tri_count | (has_uv ? kAreaHasUv : 0u);
     for (uint32_t t = 0; t < g.tri_count; ++t) entries.push_back(make_uint4(g.prim_base + t, g.tri_count, has_uv, 0u));
   }
   cudaStream_t st = s->ctx->stream;
-  SHB_TRY(s->area_info.reserve(sizeof(uint2) * info.size()));
-  SHB_CUDA(cudaMemcpyAsync(s->area_info.ptr, info.data(), sizeof(uint2) * info.size(), cudaMemcpyHostToDevice, st));
+  if (!s->h_lights.empty())
+    SHB_CUDA(cudaMemcpyAsync(s->lights.ptr, s->h_lights.data(), sizeof(DLight) * s->h_lights.size(),
+                             cudaMemcpyHostToDevice, st));
   SHB_TRY(s->area_tris.reserve(sizeof(float4) * 4 * std::max<size_t>(entries.size(), 1)));
   if (!entries.empty()) {
     DevBuf tmp;

@@ -317,7 +317,6 @@ SceneView shb_scene::view() const {
   v.pixels = pixels.as<uint8_t>();
   v.lights = lights.as<DLight>();
   v.area_tris = area_tris.as<float4>();
-  v.area_info = area_info.as<uint2>();
   v.geom_count = geom_count;
   v.mat_count = mat_count;
   v.light_count = light_count;

@@ -132,6 +132,10 @@ struct DLight {
   // host with the device's operations; emis_const 0: look it up per sample
   float er, eg, eb;
   int32_t emis_const;
+  // area: the light's first triangle record (shade.cu sample_area) and its
+  // triangle count | has-texture-uv << 31, so a sample reads them with the
+  // light instead of from a separate table
+  uint32_t area_first, area_count;
 };
 
 // Compressed 8-wide BVH node (80 bytes).  Children boxes are quantised on
@@ -176,7 +180,6 @@ struct SceneView {
   const uint8_t* pixels;
   const DLight* lights;
   const float4* area_tris;  // 4 per area-light triangle (shade.cu sample_area)
-  const uint2* area_info;   // per area light: first record, count | uv flag
   uint32_t geom_count, mat_count, light_count, area_light_count;
   uint32_t prim_count, vertex_count;
   int32_t has_alpha;     // any material with 4-channel albedo
@@ -211,7 +214,7 @@ struct shb_scene {
   // uploaded per-vertex arrays
   shb::DevBuf obj_v, obj_n, tex_uv, lm_uv, obj_t, world_v, world_n, world_t;
   shb::DevBuf tri_vidx, tri_geom, geoms, mats, pixels, lights, rot, lin, vgeom;
-  shb::DevBuf area_tris, area_info;
+  shb::DevBuf area_tris;
   uint32_t vertex_count = 0, prim_count = 0, geom_count = 0, mat_count = 0, light_count = 0;
   uint32_t area_light_count = 0;
   int32_t has_alpha = 0;
