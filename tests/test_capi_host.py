@@ -121,3 +121,15 @@ def test_room_scene_counts():
 def test_unit_quad_scene():
     sc = scenes.unit_quad()
     assert sc.triangle_count == 2 and len(sc.lights) == 2
+
+
+def test_srgb_table_matches_oracle():
+    """shb_srgb_to_linear_table (GetAlbedo's SRGBToLinear, src/colorspace.h:10-14)
+    against the oracle's restatement, all 256 values bit for bit; host only."""
+    import numpy as np
+
+    from oracle import pyoracle as O
+    from sh_baker_b200 import api
+    got = api.srgb_to_linear_table()
+    want = np.array([O.srgb_to_linear(i) for i in range(256)], np.float32)
+    assert got.tobytes() == want.tobytes()
