@@ -3,13 +3,17 @@
 // shadow rays (src/light.cpp:173,275).
 //
 // Persistent kernels with per-lane ray replacement: the grid fills every SM
-// once; a lane whose ray finishes takes the next queue entry (one atomic per
-// warp for all lanes that refill), so lanes do not wait for the slowest ray
-// of a batch.  Within a ray, children are visited in the ray-octant order of
-// their slots.  Triangle groups can be postponed on the stack while too few
-// lanes of the warp want to test triangles (Ylitie, Karras, Laine 2017);
-// measured here that only slows both kernels down (the any-hit kernel most,
-// it ends on the first triangle it hits), so SHB_POSTPONE defaults to off.
+// once; lanes whose rays finished take the next queue entries together (one
+// atomic per warp) once enough of them wait, so lanes do not wait for the
+// slowest ray of a batch.  Within a ray, children are visited in the
+// ray-octant order of their slots.
+//
+// Each traversal step is a node visit per lane followed by a triangle phase
+// for the whole warp: the triangles that the visited nodes' hit leaves hold
+// (a few lanes have several, most have none) are spread over all 32 lanes,
+// one test per lane, instead of each lane looping over its own.  Each ray's
+// lane then replays its accepted tests in triangle order against its
+// shrinking tmax, which gives exactly the hit a sequential loop gives.
 // The watertight triangle test (Woop, Benthin, Wald 2013) uses explicit
 // round-to-nearest intrinsics so it rounds exactly like the CPU restatement
 // even though this file is compiled with FMA contraction for the box tests.
@@ -31,10 +35,19 @@ constexpr int kTravThreads = 128;
 #else
 #define SHB_TRAV_BOUNDS __launch_bounds__(kTravThreads)
 #endif
-#ifndef SHB_POSTPONE
-#define SHB_POSTPONE 0
+// A warp refills its idle lanes from the queue once at least this many
+// lanes wait for a ray (or none of its lanes has one left): the refill
+// (queue atomic, ray load and setup) then runs once for several lanes.
+#ifndef SHB_REFILL_MIN
+#define SHB_REFILL_MIN 8
 #endif
-constexpr int kPostpone = SHB_POSTPONE;  // fewer lanes than this on triangles: postpone them
+constexpr int kRefillMin = SHB_REFILL_MIN;
+// 1: the warp-cooperative triangle phase; 0: each lane tests its own
+// triangles in a loop.
+#ifndef SHB_TRI_COOP
+#define SHB_TRI_COOP 1
+#endif
+constexpr bool kTriCoop = SHB_TRI_COOP != 0;
 constexpr uint32_t kNodeGroup = 0x80000000u;
 constexpr uint32_t kMaxIters = 1u << 22;  // default bound of one ray's traversal steps
 
@@ -77,19 +90,24 @@ __device__ __forceinline__ void prepare(TravRay& r) {
 }
 
 // Watertight ray/triangle test; accepts tnear < t < tfar (t in units of
-// |d|); u, v are the weights of v1, v2.
-__device__ __forceinline__ bool tri_test(const TravRay& r, float4 a, float4 b, float4 c, float tnear, float tfar,
-                                         float& t, float& u, float& v) {
-  float Ax_ = __fsub_rn(a.x, r.ox), Ay_ = __fsub_rn(a.y, r.oy), Az_ = __fsub_rn(a.z, r.oz);
-  float Bx_ = __fsub_rn(b.x, r.ox), By_ = __fsub_rn(b.y, r.oy), Bz_ = __fsub_rn(b.z, r.oz);
-  float Cx_ = __fsub_rn(c.x, r.ox), Cy_ = __fsub_rn(c.y, r.oy), Cz_ = __fsub_rn(c.z, r.oz);
-  float Akz = comp(Ax_, Ay_, Az_, r.kz), Bkz = comp(Bx_, By_, Bz_, r.kz), Ckz = comp(Cx_, Cy_, Cz_, r.kz);
-  float Ax = __fsub_rn(comp(Ax_, Ay_, Az_, r.kx), __fmul_rn(r.Sx, Akz));
-  float Ay = __fsub_rn(comp(Ax_, Ay_, Az_, r.ky), __fmul_rn(r.Sy, Akz));
-  float Bx = __fsub_rn(comp(Bx_, By_, Bz_, r.kx), __fmul_rn(r.Sx, Bkz));
-  float By = __fsub_rn(comp(Bx_, By_, Bz_, r.ky), __fmul_rn(r.Sy, Bkz));
-  float Cx = __fsub_rn(comp(Cx_, Cy_, Cz_, r.kx), __fmul_rn(r.Sx, Ckz));
-  float Cy = __fsub_rn(comp(Cx_, Cy_, Cz_, r.ky), __fmul_rn(r.Sy, Ckz));
+// |d|).  On acceptance gives T, det, V, W with det > 0: t = T / det, and
+// V / det, W / det are the weights of v1, v2 (the divisions are left to the
+// caller: only the last accepted triangle of a ray needs its weights).
+// `k` holds the ray's axes kx | ky << 2 | kz << 4.
+__device__ __forceinline__ bool tri_core(float ox, float oy, float oz, uint32_t k, float Sx, float Sy, float Sz,
+                                         float4 a, float4 b, float4 c, float tnear, float tfar, float& T_,
+                                         float& det_, float& V_, float& W_) {
+  const int kx = (int)(k & 3u), ky = (int)((k >> 2) & 3u), kz = (int)(k >> 4);
+  float Ax_ = __fsub_rn(a.x, ox), Ay_ = __fsub_rn(a.y, oy), Az_ = __fsub_rn(a.z, oz);
+  float Bx_ = __fsub_rn(b.x, ox), By_ = __fsub_rn(b.y, oy), Bz_ = __fsub_rn(b.z, oz);
+  float Cx_ = __fsub_rn(c.x, ox), Cy_ = __fsub_rn(c.y, oy), Cz_ = __fsub_rn(c.z, oz);
+  float Akz = comp(Ax_, Ay_, Az_, kz), Bkz = comp(Bx_, By_, Bz_, kz), Ckz = comp(Cx_, Cy_, Cz_, kz);
+  float Ax = __fsub_rn(comp(Ax_, Ay_, Az_, kx), __fmul_rn(Sx, Akz));
+  float Ay = __fsub_rn(comp(Ax_, Ay_, Az_, ky), __fmul_rn(Sy, Akz));
+  float Bx = __fsub_rn(comp(Bx_, By_, Bz_, kx), __fmul_rn(Sx, Bkz));
+  float By = __fsub_rn(comp(Bx_, By_, Bz_, ky), __fmul_rn(Sy, Bkz));
+  float Cx = __fsub_rn(comp(Cx_, Cy_, Cz_, kx), __fmul_rn(Sx, Ckz));
+  float Cy = __fsub_rn(comp(Cx_, Cy_, Cz_, ky), __fmul_rn(Sy, Ckz));
   float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
   float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
   float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
@@ -101,7 +119,7 @@ __device__ __forceinline__ bool tri_test(const TravRay& r, float4 a, float4 b, f
   if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
   float det = __fadd_rn(__fadd_rn(U, V), W);
   if (det == 0.f) return false;
-  float Az = __fmul_rn(r.Sz, Akz), Bz = __fmul_rn(r.Sz, Bkz), Cz = __fmul_rn(r.Sz, Ckz);
+  float Az = __fmul_rn(Sz, Akz), Bz = __fmul_rn(Sz, Bkz), Cz = __fmul_rn(Sz, Ckz);
   float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
   if (det < 0.f) {
     T = -T;
@@ -110,10 +128,15 @@ __device__ __forceinline__ bool tri_test(const TravRay& r, float4 a, float4 b, f
     W = -W;
   }
   if (!(T > __fmul_rn(tnear, det) && T < __fmul_rn(tfar, det))) return false;
-  t = __fdiv_rn(T, det);
-  u = __fdiv_rn(V, det);
-  v = __fdiv_rn(W, det);
+  T_ = T;
+  det_ = det;
+  V_ = V;
+  W_ = W;
   return true;
+}
+
+__device__ __forceinline__ uint32_t axes(const TravRay& r) {
+  return (uint32_t)r.kx | ((uint32_t)r.ky << 2) | ((uint32_t)r.kz << 4);
 }
 
 // Byte k of w as a float (exact): one byte permute builds the bit pattern
@@ -134,7 +157,7 @@ struct Walk {
   int sp;
   uint32_t iters;
   bool hit;
-  float u, v;
+  float hV, hW, hdet;  // barycentric numerators and determinant of the hit
   uint32_t prim;
 };
 
@@ -146,7 +169,8 @@ __device__ __forceinline__ void walk_init(Walk& w, const BvhView& bvh, float tne
   w.sp = 0;
   w.iters = 0;
   w.hit = false;
-  w.u = w.v = 0.f;
+  w.hV = w.hW = 0.f;
+  w.hdet = 1.f;
   w.prim = kMissPrim;
 }
 
@@ -224,15 +248,15 @@ __device__ __forceinline__ void intersect_node(const BvhView& bvh, const Walk& w
   Tn = make_uint2(n1.y, hm & 0x00FFFFFFu);
 }
 
-// One step: visit one node (or take a popped triangle group) and test the
-// current triangle group.  Returns true when the ray is finished.
-template <bool ANY>
-__device__ __forceinline__ bool walk_step(const BvhView& bvh, Walk& w, uint2* stack, int* err, uint32_t max_iters) {
+// The node part of one step: visit one node (or take a popped triangle
+// group) and leave the triangles to test in w.T.  Returns true when the ray
+// ran out of steps (w.T is then empty).
+__device__ __forceinline__ bool walk_node(const BvhView& bvh, Walk& w, uint2* stack, int* err, uint32_t max_iters) {
   if (++w.iters > max_iters) {
     atomicOr(err, ERR_ITER);
+    w.T.y = 0;
     return true;
   }
-  bool descended = false;
   if ((w.G.y & kNodeGroup) && (w.G.y & 0xFFu)) {
     uint32_t hits = w.G.y & 0xFFu;
     uint32_t imask = (w.G.y >> 8) & 0xFFu;
@@ -244,45 +268,162 @@ __device__ __forceinline__ bool walk_step(const BvhView& bvh, Walk& w, uint2* st
       if (w.sp < kStack) stack[w.sp++] = make_uint2(w.G.x, kNodeGroup | (imask << 8) | hits);
       else atomicOr(err, ERR_STACK);
     }
-    uint2 Tn;
-    intersect_node(bvh, w, node, w.G, Tn);
-    w.T = Tn;
-    descended = true;
+    intersect_node(bvh, w, node, w.G, w.T);
   } else if (!(w.G.y & kNodeGroup)) {
     w.T = w.G;  // a popped triangle group
     w.G = make_uint2(0u, 0u);
   } else {
     w.G = make_uint2(0u, 0u);
   }
-  while (w.T.y) {
-    // postpone when few lanes test triangles and this ray still has nodes to visit
-    if (descended && (w.G.y & 0xFFu) && __popc(__activemask()) < kPostpone) {
-      if (w.sp < kStack) {
-        stack[w.sp++] = w.T;
-        w.T.y = 0;
-        break;
-      }
-    }
-    int k = __ffs(w.T.y) - 1;
-    w.T.y &= w.T.y - 1;
-    const float4* tp = bvh.tris + 3 * (size_t)(w.T.x + k);
-    float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
-    float t, u, v;
-    if (tri_test(w.r, a, b, c, w.tnear, w.tmax, t, u, v)) {
-      w.hit = true;
-      w.tmax = t;
-      w.u = u;
-      w.v = v;
-      w.prim = __float_as_uint(a.w);
-      if (ANY) return true;
-    }
-  }
+  return false;
+}
+
+// The end of a step: take the next group from the stack when the current
+// one is used up.  Returns true when the ray is finished.
+__device__ __forceinline__ bool walk_pop(Walk& w, const uint2* stack) {
   bool g_empty = !((w.G.y & kNodeGroup) ? (w.G.y & 0xFFu) : w.G.y);
   if (g_empty) {
     if (w.sp == 0) return true;
     w.G = stack[--w.sp];
   }
   return false;
+}
+
+// Accepts a test that passed against the tmax of its step if it still
+// passes against the ray's current tmax (the sequential loop's test with
+// the tmax of the triangles before it).
+__device__ __forceinline__ void accept(Walk& w, float T, float det, float V, float W, float prim_bits) {
+  if (T < __fmul_rn(w.tmax, det)) {
+    w.hit = true;
+    w.tmax = __fdiv_rn(T, det);
+    w.hV = V;
+    w.hW = W;
+    w.hdet = det;
+    w.prim = __float_as_uint(prim_bits);
+  }
+}
+
+// The triangle part of one step, one lane: its own triangles in bit order.
+template <bool ANY>
+__device__ __forceinline__ void tri_seq(Walk& w, const float4* tris) {
+  const uint32_t k = axes(w.r);
+  while (w.T.y) {
+    int b = __ffs(w.T.y) - 1;
+    w.T.y &= w.T.y - 1;
+    const float4* tp = tris + 3 * (size_t)(w.T.x + b);
+    float4 a = __ldg(tp), bb = __ldg(tp + 1), c = __ldg(tp + 2);
+    float T, det, V, W;
+    if (tri_core(w.r.ox, w.r.oy, w.r.oz, k, w.r.Sx, w.r.Sy, w.r.Sz, a, bb, c, w.tnear, w.tmax, T, det, V, W)) {
+      accept(w, T, det, V, W, a.w);
+      if (ANY) {
+        w.T.y = 0;
+        return;
+      }
+    }
+  }
+}
+
+// Position of the n-th (from 0) set bit of x; x has more than n set bits.
+__device__ __forceinline__ uint32_t nth_bit(uint32_t x, uint32_t n) {
+  uint32_t pos = 0, c;
+  c = __popc(x & 0xFFFFu);
+  if (n >= c) { n -= c; x >>= 16; pos += 16; }
+  c = __popc(x & 0xFFu);
+  if (n >= c) { n -= c; x >>= 8; pos += 8; }
+  c = __popc(x & 0xFu);
+  if (n >= c) { n -= c; x >>= 4; pos += 4; }
+  c = __popc(x & 0x3u);
+  if (n >= c) { n -= c; x >>= 2; pos += 2; }
+  if (n >= (x & 1u)) pos += 1;
+  return pos;
+}
+
+// Per-warp shared tables of the cooperative triangle phase: each lane's ray
+// (written when the lane takes the ray), the lane owning each slot window
+// start, and the accepted tests of a window.
+struct CoopWarp {
+  float4 r0[32];   // ox, oy, oz, tnear
+  float4 r1[32];   // Sx, Sy, Sz, axes
+  float4 hit[32];  // T, det, V, W
+  float hprim[32];
+  int own[32];
+};
+
+__device__ __forceinline__ void coop_store_ray(CoopWarp& s, int lane, const Walk& w) {
+  s.r0[lane] = make_float4(w.r.ox, w.r.oy, w.r.oz, w.tnear);
+  s.r1[lane] = make_float4(w.r.Sx, w.r.Sy, w.r.Sz, __uint_as_float(axes(w.r)));
+}
+
+// The triangle part of one step for the whole warp (every lane calls it;
+// lanes without a ray have an empty w.T).  The warp's pending tests,
+// ordered by lane and then by triangle bit, are dealt out 32 at a time, one
+// per lane; each owner lane then replays its accepted tests in bit order
+// (accept), so the result is the sequential loop's.  For ANY, an accepted
+// test ends the ray (w.hit).
+template <bool ANY>
+__device__ __forceinline__ void tri_coop(CoopWarp& s, Walk& w, const float4* tris, int lane) {
+  const uint32_t full = 0xFFFFFFFFu;
+  const uint32_t cnt = __popc(w.T.y);
+  uint32_t incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t x = __shfl_up_sync(full, incl, o);
+    if (lane >= o) incl += x;
+  }
+  const uint32_t total = __shfl_sync(full, incl, 31);
+  if (total == 0) return;
+  const uint32_t excl = incl - cnt;
+  const unsigned long long tb = (unsigned long long)(tris + 3 * (size_t)w.T.x);
+  for (uint32_t base = 0; base < total; base += 32) {
+    // the lane whose tests cover the window's first slot, and the lanes
+    // whose tests start inside the window
+    const bool c0 = cnt && excl <= base && base < excl + cnt;
+    const bool st = cnt && excl > base && excl < base + 32;
+    if (c0) s.own[0] = lane;
+    if (st) s.own[excl - base] = lane;
+    const uint32_t starts = __reduce_or_sync(full, c0 ? 1u : (st ? 1u << (excl - base) : 0u));
+    __syncwarp();
+    const uint32_t g = base + (uint32_t)lane;
+    const bool act = g < total;
+    const int owner = act ? s.own[31 - __clz(starts & (full >> (31 - lane)))] : lane;
+    const uint32_t oty = __shfl_sync(full, w.T.y, owner);
+    const uint32_t oex = __shfl_sync(full, excl, owner);
+    const float otmax = __shfl_sync(full, w.tmax, owner);
+    const unsigned long long otb = __shfl_sync(full, tb, owner);
+    bool hit = false;
+    if (act) {
+      const float4* tp = reinterpret_cast<const float4*>(otb) + 3 * nth_bit(oty, g - oex);
+      const float4 a = __ldg(tp), b = __ldg(tp + 1), c = __ldg(tp + 2);
+      const float4 r0 = s.r0[owner], r1 = s.r1[owner];
+      float T, det, V, W;
+      hit = tri_core(r0.x, r0.y, r0.z, __float_as_uint(r1.w), r1.x, r1.y, r1.z, a, b, c, r0.w, otmax, T, det, V, W);
+      if (hit && !ANY) {
+        s.hit[lane] = make_float4(T, det, V, W);
+        s.hprim[lane] = a.w;
+      }
+    }
+    const uint32_t hm = __ballot_sync(full, hit);
+    if (hm) {
+      __syncwarp();
+      const int lo = (int)excl - (int)base, hi = (int)(excl + cnt) - (int)base;
+      if (cnt && hi > 0 && lo < 32) {
+        const int l0 = lo < 0 ? 0 : lo, l1 = hi > 32 ? 32 : hi;
+        uint32_t m = hm & bit_mask((uint32_t)l0, (uint32_t)(l1 - l0));
+        if (ANY) {
+          if (m) w.hit = true;
+        } else {
+          while (m) {
+            const int sl = __ffs(m) - 1;
+            m &= m - 1;
+            const float4 h = s.hit[sl];
+            accept(w, h.x, h.y, h.z, h.w, s.hprim[sl]);
+          }
+        }
+      }
+    }
+    __syncwarp();  // the tables are rewritten by the next window
+  }
+  w.T.y = 0;
 }
 
 __device__ __forceinline__ void load_ray(TravRay& r, float4 o, float4 d) {
@@ -295,21 +436,29 @@ __device__ __forceinline__ void load_ray(TravRay& r, float4 o, float4 d) {
   prepare(r);
 }
 
+__device__ __forceinline__ float4 hit_record(const Walk& w) {
+  return w.hit ? make_float4(w.tmax, __fdiv_rn(w.hV, w.hdet), __fdiv_rn(w.hW, w.hdet), __uint_as_float(w.prim))
+               : make_float4(0.f, 0.f, 0.f, __uint_as_float(kMissPrim));
+}
+
 // Persistent queue consumer: lanes refill from the queue as their rays end.
 // `bvh_of(i, o, d)` gives the BVH of queue entry i (its bake's).
 template <bool SHADOW, class Q, class B, class Fin>
-__device__ __forceinline__ void consume(const Q& q, int n, int* fetch, int* err, uint32_t max_iters, B&& bvh_of,
-                                       Fin&& finish) {
+__device__ __forceinline__ void consume(CoopWarp& s, const Q& q, int n, int* fetch, int* err, uint32_t max_iters,
+                                        B&& bvh_of, Fin&& finish) {
   const int lane = threadIdx.x & 31;
   const unsigned lt = (1u << lane) - 1u;
   uint2 stack[kStack];
   Walk w;
+  w.T = make_uint2(0u, 0u);
   BvhView bvh;
+  bvh.tris = nullptr;
   int ray = -1;
   bool exhausted = false;
   while (true) {
     bool need = ray < 0 && !exhausted;
     unsigned needm = __ballot_sync(0xFFFFFFFFu, need);
+    if (kRefillMin > 1 && __popc(needm) < kRefillMin && __any_sync(0xFFFFFFFFu, ray >= 0)) needm = 0;
     if (needm) {
       int leader = __ffs(needm) - 1;
       int base = 0;
@@ -323,50 +472,56 @@ __device__ __forceinline__ void consume(const Q& q, int n, int* fetch, int* err,
           bvh = bvh_of(r, o, d);
           load_ray(w.r, o, d);
           walk_init(w, bvh, 0.001f, SHADOW ? o.w : INFINITY);
+          if (kTriCoop) coop_store_ray(s, lane, w);
         } else {
           exhausted = true;
         }
       }
     }
     if (!__any_sync(0xFFFFFFFFu, ray >= 0)) break;
+    bool done = false;
+    if (ray >= 0) done = walk_node(bvh, w, stack, err, max_iters);
+    if (kTriCoop) tri_coop<SHADOW>(s, w, bvh.tris, lane);
+    else if (ray >= 0) tri_seq<SHADOW>(w, bvh.tris);
     if (ray >= 0) {
-      if (walk_step<SHADOW>(bvh, w, stack, err, max_iters)) {
+      if (!done) done = (SHADOW && w.hit) || walk_pop(w, stack);
+      if (done) {
         finish(ray, w);
         ray = -1;
+        w.T = make_uint2(0u, 0u);
       }
     }
   }
 }
 
 __global__ void SHB_TRAV_BOUNDS k_extend(const BakeItem* __restrict__ bakes, int n_bakes,
-                                                        const PathInfo* __restrict__ info, ExtQueue q,
-                                                        const int* __restrict__ n_ptr, int cap,
-                                                        float4* __restrict__ hits, int* fetch, int* err,
-                                                        Counters64* stats, uint32_t max_iters) {
+                                         const PathInfo* __restrict__ info, ExtQueue q,
+                                         const int* __restrict__ n_ptr, int cap, float4* __restrict__ hits,
+                                         int* fetch, int* err, Counters64* stats, uint32_t max_iters) {
+  __shared__ CoopWarp coop[kTriCoop ? kTravThreads / 32 : 1];
   const int n = min(*n_ptr, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&stats->extend_rays, (unsigned long long)n);
   const BvhView bvh0 = bakes[0].bvh;
   auto bvh_of = [&](int, float4 o, float4) {
     return n_bakes == 1 ? bvh0 : bakes[info[__float_as_uint(o.w)].x].bvh;
   };
-  consume<false>(q, n, fetch, err, max_iters, bvh_of, [&](int i, const Walk& w) {
-    hits[i] = w.hit ? make_float4(w.tmax, w.u, w.v, __uint_as_float(w.prim))
-                    : make_float4(0.f, 0.f, 0.f, __uint_as_float(kMissPrim));
-  });
+  consume<false>(coop[kTriCoop ? threadIdx.x / 32 : 0], q, n, fetch, err, max_iters, bvh_of,
+                 [&](int i, const Walk& w) { hits[i] = hit_record(w); });
 }
 
 __global__ void SHB_TRAV_BOUNDS k_shadow(const BakeItem* __restrict__ bakes, int n_bakes, ShadowQueue q,
-                                                        const int* __restrict__ n_ptr, int cap,
-                                                        float4* __restrict__ path_L, float4* __restrict__ nee_li,
-                                                        float4* __restrict__ pend, int* fetch, int* err,
-                                                        Counters64* stats, uint32_t max_iters) {
+                                         const int* __restrict__ n_ptr, int cap, float4* __restrict__ path_L,
+                                         float4* __restrict__ nee_li, float4* __restrict__ pend, int* fetch,
+                                         int* err, Counters64* stats, uint32_t max_iters) {
+  __shared__ CoopWarp coop[kTriCoop ? kTravThreads / 32 : 1];
   const int n = min(*n_ptr, cap);
   if (blockIdx.x == 0 && threadIdx.x == 0 && n > 0) atomicAdd(&stats->shadow_rays, (unsigned long long)n);
   const BvhView bvh0 = bakes[0].bvh;
   auto bvh_of = [&](int i, float4, float4) {
     return n_bakes == 1 ? bvh0 : bakes[__float_as_uint(q.c[i].w) >> 2].bvh;
   };
-  consume<true>(q, n, fetch, err, max_iters, bvh_of, [&](int i, const Walk& w) {
+  consume<true>(coop[kTriCoop ? threadIdx.x / 32 : 0], q, n, fetch, err, max_iters, bvh_of,
+                [&](int i, const Walk& w) {
     float4 c = q.c[i];
     uint32_t target = __float_as_uint(q.d[i].w);
     const uint32_t kind = __float_as_uint(c.w) & 3u;
@@ -383,6 +538,7 @@ __global__ void SHB_TRAV_BOUNDS k_shadow(const BakeItem* __restrict__ bakes, int
   });
 }
 
+// One thread per ray, the per-lane triangle loop (FindOcclusion queries).
 __global__ void k_closest_rays(BvhView bvh, const shb_ray* __restrict__ rays, int64_t n, float4* __restrict__ hits,
                                int* err) {
   uint2 stack[kStack];
@@ -397,10 +553,12 @@ __global__ void k_closest_rays(BvhView bvh, const shb_ray* __restrict__ rays, in
     w.r.dz = sr.direction[2];
     prepare(w.r);
     walk_init(w, bvh, sr.tnear, sr.tfar);
-    while (!walk_step<false>(bvh, w, stack, err, kMaxIters)) {
+    while (true) {
+      if (walk_node(bvh, w, stack, err, kMaxIters)) break;
+      tri_seq<false>(w, bvh.tris);
+      if (walk_pop(w, stack)) break;
     }
-    hits[i] = w.hit ? make_float4(w.tmax, w.u, w.v, __uint_as_float(w.prim))
-                    : make_float4(0.f, 0.f, 0.f, __uint_as_float(kMissPrim));
+    hits[i] = hit_record(w);
   }
 }
 
