@@ -1492,7 +1492,8 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
   a.grad = prm.grad;
   const size_t gsmem = bwd ? sizeof(float) * (size_t)n_params : 0;
 
-  const int tgrid = traversal_grid(c->device) * std::max(1, prm.grid_scale);
+  const int tgrid = traversal_grid(c->device, false) * std::max(1, prm.grid_scale);
+  const int tgrid_sh = traversal_grid(c->device, true) * std::max(1, prm.grid_scale);
   const int sgrid = sm_count() * 8;
   const bool timed = c->profiling && !prm.use_graph;
   struct Pair {
@@ -1563,7 +1564,7 @@ shb_status bake_batch_device(shb_context* c, const std::vector<BakeSpec>& specs,
       }
       close_stamp(pd);
       Pair ps = stamp(1);
-      launch_shadow(st, tgrid, bk, nbk, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, a.pend,
+      launch_shadow(st, tgrid_sh, bk, nbk, a.sh, cnt + CNT_SHADOW, a.sh_cap, a.path_L, a.nee_li, a.pend,
                     cnt + CNT_FETCH_SHADOW, cnt + CNT_ERROR, c64, prm.max_iters);
       close_stamp(ps);
       if (bwd) {

@@ -86,6 +86,6 @@ void launch_shadow(cudaStream_t st, int grid, const BakeItem* bakes, int n_bakes
                    uint32_t max_iters);
 void launch_closest_rays(cudaStream_t st, const BvhView& bvh, const shb_ray* rays, int64_t n, float4* hits,
                          int* err);
-int traversal_grid(int device);
+int traversal_grid(int device, bool shadow);
 
 }  // namespace shb
