@@ -285,6 +285,12 @@ __device__ LightEval eval_light(const SceneView& sc, const DLight* lights, uint3
 // `lights` is the bake's light table in global memory or the block's copy
 // of it in shared memory.
 constexpr uint32_t kWeightCache = 32;
+// 1: the picked light is evaluated after the weight scan (one convergent
+// evaluation per warp); 0: inside the scan, where the lane's pick is found.
+#ifndef SHB_PICK_AFTER_LOOP
+#define SHB_PICK_AFTER_LOOP 1
+#endif
+constexpr bool kPickAfterLoop = SHB_PICK_AFTER_LOOP != 0;
 // Texel next-event estimation shares the punctual lights' weights across a
 // warp of one texel's samples also in scenes with area lights.
 #ifndef SHB_TEXEL_COOP_AREA
@@ -299,6 +305,25 @@ __device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N
   float cum = 0.f;
   int last = -1;
   const bool cached = sc.light_count <= kWeightCache;
+  if (cached && kPickAfterLoop) {
+    // Find the index first and evaluate the picked light once, after the
+    // loop: evaluated inside it, the warp would run the evaluation once for
+    // every distinct pick among its lanes, each time with those lanes only.
+    int pick = -1;
+    for (uint32_t i = 0; i < sc.light_count; ++i) {
+      const float w = wcache[i * ws];
+      cum += w;
+      if (w > 0.f) last = (int)i;
+      if (target < cum) {
+        pick = (int)i;
+        break;
+      }
+    }
+    if (pick < 0) pick = last;
+    if (pick < 0) return false;
+    out = eval_light<HIT, BWD>(sc, lights, (uint32_t)pick, P, N, ev, wo_back, aop);
+    return true;
+  }
   for (uint32_t i = 0; i < sc.light_count; ++i) {
     float w;
     LightEval e;
