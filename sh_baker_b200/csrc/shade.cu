@@ -27,15 +27,29 @@ __constant__ float g_srgb[256];
 namespace {
 
 constexpr int kThreads = 256;
-// Launch bounds of the shading kernels: SHB_SHADE_BLOCKS_PER_SM > 0 asks
-// the compiler to fit that many resident blocks per SM (fewer registers).
+// Launch bounds of k_shade when next-event estimation runs in k_nee:
+// SHB_SHADE_BLOCKS_PER_SM > 0 asks the compiler to fit that many resident
+// blocks per SM (fewer registers), 4 by default (64 registers).  With
+// k_generate also held to 64 registers the atrium's shading measured 1.2 %
+// faster but the room's (5 lights) 1.9 % slower, so k_generate follows
+// SHB_GEN_BLOCKS_PER_SM (0: the compiler's choice).  The adjoint instances
+// and the k_shade with next-event estimation inline keep the compiler's
+// choice.
 #ifndef SHB_SHADE_BLOCKS_PER_SM
-#define SHB_SHADE_BLOCKS_PER_SM 0
+#define SHB_SHADE_BLOCKS_PER_SM 4
+#endif
+#ifndef SHB_GEN_BLOCKS_PER_SM
+#define SHB_GEN_BLOCKS_PER_SM 0
 #endif
 #if SHB_SHADE_BLOCKS_PER_SM > 0
-#define SHB_SHADE_BOUNDS __launch_bounds__(kThreads, SHB_SHADE_BLOCKS_PER_SM)
+#define SHB_SHADE_BOUNDS __launch_bounds__(kThreads, (BWD || !SPLIT) ? 1 : SHB_SHADE_BLOCKS_PER_SM)
 #else
 #define SHB_SHADE_BOUNDS __launch_bounds__(kThreads)
+#endif
+#if SHB_GEN_BLOCKS_PER_SM > 0
+#define SHB_GEN_BOUNDS __launch_bounds__(kThreads, BWD ? 1 : SHB_GEN_BLOCKS_PER_SM)
+#else
+#define SHB_GEN_BOUNDS __launch_bounds__(kThreads)
 #endif
 // Alpha branches per path kept apart for deterministic accumulation: the
 // wave is shrunk by 2^min(bounces, kMaxBranchLog).  Branch slots beyond that
@@ -559,7 +573,7 @@ __device__ __forceinline__ int find_tile(const WaveArgs& a, int64_t x) {
 
 // ------------------------------------------------------------- generate --
 template <bool BWD>
-__global__ void SHB_SHADE_BOUNDS k_generate(WaveArgs a) {
+__global__ void SHB_GEN_BOUNDS k_generate(WaveArgs a) {
   extern __shared__ float dyn_smem[];
   const DLight* wave_lights = BWD ? nullptr : stage_lights(a.bakes, a.one_bake, reinterpret_cast<DLight*>(dyn_smem));
   const int64_t warps = (int64_t)gridDim.x * (blockDim.x >> 5);
