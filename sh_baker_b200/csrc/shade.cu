@@ -32,22 +32,28 @@ constexpr int kThreads = 256;
 // blocks per SM (fewer registers), 4 by default (64 registers).  With
 // k_generate also held to 64 registers the atrium's shading measured 1.2 %
 // faster but the room's (5 lights) 1.9 % slower, so k_generate follows
-// SHB_GEN_BLOCKS_PER_SM (0: the compiler's choice).  The adjoint instances
-// and the k_shade with next-event estimation inline keep the compiler's
-// choice.
+// SHB_GEN_BLOCKS_PER_SM (0: the compiler's choice).  The adjoint k_shade
+// (SHB_BWD_BLOCKS_PER_SM) and the k_shade with next-event estimation inline
+// are bounded to 2 blocks (at most 128 registers), the compiler's own
+// choice for them: with a bound of 1 block the adjoint k_shade took 160
+// registers and its backward pass ran 14 % slower.
 #ifndef SHB_SHADE_BLOCKS_PER_SM
 #define SHB_SHADE_BLOCKS_PER_SM 4
+#endif
+#ifndef SHB_BWD_BLOCKS_PER_SM
+#define SHB_BWD_BLOCKS_PER_SM 2
 #endif
 #ifndef SHB_GEN_BLOCKS_PER_SM
 #define SHB_GEN_BLOCKS_PER_SM 0
 #endif
 #if SHB_SHADE_BLOCKS_PER_SM > 0
-#define SHB_SHADE_BOUNDS __launch_bounds__(kThreads, (BWD || !SPLIT) ? 1 : SHB_SHADE_BLOCKS_PER_SM)
+#define SHB_SHADE_BOUNDS \
+  __launch_bounds__(kThreads, BWD ? SHB_BWD_BLOCKS_PER_SM : (!SPLIT ? 2 : SHB_SHADE_BLOCKS_PER_SM))
 #else
 #define SHB_SHADE_BOUNDS __launch_bounds__(kThreads)
 #endif
 #if SHB_GEN_BLOCKS_PER_SM > 0
-#define SHB_GEN_BOUNDS __launch_bounds__(kThreads, BWD ? 1 : SHB_GEN_BLOCKS_PER_SM)
+#define SHB_GEN_BOUNDS __launch_bounds__(kThreads, BWD ? SHB_BWD_BLOCKS_PER_SM : SHB_GEN_BLOCKS_PER_SM)
 #else
 #define SHB_GEN_BOUNDS __launch_bounds__(kThreads)
 #endif
@@ -305,6 +311,11 @@ constexpr uint32_t kWeightCache = 32;
 #define SHB_PICK_AFTER_LOOP 1
 #endif
 constexpr bool kPickAfterLoop = SHB_PICK_AFTER_LOOP != 0;
+// The same for the adjoint's picks (whose light evaluation carries the
+// parameter derivatives).
+#ifndef SHB_PICK_AFTER_LOOP_BWD
+#define SHB_PICK_AFTER_LOOP_BWD 1
+#endif
 // Texel next-event estimation shares the punctual lights' weights across a
 // warp of one texel's samples also in scenes with area lights.
 #ifndef SHB_TEXEL_COOP_AREA
@@ -319,7 +330,7 @@ __device__ bool pick_light(const SceneView& sc, const DLight* lights, f3 P, f3 N
   float cum = 0.f;
   int last = -1;
   const bool cached = sc.light_count <= kWeightCache;
-  if (cached && kPickAfterLoop) {
+  if (cached && kPickAfterLoop && (!BWD || SHB_PICK_AFTER_LOOP_BWD)) {
     // Find the index first and evaluate the picked light once, after the
     // loop: evaluated inside it, the warp would run the evaluation once for
     // every distinct pick among its lanes, each time with those lanes only.
