@@ -28,11 +28,12 @@ SOURCES = {
     "batch.cu": ["-fmad=false"],
     "exr.cu": ["-fmad=false"],
     "gltf.cpp": [],
+    "tspace.cpp": [],
     "jpeg.cpp": [],
     "atlas.cpp": [],
     "preview.cu": ["-fmad=false"],
 }
-HEADERS = ["shb_internal.h", "shb_math.cuh", "wavefront.h"]
+HEADERS = ["shb_internal.h", "shb_math.cuh", "wavefront.h", "tspace.h"]
 
 
 def nvcc() -> str:

@@ -19,14 +19,15 @@
 //     without materials a white default is used (:438-465);
 //   - a light takes the node's translation and its rotation applied to -Z
 //     (:541-560), cone angles become cosines (:587-598).
-// Differences: tangents missing from the file are built from per-vertex UV
-// derivatives (MikkTSpace, a third-party library, is not vendored); the
-// bake's hemisphere sampling is invariant to the tangent's rotation about the
-// normal, so only the random stream's orientation differs.  JPEG textures
+// Tangents missing from the file are built by the MikkTSpace method
+// (tspace.cpp), as the reference builds them with that library.
+// Differences: JPEG textures
 // are decoded by jpeg.cpp (sequential files only; progressive ones are
 // rejected).  The sky environment (:705-797) is not read: the bake never
 // samples it.
 #include <zlib.h>
+
+#include "tspace.h"
 
 #include <algorithm>
 #include <cmath>
@@ -591,56 +592,11 @@ float surface_area(const shb_host_scene::Geo& g) {
   return total;
 }
 
-// Tangents from UV derivatives accumulated per vertex, orthogonalised
-// against the normal; handedness from the UV bitangent.  Vertices whose UV
-// frame is degenerate get the geometric fallback of the reference
-// (src/loader.cpp:368-381).
+// Tangents of a primitive that has no TANGENT attribute
+// (src/loader.cpp:363-385): the MikkTSpace method of tspace.cpp.
 void build_tangents(shb_host_scene::Geo& g, size_t nv) {
-  std::vector<double> T(3 * nv, 0.0), B(3 * nv, 0.0);
-  for (size_t i = 0; i + 2 < g.idx.size(); i += 3) {
-    const uint32_t id[3] = {g.idx[i], g.idx[i + 1], g.idx[i + 2]};
-    const float* p0 = &g.v[3 * id[0]];
-    const float* p1 = &g.v[3 * id[1]];
-    const float* p2 = &g.v[3 * id[2]];
-    const float* u0 = &g.uv0[2 * id[0]];
-    const float* u1 = &g.uv0[2 * id[1]];
-    const float* u2 = &g.uv0[2 * id[2]];
-    const double e1[3] = {p1[0] - p0[0], p1[1] - p0[1], p1[2] - p0[2]};
-    const double e2[3] = {p2[0] - p0[0], p2[1] - p0[1], p2[2] - p0[2]};
-    const double du1 = u1[0] - u0[0], dv1 = u1[1] - u0[1], du2 = u2[0] - u0[0], dv2 = u2[1] - u0[1];
-    const double det = du1 * dv2 - du2 * dv1;
-    if (std::fabs(det) < 1e-20) continue;
-    const double r = 1.0 / det;
-    for (int k = 0; k < 3; ++k) {
-      const double t = (e1[k] * dv2 - e2[k] * dv1) * r, b = (e2[k] * du1 - e1[k] * du2) * r;
-      for (int j = 0; j < 3; ++j) {
-        T[3 * id[j] + k] += t;
-        B[3 * id[j] + k] += b;
-      }
-    }
-  }
   g.t.assign(4 * nv, 0.0f);
-  for (size_t v = 0; v < nv; ++v) {
-    const double n[3] = {g.n[3 * v], g.n[3 * v + 1], g.n[3 * v + 2]};
-    double t[3] = {T[3 * v], T[3 * v + 1], T[3 * v + 2]};
-    const double nd = n[0] * t[0] + n[1] * t[1] + n[2] * t[2];
-    for (int k = 0; k < 3; ++k) t[k] -= n[k] * nd;
-    double len = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
-    double w = 1.0;
-    if (len > 1e-12) {
-      const double c[3] = {n[1] * t[2] - n[2] * t[1], n[2] * t[0] - n[0] * t[2], n[0] * t[1] - n[1] * t[0]};
-      w = (c[0] * B[3 * v] + c[1] * B[3 * v + 1] + c[2] * B[3 * v + 2]) < 0.0 ? -1.0 : 1.0;
-    } else {
-      // reference fallback: (a - n (n.a)) normalised, a = X unless |n.x| >= 0.9
-      const double a[3] = {std::fabs(n[0]) < 0.9 ? 1.0 : 0.0, std::fabs(n[0]) < 0.9 ? 0.0 : 1.0, 0.0};
-      const double na = n[0] * a[0] + n[1] * a[1] + n[2] * a[2];
-      for (int k = 0; k < 3; ++k) t[k] = a[k] - n[k] * na;
-      len = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
-      if (len < 1e-12) len = 1.0;
-    }
-    for (int k = 0; k < 3; ++k) g.t[4 * v + k] = (float)(t[k] / len);
-    g.t[4 * v + 3] = (float)w;
-  }
+  shb::generate_tangent_frames(g.v.data(), g.n.data(), g.uv0.data(), nv, g.idx.data(), g.idx.size(), g.t.data());
 }
 
 struct Loader {
