@@ -131,6 +131,13 @@ __device__ __forceinline__ float max_coeff_std(f3 a) {
 // index, vertex and uv gathers.  The light record carries its first record
 // and its triangle count | has-texture-uv << 31.
 constexpr uint32_t kAreaHasUv = 0x80000000u;
+// 1: the record's uv float4 is read only by a sample that looks up a
+// textured emission (an emitter of constant emission never reads it);
+// 0: all four are read up front.
+#ifndef SHB_AREA_UV_LATE
+#define SHB_AREA_UV_LATE 1
+#endif
+constexpr bool kAreaUvLate = SHB_AREA_UV_LATE != 0;
 
 __device__ __forceinline__ float area_pdf(f3 v0, f3 v1, f3 v2, uint32_t n) {
   float area = sqrtf(sqnorm(cross(v0 - v1, v0 - v2))) / 2.f;
@@ -149,7 +156,9 @@ __device__ void sample_area(const SceneView& sc, const DLight& L, Event& ev, int
   if (n == 0) return;
   uint32_t tri = ev.tri(ubase, n);
   const float4* r = sc.area_tris + 4 * ((size_t)L.area_first + tri);
-  const float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2), d = __ldg(r + 3);
+  const float4 a = __ldg(r), b = __ldg(r + 1), c = __ldg(r + 2);
+  float4 d = make_float4(0.f, 0.f, 0.f, 0.f);
+  if (!kAreaUvLate) d = __ldg(r + 3);
   float u1 = ev.u(ubase + 1);
   float u2 = ev.u(ubase + 2);
   if (u1 + u2 > 1.0f) {
@@ -163,7 +172,10 @@ __device__ void sample_area(const SceneView& sc, const DLight& L, Event& ev, int
     rad = {L.er, L.eg, L.eb};
   } else {
     f2 uv = {0.f, 0.f};
-    if (L.area_count & kAreaHasUv) uv = w * f2{b.w, c.w} + u1 * f2{d.x, d.y} + u2 * f2{d.z, d.w};
+    if (L.area_count & kAreaHasUv) {
+      if (kAreaUvLate) d = __ldg(r + 3);
+      uv = w * f2{b.w, c.w} + u1 * f2{d.x, d.y} + u2 * f2{d.z, d.w};
+    }
     rad = get_emission(sc, load_mat(sc, L.mat), uv);
   }
   pdf = a.w;
