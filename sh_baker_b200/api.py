@@ -328,7 +328,8 @@ def bake_batch(ctx: Context, bakes, use_graph: bool = True, autotune: bool = Fal
                wave_paths: int = 0, tile_texels: int = 0, grid_scale: int = 0, share_paths: int = 0,
                nee_split: int = 0, outputs=None, max_traversal_steps: int = 0, queue_capacity: int = 0,
                check: bool = True):
-    """Runs many bakes in one persistent launch (shb_bake_batch).  Returns
+    """Runs many bakes through one shared sequence of wavefront launches
+    (shb_bake_batch; small bakes share waves).  Returns
     ([(sh, env)] device tensors of W*s*H*s*27 and W*s*H*s floats, stats).
     `outputs` may supply those tensors (reused across calls).  Bakes of fewer
     than `share_paths` paths share waves, larger ones get their own (0: half

@@ -1,6 +1,7 @@
-"""Batched bakes (shb_bake_batch): uneven scenes, sizes, spp and bounces in
-one persistent launch give results bit-identical to one plain bake each,
-with and without the CUDA graph, and with autotuned launch parameters."""
+"""Batched bakes (shb_bake_batch): uneven scenes, sizes, spp and bounces run
+through one shared launch sequence give results bit-identical to one plain
+bake each, with and without the CUDA graph, and with autotuned launch
+parameters."""
 import numpy as np
 import pytest
 
