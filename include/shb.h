@@ -21,6 +21,9 @@
  * One context owns one CUDA stream; use one context per host thread.
  * Entry points run on their context's device and give the calling thread
  * its previous current device back before they return.
+ * Image arguments hold at most 2^31 - 1 texels (the G-buffer limit of
+ * shb_rasterize) and shb_find_occlusion takes at most 2^31 - 1 rays per
+ * call; larger sizes are SHB_ERR_INVALID_ARG.
  *
  * Memory layouts are binary compatible with the reference's Eigen structs:
  *   shb_surface_point == sh_baker::SurfacePoint (64 bytes, Vector4f 16-byte

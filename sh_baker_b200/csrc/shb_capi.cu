@@ -290,6 +290,16 @@ static shb_status bad(const std::string& m) {
   return SHB_ERR_INVALID_ARG;
 }
 
+// Image arguments hold at most 2^31 - 1 texels, the G-buffer limit of
+// shb_rasterize, and shb_find_occlusion takes at most that many rays, so that
+// every byte count formed from them fits 64 bits and every texel index an
+// int32.  The size checks come before the handle checks.
+constexpr int64_t kMaxTexels = (1ll << 31) - 1;
+static bool too_many_texels(int64_t w, int64_t h) {
+  return w > 0 && h > 0 && (w > kMaxTexels || h > kMaxTexels || w * h > kMaxTexels);
+}
+static const char* kTooLarge = "image larger than 2^31 - 1 texels";
+
 // Host<->device staging for the host-pointer variants.
 struct Staging {
   shb_context* c;
@@ -696,8 +706,9 @@ shb_status shb_rasterize(shb_scene* s, const shb_raster_config* cfg, shb_surface
 
 shb_status shb_gbuffer_upload(shb_context* ctx, const shb_surface_point* points, int32_t width, int32_t height,
                               shb_gbuffer** out) {
-  if (!ctx || !points || !out) return bad("NULL argument");
   if (width <= 0 || height <= 0) return bad("width and height must be positive");
+  if (too_many_texels(width, height)) return bad(kTooLarge);
+  if (!ctx || !points || !out) return bad("NULL argument");
   SHB_ON_DEVICE(ctx->device);
   auto* g = new shb_gbuffer();
   g->ctx = ctx;
@@ -762,8 +773,9 @@ shb_status shb_validity_mask(shb_context* ctx, const shb_gbuffer* g, uint8_t* ma
 
 shb_status shb_downsample_validity_mask(shb_context* ctx, const uint8_t* in, int32_t width, int32_t height,
                                         int32_t scale, uint8_t* out, int32_t device_ptrs) {
-  if (!ctx || !in || !out) return bad("NULL argument");
   if (width <= 0 || height <= 0 || scale <= 0) return bad("width, height and scale must be positive");
+  if (too_many_texels((int64_t)width * scale, (int64_t)height * scale)) return bad(kTooLarge);
+  if (!ctx || !in || !out) return bad("NULL argument");
   SHB_ON_DEVICE(ctx->device);
   size_t nin = (size_t)width * scale * height * scale, nout = (size_t)width * height;
   const uint8_t* din = in;
@@ -818,6 +830,7 @@ shb_status shb_bake(shb_scene* s, const shb_gbuffer* g, const shb_raster_config*
 
 shb_status shb_save_sh_lightmap(shb_context* ctx, const float* sh, const float* env, int32_t width, int32_t height,
                                 int32_t device_ptrs, const char* path, int32_t mode) {
+  if (too_many_texels(width, height)) return bad(kTooLarge);
   if (!ctx || !sh || !path || !*path) return bad("NULL argument");
   if (width <= 0 || height <= 0) return bad("Invalid SHTexture dimensions or empty pixels.");
   if (mode < SHB_SAVE_COMBINED || mode > SHB_SAVE_LUMINANCE_PACKED) return bad("unknown save mode");
@@ -842,6 +855,7 @@ shb_status shb_save_sh_lightmap(shb_context* ctx, const float* sh, const float* 
 shb_status shb_sh_preview(shb_context* ctx, const float* sh, int32_t width, int32_t height, const float* normals,
                           const float direction[3], int32_t mode, int32_t reinhard, int32_t device_ptrs,
                           uint8_t* rgb_out) {
+  if (too_many_texels(width, height)) return bad(kTooLarge);
   if (!ctx || !sh || !rgb_out) return bad("NULL argument");
   if (width <= 0 || height <= 0) return bad("empty image");
   if (mode < SHB_PREVIEW_L0 || mode > SHB_PREVIEW_SH_PACKED) return bad("unknown preview mode");
@@ -955,8 +969,10 @@ shb_status shb_backward(shb_scene* s, const shb_gbuffer* g, const shb_raster_con
 
 shb_status shb_downsample(shb_context* ctx, const float* in, int32_t in_width, int32_t in_height, int32_t channels,
                           int32_t scale, float* out, int32_t device_ptrs) {
-  if (!ctx || !in || !out) return bad("NULL argument");
   if (in_width <= 0 || in_height <= 0 || channels <= 0 || scale <= 0) return bad("sizes must be positive");
+  if (too_many_texels(in_width, in_height) || (int64_t)in_width * in_height * channels > 27 * kMaxTexels)
+    return bad("image larger than 2^31 - 1 texels or 27 * (2^31 - 1) floats");
+  if (!ctx || !in || !out) return bad("NULL argument");
   SHB_ON_DEVICE(ctx->device);
   size_t nin = (size_t)in_width * in_height * channels;
   size_t nout = scale <= 1 ? nin : (size_t)(in_width / scale) * (in_height / scale) * channels;
@@ -978,6 +994,7 @@ shb_status shb_downsample(shb_context* ctx, const float* in, int32_t in_width, i
 
 shb_status shb_dilate(shb_context* ctx, int32_t kind, int32_t width, int32_t height, void* pixels, uint8_t* mask,
                       int32_t passes, int32_t device_ptrs) {
+  if (too_many_texels(width, height)) return bad(kTooLarge);
   if (!ctx) return bad("ctx is NULL");
   if (kind < SHB_DILATE_SH9 || kind > SHB_DILATE_U8) return bad("bad dilate kind");
   if (width <= 0 || height <= 0 || passes <= 0) return SHB_OK;  // reference: nothing to do
@@ -1059,6 +1076,7 @@ shb_status shb_bake_pipeline(shb_scene* s, const shb_pipeline_config* cfg, float
 }
 
 shb_status shb_find_occlusion(shb_scene* s, const shb_ray* rays, int64_t count, shb_hit* hits, int32_t device_ptrs) {
+  if (count > kMaxTexels) return bad("more than 2^31 - 1 rays in one call");
   if (!s || (count > 0 && (!rays || !hits))) return bad("NULL argument");
   if (count <= 0) return SHB_OK;
   shb_context* c = s->ctx;

@@ -58,6 +58,34 @@ def test_context_without_gpu_fails_cleanly(lib):
     assert b"CUDA" in lib.shb_last_error() or b"device" in lib.shb_last_error()
 
 
+def test_oversized_arguments_are_rejected_before_any_device_work(lib):
+    """Sizes whose byte counts could wrap are refused by the C ABI itself:
+    image arguments above 2^31 - 1 texels (the limit shb_rasterize applies to
+    its G-buffer) and more than 2^31 - 1 rays per shb_find_occlusion call.
+    The size checks come before the handle checks, so NULL handles show which
+    check answered."""
+    big = (65536, 32768)  # 2^31 texels
+    out = C.c_void_p()
+
+    def err(st):
+        assert st == 1, st  # SHB_ERR_INVALID_ARG
+        return lib.shb_last_error().decode()
+
+    assert "2^31 - 1 texels" in err(lib.shb_gbuffer_upload(None, None, *big, C.byref(out)))
+    assert "NULL" in err(lib.shb_gbuffer_upload(None, None, 4, 4, C.byref(out)))
+    assert "2^31 - 1 texels" in err(lib.shb_downsample_validity_mask(None, None, 30000, 30000, 3, None, 0))
+    assert "NULL" in err(lib.shb_downsample_validity_mask(None, None, 100, 100, 3, None, 0))
+    assert "2^31 - 1 texels" in err(lib.shb_downsample(None, None, 46341, 46341, 1, 1, None, 0))
+    assert "floats" in err(lib.shb_downsample(None, None, 2**31 - 1, 1, 28, 1, None, 0))
+    assert "NULL" in err(lib.shb_downsample(None, None, 2**31 - 1, 1, 27, 1, None, 0))
+    assert "2^31 - 1 texels" in err(lib.shb_dilate(None, A.DILATE_SH9, *big, None, None, 1, 0))
+    assert "NULL" in err(lib.shb_dilate(None, A.DILATE_SH9, 0, 5, None, None, 1, 0))
+    assert "2^31 - 1 texels" in err(lib.shb_save_sh_lightmap(None, None, None, *big, 0, b"x.exr", 0))
+    assert "2^31 - 1 texels" in err(lib.shb_sh_preview(None, None, *big, None, None, 0, 0, 0, None))
+    assert "rays" in err(lib.shb_find_occlusion(None, None, 2**31, None, 0))
+    assert "NULL" in err(lib.shb_find_occlusion(None, None, 2**31 - 1, None, 0))
+
+
 def test_struct_layouts_match_header(tmp_path):
     """Compiles a probe against include/shb.h and compares sizes/offsets
     with the ctypes mirror."""
