@@ -30,6 +30,8 @@
 #include "tspace.h"
 
 #include <algorithm>
+#include <cfloat>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -71,8 +73,38 @@ struct Json {
     const Json* j = get(k);
     return j && j->kind == Num ? j->num : def;
   }
-  int integer(const std::string& k, int def) const { return (int)number(k, def); }
+  // `def` when the key is absent or not a number; INT_MIN (an index no
+  // array has) when the number is not an integer that fits an int.
+  int integer(const std::string& k, int def) const {
+    const Json* j = get(k);
+    return j && j->kind == Num ? to_index(j->num, INT_MIN) : def;
+  }
+  // A JSON number as an int: the value when it is integral and fits an int,
+  // else `bad` (an out-of-range double-to-int conversion is undefined).
+  static int to_index(double x, int bad) {
+    return x >= -2147483648.0 && x <= 2147483647.0 && x == std::floor(x) ? (int)x : bad;
+  }
 };
+
+// An accessor or buffer-view size field (count, byteOffset, byteLength,
+// byteStride): 0 when absent, false unless it is an integral number in
+// [0, 2^53].
+bool size_field(const Json& o, const char* k, size_t& out) {
+  const Json* j = o.get(k);
+  out = 0;
+  if (!j) return true;
+  if (j->kind != Json::Num || !(j->num >= 0.0 && j->num <= 9007199254740992.0) || j->num != std::floor(j->num))
+    return false;
+  out = (size_t)j->num;
+  return true;
+}
+
+// A JSON number as a float: the nearest float, with magnitudes beyond the
+// float range taken to infinity explicitly (C++ leaves that cast undefined).
+float to_f32(double x) {
+  if (std::isfinite(x) && std::fabs(x) > (double)FLT_MAX) return x > 0 ? INFINITY : -INFINITY;
+  return (float)x;
+}
 
 struct Parser {
   const char* p;
@@ -465,7 +497,11 @@ bool accessor(const Model& m, int idx, View& v, std::string& err) {
   v.comp_type = a->integer("componentType", 0);
   const Json* t = a->get("type");
   v.comps = t && t->kind == Json::Str ? type_comps(t->str) : 0;
-  v.count = (size_t)a->number("count", 0);
+  size_t a_off = 0;
+  if (!size_field(*a, "count", v.count) || !size_field(*a, "byteOffset", a_off)) {
+    err = "accessor count and byteOffset must be non-negative integers";
+    return false;
+  }
   const int cs = comp_size(v.comp_type);
   if (!cs || !v.comps) {
     err = "bad accessor type";
@@ -476,7 +512,7 @@ bool accessor(const Model& m, int idx, View& v, std::string& err) {
     err = "accessor without bufferView";
     return false;
   }
-  const Json* bv = arr_at(m.j, "bufferViews", (int)bvi->num);
+  const Json* bv = bvi->kind == Json::Num ? arr_at(m.j, "bufferViews", Json::to_index(bvi->num, -1)) : nullptr;
   if (!bv) {
     err = "bad bufferView index";
     return false;
@@ -486,18 +522,23 @@ bool accessor(const Model& m, int idx, View& v, std::string& err) {
     err = "bad buffer index";
     return false;
   }
-  const size_t off = (size_t)bv->number("byteOffset", 0) + (size_t)a->number("byteOffset", 0);
-  const size_t len = (size_t)bv->number("byteLength", 0);
+  size_t view_begin = 0, len = 0;
+  if (!size_field(*bv, "byteOffset", view_begin) || !size_field(*bv, "byteLength", len) ||
+      !size_field(*bv, "byteStride", v.stride)) {
+    err = "bufferView byteOffset, byteLength and byteStride must be non-negative integers";
+    return false;
+  }
   const size_t elem = (size_t)cs * v.comps;
-  v.stride = (size_t)bv->number("byteStride", 0);
   if (!v.stride) v.stride = elem;
-  const size_t need = v.count ? (v.count - 1) * v.stride + elem : 0;
-  const size_t view_begin = (size_t)bv->number("byteOffset", 0);
-  if (off + need > view_begin + len || view_begin + len > m.buffers[b].size()) {
+  // in 128 bits: counts and offsets up to 2^53 cannot wrap the check
+  using u128 = unsigned __int128;
+  const u128 need = v.count ? (u128)(v.count - 1) * v.stride + elem : 0;
+  const u128 off = (u128)view_begin + a_off;
+  if (off + need > (u128)view_begin + len || (u128)view_begin + len > m.buffers[b].size()) {
     err = "accessor exceeds its buffer";
     return false;
   }
-  v.data = m.buffers[b].data() + off;
+  v.data = m.buffers[b].data() + (size_t)off;
   return true;
 }
 
@@ -517,7 +558,7 @@ bool float_attr(const Model& m, int idx, int comps, std::vector<float>& out, siz
 // Column-major 4x4 (glTF) -> our 3x4 row-major [L | t]
 void mat_from_gltf(const double m[16], float out[12]) {
   for (int r = 0; r < 3; ++r)
-    for (int c = 0; c < 4; ++c) out[r * 4 + c] = (float)m[c * 4 + r];
+    for (int c = 0; c < 4; ++c) out[r * 4 + c] = to_f32(m[c * 4 + r]);
 }
 
 // Eigen Affine3f composition: identity.translate(t).rotate(q).scale(s) = T R S
@@ -532,14 +573,14 @@ void node_local(const Json& node, float out[12]) {
   float t[3] = {0, 0, 0}, q[4] = {0, 0, 0, 1}, s[3] = {1, 1, 1};
   const Json* tj = node.get("translation");
   if (tj && tj->kind == Json::Arr && tj->arr.size() == 3)
-    for (int i = 0; i < 3; ++i) t[i] = (float)tj->arr[i].num;
+    for (int i = 0; i < 3; ++i) t[i] = to_f32(tj->arr[i].num);
   const Json* rj = node.get("rotation");
   bool has_r = rj && rj->kind == Json::Arr && rj->arr.size() == 4;
   if (has_r)
-    for (int i = 0; i < 4; ++i) q[i] = (float)rj->arr[i].num;
+    for (int i = 0; i < 4; ++i) q[i] = to_f32(rj->arr[i].num);
   const Json* sj = node.get("scale");
   if (sj && sj->kind == Json::Arr && sj->arr.size() == 3)
-    for (int i = 0; i < 3; ++i) s[i] = (float)sj->arr[i].num;
+    for (int i = 0; i < 3; ++i) s[i] = to_f32(sj->arr[i].num);
   // Eigen's quaternion -> matrix (expects a unit quaternion, not normalised)
   const float x = q[0], y = q[1], z = q[2], w = q[3];
   float R[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
@@ -572,11 +613,22 @@ void compose(const float a[12], const float b[12], float out[12]) {
   }
 }
 
+// The reference casts the rounded value straight to uint8_t, which C++
+// leaves undefined outside [0, 255] (a baseColorFactor above 1 or below 0).
+// Compiled for x86-64 that cast is a truncating conversion to a 32-bit
+// integer (INT_MIN for values out of its range and for NaN) whose low byte
+// is kept; the same steps are written out here without undefined behaviour.
+uint8_t byte_of(float r) {
+  const int32_t i = r >= -2147483648.0f && r < 2147483648.0f ? (int32_t)r : INT32_MIN;
+  return (uint8_t)(uint32_t)i;
+}
+
 // src/colorspace.h:17-21
 uint8_t linear_to_srgb(float x) {
-  if (x <= 0.0031308f) return static_cast<uint8_t>(std::rint(x * 12.92f * 255.0f));
-  return static_cast<uint8_t>(std::rint((1.055f * std::pow(x, 1.0f / 2.4f) - 0.055f) * 255.0f));
+  if (x <= 0.0031308f) return byte_of(std::rint(x * 12.92f * 255.0f));
+  return byte_of(std::rint((1.055f * std::pow(x, 1.0f / 2.4f) - 0.055f) * 255.0f));
 }
+
 
 float surface_area(const shb_host_scene::Geo& g) {
   float total = 0.0f;
@@ -610,7 +662,7 @@ struct Loader {
     if (mat < 0) return fail("Primitive missing material.");
     auto attr = [&](const char* k) -> int {
       const Json* a = attrs ? attrs->get(k) : nullptr;
-      return a && a->kind == Json::Num ? (int)a->num : -1;
+      return a && a->kind == Json::Num ? Json::to_index(a->num, -1) : -1;
     };
     if (attr("POSITION") < 0) return fail("Primitive missing POSITION attribute.");
     if (attr("NORMAL") < 0) return fail("Primitive missing NORMAL attribute. Baking requires Vertex Normals.");
@@ -706,12 +758,12 @@ struct Loader {
     }
     const Json* c = l.get("color");
     if (c && c->kind == Json::Arr && c->arr.size() == 3)
-      for (int k = 0; k < 3; ++k) L.color[k] = (float)c->arr[k].num;
-    L.intensity = (float)l.number("intensity", 1.0);
+      for (int k = 0; k < 3; ++k) L.color[k] = to_f32(c->arr[k].num);
+    L.intensity = to_f32(l.number("intensity", 1.0));
     const Json* sp = l.get("spot");
     if (L.type == SHB_LIGHT_SPOT && sp) {
-      if (sp->get("innerConeAngle")) L.cos_inner_cone = std::cos((float)sp->number("innerConeAngle", 0));
-      if (sp->get("outerConeAngle")) L.cos_outer_cone = std::cos((float)sp->number("outerConeAngle", 0));
+      if (sp->get("innerConeAngle")) L.cos_inner_cone = std::cos(to_f32(sp->number("innerConeAngle", 0)));
+      if (sp->get("outerConeAngle")) L.cos_outer_cone = std::cos(to_f32(sp->number("outerConeAngle", 0)));
     }
     s->lights.push_back(L);
   }
@@ -744,7 +796,7 @@ struct Loader {
     const Json* ch = n->get("children");
     if (ch && ch->kind == Json::Arr)
       for (const Json& c : ch->arr)
-        if (!node((int)c.num, xf, depth + 1)) return false;
+        if (!node(c.kind == Json::Num ? Json::to_index(c.num, -1) : -1, xf, depth + 1)) return false;
     return true;
   }
 
@@ -763,8 +815,10 @@ struct Loader {
       const Json* bv = arr_at(m.j, "bufferViews", img->integer("bufferView", -1));
       const int b = bv ? bv->integer("buffer", -1) : -1;
       if (b < 0 || (size_t)b >= m.buffers.size()) return fail("bad image bufferView");
-      const size_t off = (size_t)bv->number("byteOffset", 0), len = (size_t)bv->number("byteLength", 0);
-      if (off + len > m.buffers[b].size()) return fail("image exceeds its buffer");
+      size_t off = 0, len = 0;
+      if (!size_field(*bv, "byteOffset", off) || !size_field(*bv, "byteLength", len) ||
+          off > m.buffers[b].size() || len > m.buffers[b].size() - off)
+        return fail("image exceeds its buffer");
       bytes.assign(m.buffers[b].begin() + off, m.buffers[b].begin() + off + len);
     } else {
       return true;
@@ -789,7 +843,7 @@ struct Loader {
       if (nm && nm->kind == Json::Str) M.name = nm->str;
       const Json* ext = gm.get("extensions");
       const Json* es = ext ? ext->get("KHR_materials_emissive_strength") : nullptr;
-      if (es && es->get("emissiveStrength")) M.emission = (float)es->number("emissiveStrength", 0.0);
+      if (es && es->get("emissiveStrength")) M.emission = to_f32(es->number("emissiveStrength", 0.0));
       const Json* pbr = gm.get("pbrMetallicRoughness");
       const Json* bct = pbr ? pbr->get("baseColorTexture") : nullptr;
       if (bct && !texture(bct->integer("index", -1), M)) return false;
@@ -798,8 +852,8 @@ struct Loader {
         M.c = 4;
         const Json* f = pbr ? pbr->get("baseColorFactor") : nullptr;
         if (f && f->kind == Json::Arr && f->arr.size() == 4) {
-          M.px = {linear_to_srgb((float)f->arr[0].num), linear_to_srgb((float)f->arr[1].num),
-                  linear_to_srgb((float)f->arr[2].num),
+          M.px = {linear_to_srgb(to_f32(f->arr[0].num)), linear_to_srgb(to_f32(f->arr[1].num)),
+                  linear_to_srgb(to_f32(f->arr[2].num)),
                   (uint8_t)std::rint(std::min(std::max(f->arr[3].num, 0.0), 1.0) * 255.0)};
         } else {
           M.px = {255, 255, 255, 255};
@@ -858,7 +912,7 @@ struct Loader {
     const Json* nodes = sc->get("nodes");
     if (nodes && nodes->kind == Json::Arr)
       for (const Json& n : nodes->arr)
-        if (!node((int)n.num, I, 0)) return false;
+        if (!node(n.kind == Json::Num ? Json::to_index(n.num, -1) : -1, I, 0)) return false;
     return true;
   }
 };
@@ -1124,56 +1178,64 @@ extern "C" {
 
 shb_status shb_save_gltf(const shb_scene_desc* scene, const char* const* material_names,
                          const char* const* albedo_files, const char* path) {
-  if (!scene || !path || !*path) {
-    shb::set_error("NULL argument");
-    return SHB_ERR_INVALID_ARG;
-  }
-  std::string err;
-  if (!shb::save_gltf(*scene, material_names, albedo_files, path, err)) {
-    shb::set_error("SaveScene: " + err);
-    return SHB_ERR_INVALID_ARG;
-  }
-  return SHB_OK;
+  return ::shb::guarded("shb_save_gltf", [&]() -> shb_status {
+    if (!scene || !path || !*path) {
+      shb::set_error("NULL argument");
+      return SHB_ERR_INVALID_ARG;
+    }
+    std::string err;
+    if (!shb::save_gltf(*scene, material_names, albedo_files, path, err)) {
+      shb::set_error("SaveScene: " + err);
+      return SHB_ERR_INVALID_ARG;
+    }
+    return SHB_OK;
+  });
 }
 
 shb_status shb_host_scene_material_info(const shb_host_scene* s, int32_t material, const char** name,
                                         const char** albedo_file) {
-  if (!s || material < 0 || (size_t)material >= s->mats.size()) {
-    shb::set_error("bad material index");
-    return SHB_ERR_INVALID_ARG;
-  }
-  if (name) *name = s->mats[(size_t)material].name.c_str();
-  if (albedo_file) {
-    const std::string& f = s->mats[(size_t)material].albedo_file;
-    *albedo_file = f.empty() ? nullptr : f.c_str();
-  }
-  return SHB_OK;
+  return ::shb::guarded("shb_host_scene_material_info", [&]() -> shb_status {
+    if (!s || material < 0 || (size_t)material >= s->mats.size()) {
+      shb::set_error("bad material index");
+      return SHB_ERR_INVALID_ARG;
+    }
+    if (name) *name = s->mats[(size_t)material].name.c_str();
+    if (albedo_file) {
+      const std::string& f = s->mats[(size_t)material].albedo_file;
+      *albedo_file = f.empty() ? nullptr : f.c_str();
+    }
+    return SHB_OK;
+  });
 }
 
 
 shb_status shb_load_gltf(const char* path, shb_host_scene** out) {
-  if (!path || !out) {
-    shb::set_error("NULL argument");
-    return SHB_ERR_INVALID_ARG;
-  }
-  *out = nullptr;
-  std::unique_ptr<shb_host_scene> s(new shb_host_scene());
-  shb::Loader L;
-  L.s = s.get();
-  if (!L.load(path)) {
-    shb::set_error("LoadScene: " + L.err);
-    return SHB_ERR_INVALID_ARG;
-  }
-  s->finish();
-  *out = s.release();
-  return SHB_OK;
+  return ::shb::guarded("shb_load_gltf", [&]() -> shb_status {
+    if (!path || !out) {
+      shb::set_error("NULL argument");
+      return SHB_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    std::unique_ptr<shb_host_scene> s(new shb_host_scene());
+    shb::Loader L;
+    L.s = s.get();
+    if (!L.load(path)) {
+      shb::set_error("LoadScene: " + L.err);
+      return SHB_ERR_INVALID_ARG;
+    }
+    s->finish();
+    *out = s.release();
+    return SHB_OK;
+  });
 }
 
 const shb_scene_desc* shb_host_scene_desc(const shb_host_scene* s) { return s ? &s->desc : nullptr; }
 
 shb_status shb_host_scene_destroy(shb_host_scene* s) {
-  delete s;
-  return SHB_OK;
+  return ::shb::guarded("shb_host_scene_destroy", [&]() -> shb_status {
+    delete s;
+    return SHB_OK;
+  });
 }
 
 }  // extern "C"

@@ -286,3 +286,61 @@ def test_damaged_jpeg_files_fail_cleanly(tmp_path):
             err = []
             sc = api.LoadScene(b.write(tmp_path / f"{n}_{t}.gltf"), err)
             assert sc is not None or "JPEG" in err[0], err
+
+
+@pytest.mark.parametrize("field,value,what", [
+    ("count", 2 ** 53, "exceeds its buffer"),         # (count - 1) * stride would wrap 64 bits at 2^62
+    ("count", 2 ** 62, "non-negative integers"),
+    ("count", 1e300, "non-negative integers"),
+    ("count", -1, "non-negative integers"),
+    ("count", 2.5, "non-negative integers"),
+    ("byteOffset", 2 ** 62, "non-negative integers"),
+    ("bufferView", 1e300, "bufferView"),
+])
+def test_malformed_accessor_numbers_are_errors(tmp_path, field, value, what):
+    """Accessor sizes and indices that are not integers in range are load
+    errors, checked before any arithmetic on them (a count near 2^62 used to
+    wrap the bounds check of (count - 1) * stride)."""
+    pos, nrm, uv, idx = quad()
+    b = GltfBuilder()
+    b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=b.material(factor=[1, 1, 1, 1]))]))
+    acc = b.j["meshes"][0]["primitives"][0]["attributes"]["POSITION"]
+    b.j["accessors"][acc][field] = value
+    err = []
+    assert api.LoadScene(b.write(tmp_path / "m.gltf"), err) is None
+    assert what in err[0], err
+
+
+def test_out_of_range_indices_are_not_cast(tmp_path):
+    pos, nrm, uv, idx = quad()
+
+    def build():
+        b = GltfBuilder()
+        b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=b.material(factor=[1, 1, 1, 1]))]))
+        return b
+
+    b = build()
+    b.j["nodes"][0]["children"] = [1e300]
+    err = []
+    assert api.LoadScene(b.write(tmp_path / "c.gltf"), err) is None and "node" in err[0]
+    b = build()
+    b.j["meshes"][0]["primitives"][0]["material"] = 1e20
+    err = []
+    assert api.LoadScene(b.write(tmp_path / "m.gltf"), err) is None and "material" in err[0]
+    b = build()
+    b.j["meshes"][0]["primitives"][0]["indices"] = -1e300  # not an index: the primitive has no triangles
+    assert len(api.LoadScene(b.write(tmp_path / "i.gltf")).geometries[0].indices) == 0
+
+
+def test_base_colour_factor_outside_unit_range_keeps_the_low_byte(tmp_path):
+    """LinearToSRGB (src/colorspace.h:17-21) casts the rounded value to
+    uint8_t.  For factors outside [0, 1] that cast is undefined in C++; the
+    reference compiled for x86-64 converts to a 32-bit integer and keeps its
+    low byte, and the loader writes out those steps: 1.5 rounds to 305 (byte
+    49), -0.5 to -1647 (byte 145)."""
+    pos, nrm, uv, idx = quad()
+    b = GltfBuilder()
+    b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=b.material(factor=[1.5, -0.5, 0.25, 1]))]))
+    px = list(api.LoadScene(b.write(tmp_path / "f.gltf")).materials[0].albedo.pixel_data)
+    assert linear_to_srgb(1.5) == 305 and linear_to_srgb(-0.5) == -1647
+    assert px == [305 & 0xFF, -1647 & 0xFF, linear_to_srgb(0.25), 255]
