@@ -559,160 +559,164 @@ using namespace shb;
 extern "C" {
 
 shb_status shb_atlas_geometry_scales(const shb_scene_desc* scene, float density_multiplier, float* scales_out) {
-  if (!scene || (scene->geometry_count && (!scene->geometries || !scales_out))) {
-    set_error("NULL argument");
-    return SHB_ERR_INVALID_ARG;
-  }
-  std::vector<float> s;
-  std::string err;
-  if (!geometry_scales(scene, density_multiplier, s, err)) {
-    set_error("CalculateGeometryScales: " + err);
-    return SHB_ERR_INVALID_ARG;
-  }
-  if (!s.empty()) std::memcpy(scales_out, s.data(), sizeof(float) * s.size());
-  return SHB_OK;
+  return ::shb::guarded("shb_atlas_geometry_scales", [&]() -> shb_status {
+    if (!scene || (scene->geometry_count && (!scene->geometries || !scales_out))) {
+      set_error("NULL argument");
+      return SHB_ERR_INVALID_ARG;
+    }
+    std::vector<float> s;
+    std::string err;
+    if (!geometry_scales(scene, density_multiplier, s, err)) {
+      set_error("CalculateGeometryScales: " + err);
+      return SHB_ERR_INVALID_ARG;
+    }
+    if (!s.empty()) std::memcpy(scales_out, s.data(), sizeof(float) * s.size());
+    return SHB_OK;
+  });
 }
 
 shb_status shb_create_atlas(const shb_scene_desc* scene, uint32_t target_resolution, uint32_t padding,
                             float density_multiplier, shb_host_scene** out, int32_t* width, int32_t* height) {
-  if (!scene || !out) {
-    set_error("NULL argument");
-    return SHB_ERR_INVALID_ARG;
-  }
-  *out = nullptr;
-  auto fail = [](const std::string& m) {
-    set_error("CreateAtlasGeometries: " + m);
-    return SHB_ERR_INVALID_ARG;
-  };
-  if (scene->geometry_count == 0 || !scene->geometries) return fail("no geometries");
-  if (target_resolution == 0 || target_resolution > 65536 || padding > 65536)
-    return fail("target_resolution must be 1..65536 and padding at most 65536");
-  std::vector<float> scales;
-  std::string err;
-  if (!geometry_scales(scene, density_multiplier, scales, err)) return fail(err);
-  const uint32_t ng = scene->geometry_count;
-  for (uint32_t g = 0; g < ng; ++g) {
-    const shb_geometry_desc& G = scene->geometries[g];
-    if (!G.vertices || !G.normals || !G.tangents)
-      return fail("geometry " + std::to_string(g) + ": vertices, normals and tangents required");
-    if (G.index_count && !G.indices) return fail("geometry " + std::to_string(g) + ": indices is NULL");
-    for (uint32_t i = 0; i < G.index_count / 3 * 3; ++i)
-      if (G.indices[i] >= G.vertex_count) return fail("geometry " + std::to_string(g) + ": index out of range");
-    // a scale of zero (an albedo of 0 texels) would collapse every chart
-    if (!(scales[g] >= kMinScale)) scales[g] = kMinScale;
-  }
-  // charts, geometries in parallel
-  std::vector<GeoCharts> gc(ng);
-  {
-    std::atomic<uint32_t> next{0};
-    auto work = [&] {
-      for (uint32_t g; (g = next.fetch_add(1)) < ng;) build_charts(scene->geometries[g], scales[g], gc[g]);
+  return ::shb::guarded("shb_create_atlas", [&]() -> shb_status {
+    if (!scene || !out) {
+      set_error("NULL argument");
+      return SHB_ERR_INVALID_ARG;
+    }
+    *out = nullptr;
+    auto fail = [](const std::string& m) {
+      set_error("CreateAtlasGeometries: " + m);
+      return SHB_ERR_INVALID_ARG;
     };
-    const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), ng));
-    std::vector<std::thread> pool;
-    for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
-    work();
-    for (auto& t : pool) t.join();
-  }
-  std::vector<Rect> rects;
-  double sum_area = 0;
-  for (uint32_t g = 0; g < ng; ++g)
-    for (uint32_t c = 0; c < gc[g].charts.size(); ++c) {
-      const Chart& ch = gc[g].charts[c];
-      rects.push_back(Rect{g, c, ch.w, ch.h});
-      sum_area += ch.w * ch.h;
+    if (scene->geometry_count == 0 || !scene->geometries) return fail("no geometries");
+    if (target_resolution == 0 || target_resolution > 65536 || padding > 65536)
+      return fail("target_resolution must be 1..65536 and padding at most 65536");
+    std::vector<float> scales;
+    std::string err;
+    if (!geometry_scales(scene, density_multiplier, scales, err)) return fail(err);
+    const uint32_t ng = scene->geometry_count;
+    for (uint32_t g = 0; g < ng; ++g) {
+      const shb_geometry_desc& G = scene->geometries[g];
+      if (!G.vertices || !G.normals || !G.tangents)
+        return fail("geometry " + std::to_string(g) + ": vertices, normals and tangents required");
+      if (G.index_count && !G.indices) return fail("geometry " + std::to_string(g) + ": indices is NULL");
+      for (uint32_t i = 0; i < G.index_count / 3 * 3; ++i)
+        if (G.indices[i] >= G.vertex_count) return fail("geometry " + std::to_string(g) + ": index out of range");
+      // a scale of zero (an albedo of 0 texels) would collapse every chart
+      if (!(scales[g] >= kMinScale)) scales[g] = kMinScale;
     }
-  const int W = (int)target_resolution, H = (int)target_resolution, pad = (int)padding;
-  double s = 1.0;
-  if (!rects.empty()) {
-    // texels per unit: the largest that fits, by bisection (area bound above)
-    double hi = sum_area > 0 ? std::sqrt((double)W * H / sum_area) : 1.0;
-    double lo = hi;
-    bool fits = false;
-    for (int i = 0; i < 64 && !fits; ++i) {
-      lo *= 0.5;
-      fits = pack(rects, lo, W, H, pad, nullptr);
-      if (!fits) {
-        bool all_unit = true;
-        for (const Rect& r : rects) all_unit = all_unit && foot(r.w, lo) == 1 && foot(r.h, lo) == 1;
-        if (all_unit) break;  // every chart is one texel: smaller scales cannot help
+    // charts, geometries in parallel
+    std::vector<GeoCharts> gc(ng);
+    {
+      std::atomic<uint32_t> next{0};
+      auto work = [&] {
+        for (uint32_t g; (g = next.fetch_add(1)) < ng;) build_charts(scene->geometries[g], scales[g], gc[g]);
+      };
+      const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), ng));
+      std::vector<std::thread> pool;
+      for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
+      work();
+      for (auto& t : pool) t.join();
+    }
+    std::vector<Rect> rects;
+    double sum_area = 0;
+    for (uint32_t g = 0; g < ng; ++g)
+      for (uint32_t c = 0; c < gc[g].charts.size(); ++c) {
+        const Chart& ch = gc[g].charts[c];
+        rects.push_back(Rect{g, c, ch.w, ch.h});
+        sum_area += ch.w * ch.h;
       }
-    }
-    if (!fits)
-      return fail("could not fit " + std::to_string(rects.size()) + " charts into one " + std::to_string(W) + "x" +
-                  std::to_string(H) + " atlas with padding " + std::to_string(pad));
-    if (sum_area > 0)
-      for (int i = 0; i < 30; ++i) {
-        const double mid = 0.5 * (lo + hi);
-        if (pack(rects, mid, W, H, pad, nullptr)) lo = mid;
-        else hi = mid;
-      }
-    s = lo;
-    std::vector<std::array<int, 3>> place;
-    pack(rects, s, W, H, pad, &place);
-    for (size_t i = 0; i < rects.size(); ++i) {
-      Chart& ch = gc[rects[i].geo].charts[rects[i].chart];
-      ch.ox = place[i][0];
-      ch.oy = place[i][1];
-      ch.turned = place[i][2] != 0;
-    }
-  }
-  std::unique_ptr<shb_host_scene> hs(new shb_host_scene());
-  hs->geos.resize(ng);
-  for (uint32_t g = 0; g < ng; ++g) {
-    const shb_geometry_desc& G = scene->geometries[g];
-    shb_host_scene::Geo& o = hs->geos[g];
-    o.material = G.material_id;
-    std::memcpy(o.transform, G.transform, sizeof(o.transform));
-    const uint32_t nf = G.index_count / 3;
-    std::unordered_map<uint64_t, uint32_t> vmap;
-    o.idx.resize(3 * (size_t)nf);
-    for (uint32_t f = 0; f < nf; ++f) {
-      const uint32_t c = gc[g].chart_of[f];
-      const Chart& ch = gc[g].charts[c];
-      const double fw = foot(ch.w, s), fh = foot(ch.h, s);
-      for (int k = 0; k < 3; ++k) {
-        const uint32_t v = G.indices[3 * f + k];
-        auto it = vmap.emplace(((uint64_t)c << 32) | v, (uint32_t)(o.v.size() / 3));
-        if (it.second) {
-          for (int a = 0; a < 3; ++a) {
-            o.v.push_back(G.vertices[3 * v + a]);
-            o.n.push_back(G.normals[3 * v + a]);
-          }
-          for (int a = 0; a < 4; ++a) o.t.push_back(G.tangents[4 * v + a]);
-          for (int a = 0; a < 2; ++a) o.uv0.push_back(G.texture_uvs[2 * v + a]);
-          // texel position: chart centred in its footprint
-          const D2 q = ch.corner[3 * (size_t)gc[g].slot_of[f] + k];
-          double x = q.x * s + 0.5 * (fw - ch.w * s), y = q.y * s + 0.5 * (fh - ch.h * s);
-          if (ch.turned) {  // quarter turn inside the placed footprint: (x, y) -> (fh - y, x)
-            const double t = x;
-            x = fh - y;
-            y = t;
-          }
-          const float u = (float)((ch.ox + x) / W), w = (float)((ch.oy + y) / H);
-          o.uv1.push_back(std::min(1.0f, std::max(0.0f, u)));
-          o.uv1.push_back(std::min(1.0f, std::max(0.0f, w)));
+    const int W = (int)target_resolution, H = (int)target_resolution, pad = (int)padding;
+    double s = 1.0;
+    if (!rects.empty()) {
+      // texels per unit: the largest that fits, by bisection (area bound above)
+      double hi = sum_area > 0 ? std::sqrt((double)W * H / sum_area) : 1.0;
+      double lo = hi;
+      bool fits = false;
+      for (int i = 0; i < 64 && !fits; ++i) {
+        lo *= 0.5;
+        fits = pack(rects, lo, W, H, pad, nullptr);
+        if (!fits) {
+          bool all_unit = true;
+          for (const Rect& r : rects) all_unit = all_unit && foot(r.w, lo) == 1 && foot(r.h, lo) == 1;
+          if (all_unit) break;  // every chart is one texel: smaller scales cannot help
         }
-        o.idx[3 * (size_t)f + k] = it.first->second;
+      }
+      if (!fits)
+        return fail("could not fit " + std::to_string(rects.size()) + " charts into one " + std::to_string(W) + "x" +
+                    std::to_string(H) + " atlas with padding " + std::to_string(pad));
+      if (sum_area > 0)
+        for (int i = 0; i < 30; ++i) {
+          const double mid = 0.5 * (lo + hi);
+          if (pack(rects, mid, W, H, pad, nullptr)) lo = mid;
+          else hi = mid;
+        }
+      s = lo;
+      std::vector<std::array<int, 3>> place;
+      pack(rects, s, W, H, pad, &place);
+      for (size_t i = 0; i < rects.size(); ++i) {
+        Chart& ch = gc[rects[i].geo].charts[rects[i].chart];
+        ch.ox = place[i][0];
+        ch.oy = place[i][1];
+        ch.turned = place[i][2] != 0;
       }
     }
-  }
-  for (uint32_t m = 0; m < scene->material_count; ++m) {
-    const shb_material_desc& M = scene->materials[m];
-    shb_host_scene::Mat mt;
-    mt.w = M.albedo_width;
-    mt.h = M.albedo_height;
-    mt.c = M.albedo_channels;
-    mt.emission = M.emission_intensity;
-    if (M.albedo_pixels) mt.px.assign(M.albedo_pixels, M.albedo_pixels + (size_t)mt.w * mt.h * mt.c);
-    hs->mats.push_back(std::move(mt));
-  }
-  if (scene->light_count && scene->lights) hs->lights.assign(scene->lights, scene->lights + scene->light_count);
-  hs->finish();
-  if (width) *width = W;
-  if (height) *height = H;
-  *out = hs.release();
-  return SHB_OK;
+    std::unique_ptr<shb_host_scene> hs(new shb_host_scene());
+    hs->geos.resize(ng);
+    for (uint32_t g = 0; g < ng; ++g) {
+      const shb_geometry_desc& G = scene->geometries[g];
+      shb_host_scene::Geo& o = hs->geos[g];
+      o.material = G.material_id;
+      std::memcpy(o.transform, G.transform, sizeof(o.transform));
+      const uint32_t nf = G.index_count / 3;
+      std::unordered_map<uint64_t, uint32_t> vmap;
+      o.idx.resize(3 * (size_t)nf);
+      for (uint32_t f = 0; f < nf; ++f) {
+        const uint32_t c = gc[g].chart_of[f];
+        const Chart& ch = gc[g].charts[c];
+        const double fw = foot(ch.w, s), fh = foot(ch.h, s);
+        for (int k = 0; k < 3; ++k) {
+          const uint32_t v = G.indices[3 * f + k];
+          auto it = vmap.emplace(((uint64_t)c << 32) | v, (uint32_t)(o.v.size() / 3));
+          if (it.second) {
+            for (int a = 0; a < 3; ++a) {
+              o.v.push_back(G.vertices[3 * v + a]);
+              o.n.push_back(G.normals[3 * v + a]);
+            }
+            for (int a = 0; a < 4; ++a) o.t.push_back(G.tangents[4 * v + a]);
+            for (int a = 0; a < 2; ++a) o.uv0.push_back(G.texture_uvs[2 * v + a]);
+            // texel position: chart centred in its footprint
+            const D2 q = ch.corner[3 * (size_t)gc[g].slot_of[f] + k];
+            double x = q.x * s + 0.5 * (fw - ch.w * s), y = q.y * s + 0.5 * (fh - ch.h * s);
+            if (ch.turned) {  // quarter turn inside the placed footprint: (x, y) -> (fh - y, x)
+              const double t = x;
+              x = fh - y;
+              y = t;
+            }
+            const float u = (float)((ch.ox + x) / W), w = (float)((ch.oy + y) / H);
+            o.uv1.push_back(std::min(1.0f, std::max(0.0f, u)));
+            o.uv1.push_back(std::min(1.0f, std::max(0.0f, w)));
+          }
+          o.idx[3 * (size_t)f + k] = it.first->second;
+        }
+      }
+    }
+    for (uint32_t m = 0; m < scene->material_count; ++m) {
+      const shb_material_desc& M = scene->materials[m];
+      shb_host_scene::Mat mt;
+      mt.w = M.albedo_width;
+      mt.h = M.albedo_height;
+      mt.c = M.albedo_channels;
+      mt.emission = M.emission_intensity;
+      if (M.albedo_pixels) mt.px.assign(M.albedo_pixels, M.albedo_pixels + (size_t)mt.w * mt.h * mt.c);
+      hs->mats.push_back(std::move(mt));
+    }
+    if (scene->light_count && scene->lights) hs->lights.assign(scene->lights, scene->lights + scene->light_count);
+    hs->finish();
+    if (width) *width = W;
+    if (height) *height = H;
+    *out = hs.release();
+    return SHB_OK;
+  });
 }
 
 }  // extern "C"

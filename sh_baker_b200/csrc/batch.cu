@@ -179,83 +179,85 @@ using namespace shb;
 
 extern "C" shb_status shb_bake_batch(shb_context* ctx, const shb_batch_item* items, int32_t count,
                                      const shb_batch_options* options, shb_bake_stats* stats) {
-  if (!ctx || (count > 0 && !items)) {
-    set_error("NULL argument");
-    return SHB_ERR_INVALID_ARG;
-  }
-  if (stats) std::memset(stats, 0, sizeof(*stats));
-  if (count <= 0) return SHB_OK;
-  SHB_ON_DEVICE(ctx->device);
-  std::vector<BakeSpec> specs;
-  specs.reserve(count);
-  for (int i = 0; i < count; ++i) {
-    const shb_batch_item& it = items[i];
-    std::string where = "batch item " + std::to_string(i) + ": ";
-    if (!it.scene || !it.gbuffer || !it.sh || !it.env_visibility) {
-      set_error(where + "NULL scene, gbuffer or output");
+  return ::shb::guarded("shb_bake_batch", [&]() -> shb_status {
+    if (!ctx || (count > 0 && !items)) {
+      set_error("NULL argument");
       return SHB_ERR_INVALID_ARG;
     }
-    if (it.scene->ctx != ctx || it.gbuffer->ctx != ctx) {
-      set_error(where + "scene and G-buffer must belong to the context");
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    if (count <= 0) return SHB_OK;
+    SHB_ON_DEVICE(ctx->device);
+    std::vector<BakeSpec> specs;
+    specs.reserve(count);
+    for (int i = 0; i < count; ++i) {
+      const shb_batch_item& it = items[i];
+      std::string where = "batch item " + std::to_string(i) + ": ";
+      if (!it.scene || !it.gbuffer || !it.sh || !it.env_visibility) {
+        set_error(where + "NULL scene, gbuffer or output");
+        return SHB_ERR_INVALID_ARG;
+      }
+      if (it.scene->ctx != ctx || it.gbuffer->ctx != ctx) {
+        set_error(where + "scene and G-buffer must belong to the context");
+        return SHB_ERR_INVALID_ARG;
+      }
+      const shb_bake_config& cfg = it.config;
+      if (cfg.samples <= 0 || cfg.bounces < 0 || cfg.bounces > 30 || cfg.num_light_samples <= 0 ||
+          cfg.rng_mode != SHB_RNG_PHILOX) {
+        set_error(where + "bad bake config");
+        return SHB_ERR_INVALID_ARG;
+      }
+      int64_t W = (int64_t)it.raster.width * it.raster.supersample_scale;
+      int64_t H = (int64_t)it.raster.height * it.raster.supersample_scale;
+      if (W != it.gbuffer->width || H != it.gbuffer->height) {
+        set_error(where + "G-buffer size does not match raster config");
+        return SHB_ERR_INVALID_ARG;
+      }
+      if (it.scene->bvh_depth > 64) {
+        set_error(where + "BVH deeper than the traversal stack");
+        return SHB_ERR_INVALID_ARG;
+      }
+      specs.push_back(BakeSpec{it.scene, it.gbuffer->points.as<shb_surface_point>(), (int)W, (int)H, cfg, it.sh,
+                               it.env_visibility});
+    }
+    BatchParams prm;
+    prm.use_graph = options && options->use_graph;
+    // defaults for batches: tiles of 8192 texels so that bakes mix in a wave
+    prm.tile_texels = int64_t(1) << 13;
+    if (options && options->autotune) {
+      const std::string file = tune_path(options->tune_cache);
+      const std::string key = device_name(ctx->device) + "|v2|" + shape_class(specs);
+      if (!lookup(file, key, &prm)) {
+        double cost = 0;
+        BatchParams best;
+        SHB_TRY(tune(ctx, specs, &best, &cost));
+        prm.wave_paths = best.wave_paths;
+        prm.tile_texels = best.tile_texels;
+        prm.grid_scale = best.grid_scale;
+        prm.share_paths = best.share_paths;
+        std::ofstream out(file, std::ios::app);
+        out << key << " " << prm.wave_paths << " " << prm.tile_texels << " " << prm.grid_scale << " "
+            << prm.share_paths << " " << cost << "\n";
+      }
+    }
+    if (options && options->wave_paths > 0) prm.wave_paths = options->wave_paths;
+    if (options && options->tile_texels > 0) prm.tile_texels = options->tile_texels;
+    if (options && options->grid_scale > 0) prm.grid_scale = options->grid_scale;
+    if (options && options->share_paths > 0) prm.share_paths = options->share_paths;
+    if (options && options->share_paths < 0) prm.share_paths = 0;
+    if (options && options->nee_split >= 0 && options->nee_split <= 2) prm.nee_split = options->nee_split;
+    if (options && options->max_traversal_steps < 0) {
+      set_error("max_traversal_steps must not be negative");
       return SHB_ERR_INVALID_ARG;
     }
-    const shb_bake_config& cfg = it.config;
-    if (cfg.samples <= 0 || cfg.bounces < 0 || cfg.bounces > 30 || cfg.num_light_samples <= 0 ||
-        cfg.rng_mode != SHB_RNG_PHILOX) {
-      set_error(where + "bad bake config");
+    if (options && options->queue_capacity < 0) {
+      set_error("queue_capacity must not be negative");
       return SHB_ERR_INVALID_ARG;
     }
-    int64_t W = (int64_t)it.raster.width * it.raster.supersample_scale;
-    int64_t H = (int64_t)it.raster.height * it.raster.supersample_scale;
-    if (W != it.gbuffer->width || H != it.gbuffer->height) {
-      set_error(where + "G-buffer size does not match raster config");
-      return SHB_ERR_INVALID_ARG;
-    }
-    if (it.scene->bvh_depth > 64) {
-      set_error(where + "BVH deeper than the traversal stack");
-      return SHB_ERR_INVALID_ARG;
-    }
-    specs.push_back(BakeSpec{it.scene, it.gbuffer->points.as<shb_surface_point>(), (int)W, (int)H, cfg, it.sh,
-                             it.env_visibility});
-  }
-  BatchParams prm;
-  prm.use_graph = options && options->use_graph;
-  // defaults for batches: tiles of 8192 texels so that bakes mix in a wave
-  prm.tile_texels = int64_t(1) << 13;
-  if (options && options->autotune) {
-    const std::string file = tune_path(options->tune_cache);
-    const std::string key = device_name(ctx->device) + "|v2|" + shape_class(specs);
-    if (!lookup(file, key, &prm)) {
-      double cost = 0;
-      BatchParams best;
-      SHB_TRY(tune(ctx, specs, &best, &cost));
-      prm.wave_paths = best.wave_paths;
-      prm.tile_texels = best.tile_texels;
-      prm.grid_scale = best.grid_scale;
-      prm.share_paths = best.share_paths;
-      std::ofstream out(file, std::ios::app);
-      out << key << " " << prm.wave_paths << " " << prm.tile_texels << " " << prm.grid_scale << " "
-          << prm.share_paths << " " << cost << "\n";
-    }
-  }
-  if (options && options->wave_paths > 0) prm.wave_paths = options->wave_paths;
-  if (options && options->tile_texels > 0) prm.tile_texels = options->tile_texels;
-  if (options && options->grid_scale > 0) prm.grid_scale = options->grid_scale;
-  if (options && options->share_paths > 0) prm.share_paths = options->share_paths;
-  if (options && options->share_paths < 0) prm.share_paths = 0;
-  if (options && options->nee_split >= 0 && options->nee_split <= 2) prm.nee_split = options->nee_split;
-  if (options && options->max_traversal_steps < 0) {
-    set_error("max_traversal_steps must not be negative");
-    return SHB_ERR_INVALID_ARG;
-  }
-  if (options && options->queue_capacity < 0) {
-    set_error("queue_capacity must not be negative");
-    return SHB_ERR_INVALID_ARG;
-  }
-  if (options) prm.max_iters = (uint32_t)options->max_traversal_steps;
-  if (options) prm.queue_cap = options->queue_capacity;
-  uint64_t l0 = ctx->launches;
-  SHB_TRY(bake_batch_device(ctx, specs, prm, stats));
-  if (stats) stats->kernel_launches = ctx->launches - l0;
-  return SHB_OK;
+    if (options) prm.max_iters = (uint32_t)options->max_traversal_steps;
+    if (options) prm.queue_cap = options->queue_capacity;
+    uint64_t l0 = ctx->launches;
+    SHB_TRY(bake_batch_device(ctx, specs, prm, stats));
+    if (stats) stats->kernel_launches = ctx->launches - l0;
+    return SHB_OK;
+  });
 }

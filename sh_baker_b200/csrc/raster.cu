@@ -514,67 +514,69 @@ shb_status noalloc_prepare(int device) {
 
 extern "C" SHB_API shb_status shb_dilate_noalloc(shb_context* ctx, int32_t kind, int32_t width, int32_t height,
                                                  void* pixels, uint8_t* mask, int32_t passes) {
-  using namespace shb;
-  if (!ctx) {
-    set_error("ctx is NULL");
-    return SHB_ERR_INVALID_ARG;
-  }
-  if (kind < SHB_DILATE_SH9 || kind > SHB_DILATE_U8) {
-    set_error("bad dilate kind");
-    return SHB_ERR_INVALID_ARG;
-  }
-  if (width <= 0 || height <= 0 || passes <= 0) return SHB_OK;  // nothing to do, as Dilate<T>
-  if (!pixels || !mask) {
-    set_error("NULL argument");
-    return SHB_ERR_INVALID_ARG;
-  }
-  const int64_t n = (int64_t)width * height;  // width, height > 0 and < 2^31: no overflow
-  const int ch = kind == SHB_DILATE_SH9 ? 27 : 1;
-  const size_t esz = kind == SHB_DILATE_U8 ? 1 : 4;
-  auto too_large = [&](const std::string& need) {
-    set_error("shb_dilate_noalloc: " + std::to_string(width) + "x" + std::to_string(height) + " texels need " + need +
-              " bytes of scratch; the fixed array holds " + std::to_string(kNoAllocScratchBytes) +
-              " (about 153,000 texels of SH9, 3.3 M of float, 8.3 M of uint8)");
-    return SHB_ERR_INVALID_ARG;
-  };
-  // every texel needs at least one mask byte of scratch: bound n before the
-  // byte counts below are formed
-  if (n > (int64_t)kNoAllocScratchBytes) return too_large("more than " + std::to_string(n));
-  const size_t pbytes = esz * (size_t)n * ch;
-  const size_t pbytes_aligned = (pbytes + 255) & ~size_t(255);
-  const size_t need = kNoAllocFlagBytes + pbytes_aligned + (size_t)n;
-  if (passes > kNoAllocMaxPasses) {
-    set_error("shb_dilate_noalloc: at most " + std::to_string(kNoAllocMaxPasses) + " passes");
-    return SHB_ERR_INVALID_ARG;
-  }
-  if (need > kNoAllocScratchBytes) return too_large(std::to_string(need));
-  SHB_ON_DEVICE(ctx->device);
-  unsigned char* base = nullptr;
-  SHB_TRY(noalloc_scratch(ctx->device, &base));
-  int* changed = reinterpret_cast<int*>(base);
-  void* pbuf = base + kNoAllocFlagBytes;
-  uint8_t* mbuf = base + kNoAllocFlagBytes + pbytes_aligned;
-  cudaStream_t st = ctx->stream;
-  // the array keeps the previous call's contents: the change flags must start at zero
-  SHB_CUDA(cudaMemsetAsync(changed, 0, sizeof(int) * (size_t)passes, st));
-  void* bufs[2] = {pixels, pbuf};
-  uint8_t* masks[2] = {mask, mbuf};
-  const int64_t work = n * ch;
-  for (int p = 0; p < passes; ++p) {
-    int src = p & 1, dst = src ^ 1;
-    if (kind == SHB_DILATE_U8)
-      k_dilate<uint8_t><<<grid_for(work), kThreads, 0, st>>>((const uint8_t*)bufs[src], masks[src],
-                                                             (uint8_t*)bufs[dst], masks[dst], width, height, ch,
-                                                             changed, p);
-    else
-      k_dilate<float><<<grid_for(work), kThreads, 0, st>>>((const float*)bufs[src], masks[src], (float*)bufs[dst],
-                                                           masks[dst], width, height, ch, changed, p);
-    count_launch(ctx);
-  }
-  if (passes & 1) {
-    SHB_CUDA(cudaMemcpyAsync(pixels, bufs[1], pbytes, cudaMemcpyDeviceToDevice, st));
-    SHB_CUDA(cudaMemcpyAsync(mask, masks[1], (size_t)n, cudaMemcpyDeviceToDevice, st));
-  }
-  SHB_CUDA(cudaGetLastError());
-  return SHB_OK;
+  return ::shb::guarded("shb_dilate_noalloc", [&]() -> shb_status {
+    using namespace shb;
+    if (!ctx) {
+      set_error("ctx is NULL");
+      return SHB_ERR_INVALID_ARG;
+    }
+    if (kind < SHB_DILATE_SH9 || kind > SHB_DILATE_U8) {
+      set_error("bad dilate kind");
+      return SHB_ERR_INVALID_ARG;
+    }
+    if (width <= 0 || height <= 0 || passes <= 0) return SHB_OK;  // nothing to do, as Dilate<T>
+    if (!pixels || !mask) {
+      set_error("NULL argument");
+      return SHB_ERR_INVALID_ARG;
+    }
+    const int64_t n = (int64_t)width * height;  // width, height > 0 and < 2^31: no overflow
+    const int ch = kind == SHB_DILATE_SH9 ? 27 : 1;
+    const size_t esz = kind == SHB_DILATE_U8 ? 1 : 4;
+    auto too_large = [&](const std::string& need) {
+      set_error("shb_dilate_noalloc: " + std::to_string(width) + "x" + std::to_string(height) + " texels need " + need +
+                " bytes of scratch; the fixed array holds " + std::to_string(kNoAllocScratchBytes) +
+                " (about 153,000 texels of SH9, 3.3 M of float, 8.3 M of uint8)");
+      return SHB_ERR_INVALID_ARG;
+    };
+    // every texel needs at least one mask byte of scratch: bound n before the
+    // byte counts below are formed
+    if (n > (int64_t)kNoAllocScratchBytes) return too_large("more than " + std::to_string(n));
+    const size_t pbytes = esz * (size_t)n * ch;
+    const size_t pbytes_aligned = (pbytes + 255) & ~size_t(255);
+    const size_t need = kNoAllocFlagBytes + pbytes_aligned + (size_t)n;
+    if (passes > kNoAllocMaxPasses) {
+      set_error("shb_dilate_noalloc: at most " + std::to_string(kNoAllocMaxPasses) + " passes");
+      return SHB_ERR_INVALID_ARG;
+    }
+    if (need > kNoAllocScratchBytes) return too_large(std::to_string(need));
+    SHB_ON_DEVICE(ctx->device);
+    unsigned char* base = nullptr;
+    SHB_TRY(noalloc_scratch(ctx->device, &base));
+    int* changed = reinterpret_cast<int*>(base);
+    void* pbuf = base + kNoAllocFlagBytes;
+    uint8_t* mbuf = base + kNoAllocFlagBytes + pbytes_aligned;
+    cudaStream_t st = ctx->stream;
+    // the array keeps the previous call's contents: the change flags must start at zero
+    SHB_CUDA(cudaMemsetAsync(changed, 0, sizeof(int) * (size_t)passes, st));
+    void* bufs[2] = {pixels, pbuf};
+    uint8_t* masks[2] = {mask, mbuf};
+    const int64_t work = n * ch;
+    for (int p = 0; p < passes; ++p) {
+      int src = p & 1, dst = src ^ 1;
+      if (kind == SHB_DILATE_U8)
+        k_dilate<uint8_t><<<grid_for(work), kThreads, 0, st>>>((const uint8_t*)bufs[src], masks[src],
+                                                               (uint8_t*)bufs[dst], masks[dst], width, height, ch,
+                                                               changed, p);
+      else
+        k_dilate<float><<<grid_for(work), kThreads, 0, st>>>((const float*)bufs[src], masks[src], (float*)bufs[dst],
+                                                             masks[dst], width, height, ch, changed, p);
+      count_launch(ctx);
+    }
+    if (passes & 1) {
+      SHB_CUDA(cudaMemcpyAsync(pixels, bufs[1], pbytes, cudaMemcpyDeviceToDevice, st));
+      SHB_CUDA(cudaMemcpyAsync(mask, masks[1], (size_t)n, cudaMemcpyDeviceToDevice, st));
+    }
+    SHB_CUDA(cudaGetLastError());
+    return SHB_OK;
+  });
 }

@@ -5,7 +5,8 @@
 #include <stdint.h>
 
 #include <atomic>
-
+#include <exception>
+#include <new>
 #include <string>
 #include <utility>
 #include <vector>
@@ -20,6 +21,26 @@ namespace shb {
 
 void set_error(const std::string& msg);
 shb_status cuda_fail(cudaError_t e, const char* what);
+
+// Runs the body of a C ABI entry point so that no C++ exception leaves it:
+// a failed host allocation becomes SHB_ERR_OOM and any other exception
+// SHB_ERR_INTERNAL, with its message in shb_last_error().  A C, ctypes or
+// cgo caller cannot unwind a C++ exception.
+template <class F>
+shb_status guarded(const char* entry, F&& body) noexcept {
+  try {
+    return body();
+  } catch (const std::bad_alloc&) {
+    try { set_error(std::string(entry) + ": host allocation failed"); } catch (...) {}
+    return SHB_ERR_OOM;
+  } catch (const std::exception& e) {
+    try { set_error(std::string(entry) + ": " + e.what()); } catch (...) {}
+    return SHB_ERR_INTERNAL;
+  } catch (...) {
+    try { set_error(std::string(entry) + ": unknown exception"); } catch (...) {}
+    return SHB_ERR_INTERNAL;
+  }
+}
 
 #define SHB_CUDA(call)                                             \
   do {                                                             \

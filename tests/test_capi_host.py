@@ -161,3 +161,31 @@ def test_srgb_table_matches_oracle():
     got = api.srgb_to_linear_table()
     want = np.array([O.srgb_to_linear(i) for i in range(256)], np.float32)
     assert got.tobytes() == want.tobytes()
+
+
+def test_entry_point_guard_maps_exceptions(tmp_path):
+    """Every status-returning C ABI entry point runs its body in
+    shb::guarded: no C++ exception reaches a C, ctypes or cgo caller.
+    tests/cpp/guard_test.cpp checks the mapping (host compiler only)."""
+    cuda_inc = Path("/usr/local/cuda/include")
+    if not (cuda_inc / "cuda_runtime.h").exists():
+        pytest.skip("CUDA headers not found")
+    exe = tmp_path / "guard_test"
+    subprocess.run(["g++", "-std=c++17", "-O1", "-I", str(cuda_inc), "-I", str(ROOT / "sh_baker_b200" / "csrc"),
+                    str(ROOT / "tests" / "cpp" / "guard_test.cpp"), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    # and every definition of a status-returning entry point goes through it
+    csrc = ROOT / "sh_baker_b200" / "csrc"
+    defs = 0
+    for f in list(csrc.glob("*.cu")) + list(csrc.glob("*.cpp")):
+        lines = f.read_text().split("\n")
+        for i, line in enumerate(lines):
+            m = re.match(r'^(extern "C" )?(SHB_API )?shb_status (shb_\w+)\(', line)
+            if m:
+                j = i
+                while not lines[j].rstrip().endswith("{"):
+                    j += 1
+                assert f'guarded("{m.group(3)}"' in lines[j + 1], (f.name, m.group(3))
+                defs += 1
+    assert defs == 34, defs
