@@ -524,8 +524,14 @@ struct Rect {
   double w, h;
 };
 
-// Footprint of a chart of extent (w, h) units at `s` texels per unit.
-inline int foot(double e, double s) { return std::max(1, (int)std::ceil(e * s - 1e-9)); }
+// Footprint of a chart of extent (w, h) units at `s` texels per unit.  An
+// extent beyond 2^30 texels, or not a number, gets a footprint of 2^30,
+// which no page holds, so packing fails instead of casting out of int range.
+inline int foot(double e, double s) {
+  const double f = std::ceil(e * s - 1e-9);
+  if (f != f || f >= 1073741824.0) return 1073741824;
+  return f < 1.0 ? 1 : (int)f;
+}
 
 bool pack(std::vector<Rect>& rects, double s, int W, int H, int pad, std::vector<std::array<int, 3>>* place) {
   std::vector<uint32_t> order(rects.size());
@@ -611,11 +617,7 @@ shb_status shb_create_atlas(const shb_scene_desc* scene, uint32_t target_resolut
       auto work = [&] {
         for (uint32_t g; (g = next.fetch_add(1)) < ng;) build_charts(scene->geometries[g], scales[g], gc[g]);
       };
-      const unsigned nt = std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), ng));
-      std::vector<std::thread> pool;
-      for (unsigned t = 1; t < nt; ++t) pool.emplace_back(work);
-      work();
-      for (auto& t : pool) t.join();
+      ::shb::run_host_threads(std::max(1u, std::min<unsigned>(std::thread::hardware_concurrency(), ng)), work);
     }
     std::vector<Rect> rects;
     double sum_area = 0;

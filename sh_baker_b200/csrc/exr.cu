@@ -212,10 +212,7 @@ shb_status write_exr(shb_context* c, const float* d_sh, const float* d_env, int 
       data[k] = std::move(z);
     }
   };
-  const int nt = std::max(1, std::min<int>(chunks, (int)std::thread::hardware_concurrency()));
-  std::vector<std::thread> th;
-  for (int i = 0; i < nt; ++i) th.emplace_back(worker);
-  for (auto& x : th) x.join();
+  run_host_threads((unsigned)std::max(1, std::min<int>(chunks, (int)std::thread::hardware_concurrency())), worker);
   if (failed) {
     set_error("zlib compression failed");
     return SHB_ERR_INTERNAL;

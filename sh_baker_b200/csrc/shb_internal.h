@@ -6,8 +6,10 @@
 
 #include <atomic>
 #include <exception>
+#include <mutex>
 #include <new>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -40,6 +42,36 @@ shb_status guarded(const char* entry, F&& body) noexcept {
     try { set_error(std::string(entry) + ": unknown exception"); } catch (...) {}
     return SHB_ERR_INTERNAL;
   }
+}
+
+// Runs `work` on up to `threads` host threads, the calling one included,
+// and joins them.  `work` must claim its items from a shared counter, so
+// that any number of threads finishes them.  A std::thread that ends with
+// an exception, or is destroyed unjoined, terminates the process, so an
+// exception of any thread is kept and rethrown here once all have joined
+// (for guarded to map), and a thread that cannot be started is skipped.
+template <class F>
+void run_host_threads(unsigned threads, F&& work) {
+  std::mutex m;
+  std::exception_ptr first;
+  auto body = [&] {
+    try {
+      work();
+    } catch (...) {
+      std::lock_guard<std::mutex> lock(m);
+      if (!first) first = std::current_exception();
+    }
+  };
+  std::vector<std::thread> pool;
+  try {
+    pool.reserve(threads > 1 ? threads - 1 : 0);
+    for (unsigned t = 1; t < threads; ++t) pool.emplace_back(body);
+  } catch (...) {
+    // fewer threads: those started, and this one, claim every item
+  }
+  body();
+  for (auto& t : pool) t.join();
+  if (first) std::rethrow_exception(first);
 }
 
 #define SHB_CUDA(call)                                             \

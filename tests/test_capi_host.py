@@ -171,7 +171,7 @@ def test_entry_point_guard_maps_exceptions(tmp_path):
     if not (cuda_inc / "cuda_runtime.h").exists():
         pytest.skip("CUDA headers not found")
     exe = tmp_path / "guard_test"
-    subprocess.run(["g++", "-std=c++17", "-O1", "-I", str(cuda_inc), "-I", str(ROOT / "sh_baker_b200" / "csrc"),
+    subprocess.run(["g++", "-std=c++17", "-O1", "-pthread", "-I", str(cuda_inc), "-I", str(ROOT / "sh_baker_b200" / "csrc"),
                     str(ROOT / "tests" / "cpp" / "guard_test.cpp"), "-o", str(exe)], check=True)
     r = subprocess.run([str(exe)], capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
