@@ -365,8 +365,14 @@ bool read_exr_header(const std::string& path, ExrFile& e, std::string& err) {
     err = "bad OpenEXR header: " + path;
     return false;
   }
-  e.W = x1 - x0 + 1;
-  e.H = y1 - y0 + 1;
+  // in 64 bits: the window's corners are arbitrary int32 values
+  const int64_t W = (int64_t)x1 - x0 + 1, H = (int64_t)y1 - y0 + 1;
+  if (W > 2147483647 || H > 2147483647 || W * H > 2147483647) {
+    err = "OpenEXR image larger than 2^31 - 1 pixels: " + path;
+    return false;
+  }
+  e.W = (int)W;
+  e.H = (int)H;
   e.chunk_table = i + 1;
   if (e.comp != 0 && e.comp != 2 && e.comp != 3) {
     err = "unsupported OpenEXR compression (NONE, ZIPS and ZIP are read)";
@@ -398,7 +404,7 @@ bool read_exr_channels(ExrFile& e, const std::vector<int>& want, float* out, std
   for (int k = 0; k < chunks; ++k) {
     uint64_t pos;
     std::memcpy(&pos, &b[e.chunk_table + 8ull * k], 8);
-    if (pos + 8 > b.size()) {
+    if (pos > b.size() || b.size() - pos < 8) {  // (pos + 8 can wrap)
       err = "bad OpenEXR chunk offset";
       return false;
     }
@@ -408,11 +414,14 @@ bool read_exr_channels(ExrFile& e, const std::vector<int>& want, float* out, std
     const int ly = k * lpc;
     const int lines = std::min(lpc, e.H - ly);
     const size_t n = line_bytes * lines;
-    if (size < 0 || pos + 8 + (uint64_t)size > b.size()) {
+    // a zlib stream inflates by at most about 1032:1, so a chunk of `size`
+    // bytes cannot hold more: refuse before allocating its lines
+    if (size < 0 || pos + 8 + (uint64_t)size > b.size() ||
+        (e.comp == 0 ? (size_t)size != n : n > 1100 * (uint64_t)size + 1024)) {
       err = "bad OpenEXR chunk size";
       return false;
     }
-    const uint8_t* d = &b[pos + 8];
+    const uint8_t* d = b.data() + pos + 8;
     raw.resize(n);
     if (e.comp == 0 || (size_t)size == n) {
       if ((size_t)size != n) {

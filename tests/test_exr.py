@@ -9,6 +9,7 @@ is what that path stores.
 GPU: the CUDA writer's files carry the same attributes, channel names and
 order, and bit-identical half samples as the fixture.
 """
+import ctypes as C
 import tempfile
 from pathlib import Path
 
@@ -124,3 +125,63 @@ def test_save_rejects_bad_arguments(gpu_ctx, tmp_path):
     assert lib.shb_save_sh_lightmap(h, sh.ctypes.data, None, 0, 1, 0, str(tmp_path / "a.exr").encode(), 0) == 1
     assert lib.shb_save_sh_lightmap(h, sh.ctypes.data, None, 1, 1, 0, str(tmp_path / "b.exr").encode(), 7) == 1
     assert lib.shb_save_sh_lightmap(h, sh.ctypes.data, None, 1, 1, 0, str(tmp_path / "no" / "c.exr").encode(), 0) != 0
+
+
+def _exr(window, rows, comp=0, offsets=None):
+    """A minimal single-part scanline OpenEXR file with one FLOAT channel R:
+    `rows` is a list of (y, payload bytes) chunks, `window` the dataWindow
+    (x0, y0, x1, y1); `offsets` overrides the offset table."""
+    import struct
+
+    def attr(name, typ, data):
+        return name.encode() + b"\0" + typ.encode() + b"\0" + struct.pack("<i", len(data)) + data
+
+    chlist = b"R\0" + struct.pack("<iB3xii", 2, 0, 1, 1) + b"\0"
+    head = b"\x76\x2f\x31\x01\x02\x00\x00\x00" + attr("channels", "chlist", chlist) + \
+        attr("compression", "compression", bytes([comp])) + attr("dataWindow", "box2i", struct.pack("<4i", *window)) + b"\0"
+    pos = len(head) + 8 * len(rows)
+    table, body = [], b""
+    for y, payload in rows:
+        table.append(pos + len(body))
+        body += struct.pack("<ii", y, len(payload)) + payload
+    table = offsets if offsets is not None else table
+    return head + b"".join(struct.pack("<Q", t) for t in table) + body
+
+
+def _load(path):
+    from sh_baker_b200 import _capi as A
+    lib = A.load()
+    names = (C.c_char_p * 1)(b"R")
+    w, h = C.c_int32(), C.c_int32()
+    st = lib.shb_exr_load_channels(str(path).encode(), C.cast(names, C.c_void_p), 1, C.byref(w), C.byref(h), None)
+    if st != 0:
+        return st, lib.shb_last_error().decode(), None
+    out = np.zeros(w.value * h.value, np.float32)
+    st = lib.shb_exr_load_channels(str(path).encode(), C.cast(names, C.c_void_p), 1, C.byref(w), C.byref(h),
+                                   out.ctypes.data)
+    return st, lib.shb_last_error().decode(), out.reshape(h.value, w.value)
+
+
+def test_reader_rejects_damaged_files(tmp_path):
+    """shb_exr_load_channels (host code, no GPU) on crafted files: a good
+    one reads back; a dataWindow whose width overflows int32, an offset
+    table entry near 2^64 (offset + 8 wraps) and a ZIP chunk too small to
+    inflate to its lines are SHB_ERR_INVALID_ARG, refused before any read
+    or allocation they would drive."""
+    vals = np.arange(6, dtype=np.float32).reshape(2, 3) + 0.5
+    p = tmp_path / "good.exr"
+    p.write_bytes(_exr((0, 0, 2, 1), [(0, vals[0].tobytes()), (1, vals[1].tobytes())]))
+    st, msg, got = _load(p)
+    assert st == 0, msg
+    np.testing.assert_array_equal(got, vals)
+    cases = {
+        "wide": (_exr((-2 ** 31, 0, 39, 0), [(0, b"")]), "larger than 2^31 - 1"),
+        "offset": (_exr((0, 0, 2, 1), [(0, vals[0].tobytes()), (1, vals[1].tobytes())],
+                        offsets=[2 ** 64 - 7, 2 ** 64 - 7]), "chunk offset"),
+        "inflate": (_exr((0, 0, 99999, 15), [(0, b"\x78\x9c" + bytes(8))], comp=3), "chunk size"),
+    }
+    for name, (data, what) in cases.items():
+        q = tmp_path / f"{name}.exr"
+        q.write_bytes(data)
+        st, msg, _ = _load(q)
+        assert st == 1 and what in msg, (name, st, msg)
