@@ -13,6 +13,8 @@
 #include <sys/stat.h>
 
 #include <chrono>
+#include <cerrno>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -94,8 +96,10 @@ bool parse(int argc, char** argv, Flags& f) {
       continue;
     }
     if (ints.count(name)) {
+      errno = 0;
       long v = std::strtol(value.c_str(), &end, 10);
-      if (value.empty() || *end) {
+      // an int32 flag, as gflags parses it: no wrap-around of larger values
+      if (value.empty() || *end || errno == ERANGE || v < INT32_MIN || v > INT32_MAX) {
         std::fprintf(stderr, "bad value for --%s: %s\n", name.c_str(), value.c_str());
         return false;
       }

@@ -31,6 +31,10 @@ def test_usage_and_flag_errors(tmp_path):
     assert r.returncode == 1 and "Usage" in r.stderr
     assert run("--no_such_flag=1").returncode == 1
     assert run("--width", "abc", "--input", "x").returncode == 1
+    # int32 flags, as gflags parses them: values beyond int32 are errors, not wrapped
+    for v in ("4294967297", "-2147483649", "99999999999999999999"):
+        r = run(f"--width={v}", "--input", "x")
+        assert r.returncode == 1 and "bad value for --width" in r.stderr, v
     r = run("--input", tmp_path / "missing.gltf")
     assert r.returncode == 1 and "does not exist" in r.stderr
 
