@@ -23,7 +23,9 @@
  * its previous current device back before they return.
  * Image arguments hold at most 2^31 - 1 texels (the G-buffer limit of
  * shb_rasterize) and shb_find_occlusion takes at most 2^31 - 1 rays per
- * call; larger sizes are SHB_ERR_INVALID_ARG.
+ * call; larger sizes are SHB_ERR_INVALID_ARG.  A scene holds at most
+ * 2^30 - 1 vertices, 2^30 - 1 triangles and 2^26 - 1 geometries, an albedo
+ * texture at most 2^31 - 1 bytes and all of a scene's at most 2^32 - 1.
  *
  * Memory layouts are binary compatible with the reference's Eigen structs:
  *   shb_surface_point == sh_baker::SurfacePoint (64 bytes, Vector4f 16-byte

@@ -447,11 +447,26 @@ uint64_t shb_context_kernel_launches(const shb_context* ctx) { return ctx ? ctx-
 
 shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene** out) {
   return ::shb::guarded("shb_scene_upload", [&]() -> shb_status {
-    if (!ctx || !d || !out) return bad("NULL argument");
+    if (!d || !out) return bad("NULL argument");
     *out = nullptr;
     if (d->geometry_count && !d->geometries) return bad("geometries is NULL");
     if (d->material_count && !d->materials) return bad("materials is NULL");
     if (d->light_count && !d->lights) return bad("lights is NULL");
+    // The kernels index per-vertex arrays as up to 4 * vertex id, per-triangle
+    // arrays as 3 * triangle id and the transforms as 12 * geometry id, all
+    // in 32-bit arithmetic: these limits keep every such index in range.
+    // (Checked from the counts alone, before the context.)
+    static const char* kTooBig =
+        "scene too large: at most 2^30 - 1 vertices, 2^30 - 1 triangles and 2^26 - 1 geometries";
+    if (d->geometry_count >= (1u << 26)) return bad(kTooBig);
+    uint64_t nv_total = 0, nt_total = 0;
+    for (uint32_t g = 0; g < d->geometry_count; ++g) {
+      const shb_geometry_desc& gd = d->geometries[g];
+      nv_total += gd.vertex_count;
+      nt_total += gd.index_count / 3;
+    }
+    if (nv_total >= (1ull << 30) || nt_total >= (1ull << 30)) return bad(kTooBig);
+    if (!ctx) return bad("NULL argument");
     SHB_ON_DEVICE(ctx->device);
     cudaStream_t st = ctx->stream;
     std::vector<float> ov, on, tuv, luv, ot, lin, rot;
@@ -459,13 +474,6 @@ shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene
     std::vector<DGeom> geoms;
     bool raster_ready = true;
     std::string raster_error;
-    uint64_t nv_total = 0, nt_total = 0;
-    for (uint32_t g = 0; g < d->geometry_count; ++g) {
-      const shb_geometry_desc& gd = d->geometries[g];
-      nv_total += gd.vertex_count;
-      nt_total += gd.index_count / 3;
-    }
-    if (nv_total >= 0xFFFFFFF0ull || nt_total >= 0x7FFFFFF0ull) return bad("scene too large for 32-bit ids");
     ov.reserve(3 * nv_total);
     on.assign(3 * nv_total, 0.f);
     tuv.assign(2 * nv_total, 0.f);
@@ -533,11 +541,16 @@ shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene
       if (md.albedo_pixels && md.albedo_width && md.albedo_height && md.albedo_channels) {
         if (md.albedo_channels != 3 && md.albedo_channels != 4)
           return bad("material " + std::to_string(m) + ": albedo_channels must be 3 or 4");
+        // a texel's byte offset is a 32-bit int inside its texture
+        // (tex_index) and a 32-bit offset among all textures (pix_offset)
+        const uint64_t n = (uint64_t)md.albedo_width * md.albedo_height * md.albedo_channels;
+        if (n > 0x7FFFFFFFull || pix.size() + n > 0xFFFFFFFFull)
+          return bad("material " + std::to_string(m) +
+                     ": albedo texture above 2^31 - 1 bytes, or all textures above 2^32 - 1 bytes");
         M.pix_offset = (uint32_t)pix.size();
         M.w = md.albedo_width;
         M.h = md.albedo_height;
         M.c = md.albedo_channels;
-        size_t n = (size_t)M.w * M.h * M.c;
         pix.insert(pix.end(), md.albedo_pixels, md.albedo_pixels + n);
         if (M.c == 4) has_alpha = 1;
       }

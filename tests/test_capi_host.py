@@ -86,6 +86,34 @@ def test_oversized_arguments_are_rejected_before_any_device_work(lib):
     assert "NULL" in err(lib.shb_find_occlusion(None, None, 2**31 - 1, None, 0))
 
 
+def test_scene_limits_are_checked_from_the_counts(lib):
+    """Scenes whose 32-bit device indices could wrap (4 * vertex id,
+    3 * triangle id) are refused from the descriptor's counts alone, before
+    any data is read or the context is used: at most 2^30 - 1 vertices and
+    2^30 - 1 triangles."""
+    out = C.c_void_p()
+
+    def upload(geoms):
+        arr = (A.GeometryDesc * len(geoms))(*geoms)
+        d = A.SceneDesc()
+        d.geometries = C.cast(arr, C.POINTER(A.GeometryDesc))
+        d.geometry_count = len(geoms)
+        st = lib.shb_scene_upload(None, C.byref(d), C.byref(out))
+        return st, lib.shb_last_error().decode()
+
+    def geo(nv, ni):
+        g = A.GeometryDesc()
+        g.vertex_count, g.index_count = nv, ni
+        return g
+
+    st, msg = upload([geo(2 ** 29, 0), geo(2 ** 29, 0)])  # 2^30 vertices in total
+    assert st == 1 and "scene too large" in msg, msg
+    st, msg = upload([geo(3, 3 * 2 ** 29), geo(3, 3 * 2 ** 29)])  # 2^30 triangles
+    assert st == 1 and "scene too large" in msg, msg
+    st, msg = upload([geo(2 ** 30 - 1, 0)])  # at the limit: only the missing context is refused
+    assert st == 1 and msg == "NULL argument", msg
+
+
 def test_struct_layouts_match_header(tmp_path):
     """Compiles a probe against include/shb.h and compares sizes/offsets
     with the ctypes mirror."""
