@@ -2,6 +2,7 @@
 // upload and validation, and dispatch of every entry point to its kernels.
 #include <cmath>
 #include <cstring>
+#include <memory>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -378,14 +379,14 @@ shb_status shb_context_create(const shb_options* options, shb_context** out) {
                 std::to_string(prop.minor));
       return SHB_ERR_NO_DEVICE;
     }
-    auto* c = new shb_context();
+    // owned here until it is handed out, so that no path (an exception
+    // included) leaks it
+    std::unique_ptr<shb_context> owner(new shb_context());
+    shb_context* c = owner.get();
     c->device = dev;
     c->profiling = options ? options->profiling : 0;
     e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess) {
-      delete c;
-      return cuda_fail(e, "cudaStreamCreate");
-    }
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
     c->stream = c->own_stream;
     float tab[256];
     srgb_table(tab);
@@ -393,7 +394,6 @@ shb_status shb_context_create(const shb_options* options, shb_context** out) {
     e = cudaGetLastError();
     if (e != cudaSuccess) {
       cudaStreamDestroy(c->own_stream);
-      delete c;
       return cuda_fail(e, "sRGB table upload");
     }
     // shb_dilate_noalloc's fixed array: its address is resolved here, so that
@@ -401,14 +401,13 @@ shb_status shb_context_create(const shb_options* options, shb_context** out) {
     shb_status ns = noalloc_prepare(dev);
     if (ns != SHB_OK) {
       cudaStreamDestroy(c->own_stream);
-      delete c;
       return ns;
     }
     {
       std::lock_guard<std::mutex> lk(g_cache_mu);
       ++g_contexts;
     }
-    *out = c;
+    *out = owner.release();
     return SHB_OK;
   });
 }
@@ -591,7 +590,8 @@ shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene
       }
       lights.push_back(L);
     }
-    auto* s = new shb_scene();
+    std::unique_ptr<shb_scene> owner(new shb_scene());  // owned here until handed out
+    shb_scene* s = owner.get();
     s->ctx = ctx;
     s->vertex_count = vbase;
     s->prim_count = pbase;
@@ -653,12 +653,9 @@ shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene
       cudaError_t e = cudaStreamSynchronize(st);
       if (e != cudaSuccess) rc = cuda_fail(e, "scene upload");
     }
-    if (rc != SHB_OK) {
-      delete s;
-      return rc;
-    }
+    if (rc != SHB_OK) return rc;
     ctx_retain(s->ctx);
-    *out = s;
+    *out = owner.release();
     return SHB_OK;
   });
 }
@@ -726,14 +723,12 @@ shb_status shb_rasterize(shb_scene* s, const shb_raster_config* cfg, shb_surface
   return ::shb::guarded("shb_rasterize", [&]() -> shb_status {
     if (!s || !cfg) return bad("NULL argument");
     if (out_gbuffer) *out_gbuffer = nullptr;
-    auto* g = new shb_gbuffer();
+    std::unique_ptr<shb_gbuffer> owner(new shb_gbuffer());  // owned here until handed out
+    shb_gbuffer* g = owner.get();
     shb_status rc = rasterize_into(s, cfg, g, host_out);
-    if (rc != SHB_OK || !out_gbuffer) {
-      delete g;
-      return rc;
-    }
+    if (rc != SHB_OK || !out_gbuffer) return rc;
     ctx_retain(g->ctx);
-    *out_gbuffer = g;
+    *out_gbuffer = owner.release();
     return SHB_OK;
   });
 }
@@ -745,7 +740,8 @@ shb_status shb_gbuffer_upload(shb_context* ctx, const shb_surface_point* points,
     if (too_many_texels(width, height)) return bad(kTooLarge);
     if (!ctx || !points || !out) return bad("NULL argument");
     SHB_ON_DEVICE(ctx->device);
-    auto* g = new shb_gbuffer();
+    std::unique_ptr<shb_gbuffer> owner(new shb_gbuffer());  // owned here until handed out
+    shb_gbuffer* g = owner.get();
     g->ctx = ctx;
     g->width = width;
     g->height = height;
@@ -756,12 +752,9 @@ shb_status shb_gbuffer_upload(shb_context* ctx, const shb_surface_point* points,
       if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
       if (e != cudaSuccess) rc = cuda_fail(e, "G-buffer upload");
     }
-    if (rc != SHB_OK) {
-      delete g;
-      return rc;
-    }
+    if (rc != SHB_OK) return rc;
     ctx_retain(g->ctx);
-    *out = g;
+    *out = owner.release();
     return SHB_OK;
   });
 }
