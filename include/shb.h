@@ -487,7 +487,7 @@ SHB_API shb_status shb_write_png(const char* path, int32_t width, int32_t height
  * shb_scene_desc (valid until shb_host_scene_destroy) feeds
  * shb_scene_upload.  Missing material / POSITION / NORMAL / TEXCOORD_0 on a
  * primitive, an unreadable file or an unsupported texture (neither PNG nor
- * sequential JPEG) are SHB_ERR_INVALID_ARG (the reference returns nullopt).
+ * Huffman-coded JPEG) are SHB_ERR_INVALID_ARG (the reference returns nullopt).
  * Emissive primitives become area lights; TEXCOORD_1 becomes the lightmap
  * UVs; a primitive without TANGENT gets tangents by the MikkTSpace method,
  * as the reference generates them (src/loader.cpp:363-385). */

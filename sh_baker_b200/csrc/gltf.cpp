@@ -21,10 +21,9 @@
 //     (:541-560), cone angles become cosines (:587-598).
 // Tangents missing from the file are built by the MikkTSpace method
 // (tspace.cpp), as the reference builds them with that library.
-// Differences: JPEG textures
-// are decoded by jpeg.cpp (sequential files only; progressive ones are
-// rejected).  The sky environment (:705-797) is not read: the bake never
-// samples it.
+// Differences: JPEG textures are decoded by jpeg.cpp (Huffman-coded
+// sequential and progressive files) instead of stb_image.  The sky
+// environment (:705-797) is not read: the bake never samples it.
 #include <zlib.h>
 
 #include "tspace.h"

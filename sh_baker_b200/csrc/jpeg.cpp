@@ -1,7 +1,7 @@
 // jpeg.cpp - JPEG base-colour textures for the glTF loader.  The reference
 // loads every image through stb_image (src/loader.cpp:687-704, tinygltf's
-// image callback); this is an own decoder of sequential Huffman-coded JPEG
-// (ITU-T T.81 baseline and extended 8-bit, SOF0 / SOF1) with restart
+// image callback); this is an own decoder of Huffman-coded JPEG (ITU-T
+// T.81 baseline, extended 8-bit and progressive, SOF0 / SOF1 / SOF2) with restart
 // intervals, 1 or 3 components and any sampling factors up to 4x4:
 //   - Huffman tables as canonical codes (T.81 annex C), DC prediction per
 //     component, AC run/size symbols with EOB and ZRL (annex F.2.2);
@@ -14,7 +14,10 @@
 // Output is 8-bit RGB, grey replicated, which is what stb_image returns for
 // three requested channels.  Pixel values can differ from libjpeg's or
 // stb_image's by a level or two: those use integer inverse DCTs.
-// Progressive (SOF2), lossless and arithmetic-coded files are rejected.
+// Progressive files (SOF2, annex G: spectral selection and successive
+// approximation, DC and AC first and refinement scans, end-of-band runs)
+// keep every block's coefficients across scans and are transformed once
+// all scans are read.  Lossless and arithmetic-coded files are rejected.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -41,6 +44,7 @@ struct Comp {
   int id = 0, h = 1, v = 1, tq = 0, td = 0, ta = 0;
   int bw = 0, bh = 0;  // blocks per line / column, padded to whole MCUs
   std::vector<uint8_t> px;  // bw*8 x bh*8 samples
+  std::vector<int> coef;    // progressive: 64 coefficients per block, zigzag order
   int pred = 0;
 };
 
@@ -171,7 +175,7 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
   Huff dc[4], ac[4];
   std::vector<Comp> comps;
   int width = 0, height = 0, hmax = 1, vmax = 1, restart = 0;
-  bool frame = false, scanned = false;
+  bool frame = false, scanned = false, progressive = false;
   size_t i = 2;
   auto u16 = [&](size_t k) { return (int)f[k] << 8 | f[k + 1]; };
   while (i + 4 <= f.size()) {
@@ -192,7 +196,7 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
     }
     const size_t s = i + 4, e = i + 2 + len;
     // the fixed part each segment reads before its own checks
-    const size_t need = mk == 0xC0 || mk == 0xC1 ? 6 : (mk == 0xDD ? 2 : (mk == 0xDA ? 1 : 0));
+    const size_t need = mk == 0xC0 || mk == 0xC1 || mk == 0xC2 ? 6 : (mk == 0xDD ? 2 : (mk == 0xDA ? 1 : 0));
     if (s + need > e) {
       err = "JPEG: truncated segment";
       return false;
@@ -238,7 +242,12 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
         h.set = true;
         k += 17 + (size_t)total;
       }
-    } else if (mk == 0xC0 || mk == 0xC1) {  // SOF0 / SOF1
+    } else if (mk == 0xC0 || mk == 0xC1 || mk == 0xC2) {  // SOF0 / SOF1 / SOF2
+      if (frame) {
+        err = "JPEG: more than one frame";
+        return false;
+      }
+      progressive = mk == 0xC2;
       if (f[s] != 8) {
         err = "JPEG: only 8-bit samples are supported";
         return false;
@@ -248,6 +257,11 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
       const int nc = f[s + 5];
       if ((nc != 1 && nc != 3) || width <= 0 || height <= 0 || s + 6 + 3 * (size_t)nc > e) {
         err = "JPEG: unsupported frame (1 or 3 components, nonzero size)";
+        return false;
+      }
+      // the frame header alone sizes the sample (and coefficient) planes
+      if ((int64_t)width * height > (1 << 28)) {
+        err = "JPEG: images above 2^28 pixels are not read";
         return false;
       }
       comps.resize((size_t)nc);
@@ -269,10 +283,11 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
         cp.bw = mcux * cp.h;
         cp.bh = mcuy * cp.v;
         cp.px.assign((size_t)cp.bw * 8 * cp.bh * 8, 0);
+        if (progressive) cp.coef.assign((size_t)cp.bw * cp.bh * 64, 0);
       }
       frame = true;
     } else if (mk >= 0xC2 && mk <= 0xCF && mk != 0xC4 && mk != 0xC8 && mk != 0xCC) {
-      err = "JPEG: only sequential Huffman-coded (baseline / extended) files are supported";
+      err = "JPEG: only Huffman-coded sequential and progressive 8-bit files are supported";
       return false;
     } else if (mk == 0xDD) {  // DRI
       restart = u16(s);
@@ -286,13 +301,24 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
         err = "JPEG: bad scan header";
         return false;
       }
+      // spectral selection and successive approximation (T.81 B.2.3): fixed
+      // at 0, 63, 0, 0 in sequential files
+      const size_t ps = s + 1 + 2 * (size_t)ns;
+      const int Ss = f[ps], Se = f[ps + 1], Ah = f[ps + 2] >> 4, Al = f[ps + 2] & 15;
+      if (progressive && (Ah > 13 || Al > 13 || (Ss == 0 ? Se != 0 : (Se < Ss || Se > 63 || ns != 1)))) {
+        err = "JPEG: bad progressive scan parameters";
+        return false;
+      }
+      // tables a scan decodes with: sequential DC and AC; a progressive DC
+      // first scan DC, an AC scan AC, a DC refinement none
+      const bool need_dc = !progressive || (Ss == 0 && Ah == 0), need_ac = !progressive || Ss > 0;
       std::vector<Comp*> sc;
       for (int c = 0; c < ns; ++c) {
         const int id = f[s + 1 + 2 * c], t = f[s + 2 + 2 * c];
         Comp* cp = nullptr;
         for (Comp& x : comps)
           if (x.id == id) cp = &x;
-        if (!cp || !dc[t >> 4 & 3].set || !ac[t & 3].set || !qset[cp->tq]) {
+        if (!cp || (need_dc && !dc[t >> 4 & 3].set) || (need_ac && !ac[t & 3].set) || !qset[cp->tq]) {
           err = "JPEG: scan names a missing component or table";
           return false;
         }
@@ -330,6 +356,93 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
         idct8x8(coef, q[cp.tq], &cp.px[((size_t)by * 8) * cp.bw * 8 + (size_t)bx * 8], cp.bw * 8);
         return true;
       };
+      // Progressive scans (T.81 annex G.1.2) add to the block's stored
+      // coefficients; the inverse DCT runs once all scans are read.
+      int eobrun = 0;  // blocks left in the current end-of-band run
+      auto prog_block = [&](Comp& cp, int bx, int by) -> bool {
+        int* z = &cp.coef[((size_t)by * cp.bw + bx) * 64];
+        if (Ss == 0) {  // DC: first scan (difference, shifted by Al) or one refinement bit
+          if (Ah == 0) {
+            const int t = decode_huff(r, dc[cp.td]);
+            if (t < 0 || t > 11) return false;
+            cp.pred += extend(r.receive(t), t);
+            z[0] = cp.pred * (1 << Al);
+          } else if (r.bit()) {
+            z[0] |= 1 << Al;
+          }
+          return true;
+        }
+        if (Ah == 0) {  // AC first scan: run/size symbols, end-of-band runs
+          if (eobrun > 0) {
+            --eobrun;
+            return true;
+          }
+          for (int k = Ss; k <= Se; ++k) {
+            const int rs = decode_huff(r, ac[cp.ta]);
+            if (rs < 0) return false;
+            const int run = rs >> 4, sz = rs & 15;
+            if (sz == 0) {
+              if (run < 15) {  // EOB run of 2^run + extra bits blocks, this one included
+                eobrun = (1 << run) - 1 + (run ? r.receive(run) : 0);
+                break;
+              }
+              k += 15;  // ZRL: sixteen zeros
+              continue;
+            }
+            k += run;
+            if (k > Se) return false;
+            z[k] = extend(r.receive(sz), sz) * (1 << Al);
+          }
+          return true;
+        }
+        // AC refinement (G.1.2.3): one correction bit for every coefficient
+        // already nonzero, new coefficients of magnitude 2^Al placed after
+        // `run` coefficients that are still zero
+        const int p1 = 1 << Al, m1 = -p1;
+        auto correct = [&](int& c) {
+          if (r.bit() && (c & p1) == 0) c += c >= 0 ? p1 : m1;
+        };
+        int k = Ss;
+        if (eobrun == 0) {
+          for (; k <= Se; ++k) {
+            const int rs = decode_huff(r, ac[cp.ta]);
+            if (rs < 0) return false;
+            int run = rs >> 4;
+            const int sz = rs & 15;
+            int value = 0;
+            if (sz == 0) {
+              if (run < 15) {  // EOB run, this block included: its rest is refined below
+                eobrun = (1 << run) + (run ? r.receive(run) : 0);
+                break;
+              }  // else ZRL: pass sixteen zero coefficients
+            } else {
+              if (sz != 1) return false;
+              value = r.bit() ? p1 : m1;
+            }
+            while (k <= Se) {
+              int& c = z[k];
+              if (c != 0) {
+                correct(c);
+              } else {
+                if (run == 0) {
+                  if (value) c = value;
+                  break;
+                }
+                --run;
+              }
+              ++k;
+            }
+            if (k > Se && value) return false;  // no zero coefficient left for the new one
+          }
+        }
+        if (eobrun > 0) {
+          for (; k <= Se; ++k)
+            if (z[k] != 0) correct(z[k]);
+          --eobrun;
+        }
+        return true;
+      };
+      auto unit = [&](Comp& cp, int bx, int by) { return progressive ? prog_block(cp, bx, by) : block(cp, bx, by); };
       int todo = restart;
       for (int my = 0; my < mcuy; ++my)
         for (int mx = 0; mx < mcux; ++mx) {
@@ -338,15 +451,16 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
             while (r.i + 1 < f.size() && !(f[r.i] == 0xFF && f[r.i + 1] >= 0xD0 && f[r.i + 1] <= 0xD7)) r.i++;
             r.i += 2;
             for (Comp* cp : sc) cp->pred = 0;
+            eobrun = 0;
             todo = restart;
           }
           bool ok = true;
           if (single) {
-            ok = block(*sc[0], mx, my);
+            ok = unit(*sc[0], mx, my);
           } else {
             for (Comp* cp : sc)
               for (int v = 0; v < cp->v && ok; ++v)
-                for (int h = 0; h < cp->h && ok; ++h) ok = block(*cp, mx * cp->h + h, my * cp->v + v);
+                for (int h = 0; h < cp->h && ok; ++h) ok = unit(*cp, mx * cp->h + h, my * cp->v + v);
           }
           if (!ok) {
             err = "JPEG: damaged entropy-coded data";
@@ -366,6 +480,12 @@ bool decode_jpeg(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint3
     err = "JPEG: no image data";
     return false;
   }
+  if (progressive)
+    for (Comp& cp : comps)
+      for (int by = 0; by < cp.bh; ++by)
+        for (int bx = 0; bx < cp.bw; ++bx)
+          idct8x8(&cp.coef[((size_t)by * cp.bw + bx) * 64], q[cp.tq],
+                  &cp.px[((size_t)by * 8) * cp.bw * 8 + (size_t)bx * 8], cp.bw * 8);
   W = (uint32_t)width;
   H = (uint32_t)height;
   C = 3;

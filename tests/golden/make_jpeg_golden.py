@@ -5,6 +5,9 @@ own JPEG decoder (sh_baker_b200/csrc/jpeg.cpp) is checked against these.
 Cases: 4:4:4, 4:2:2 and 4:2:0 chroma sampling at quality 90, 4:2:0 at
 quality 50, 4:2:0 with a restart marker every 3 MCUs, a greyscale file,
 and odd sizes (37 x 53, 1 x 1, 17 x 9) so that partial MCUs are cut.
+Progressive twins (`prog_<case>`): the same image and settings written as a
+progressive file (spectral selection and successive approximation scans),
+whose quantised coefficients equal its sequential twin's.
 
     python tests/golden/make_jpeg_golden.py
 """
@@ -34,6 +37,7 @@ CASES = {
     "tiny": (1, 1, dict(subsampling=2, quality=90)),
     "odd": (9, 17, dict(subsampling=1, quality=75)),
 }
+PROGRESSIVE = ["s444_q90", "s422_q90", "s420_q90", "s420_restart", "grey", "odd"]
 
 
 def main():
@@ -48,9 +52,19 @@ def main():
         data = b.getvalue()
         out[f"{name}_jpeg"] = np.frombuffer(data, np.uint8)
         out[f"{name}_rgb"] = np.array(Image.open(io.BytesIO(data)).convert("RGB"))
+        if name in PROGRESSIVE:
+            b = io.BytesIO()
+            if kw is None:
+                Image.fromarray(img[..., 0]).save(b, "JPEG", quality=90, progressive=True)
+            else:
+                Image.fromarray(img).save(b, "JPEG", progressive=True, **kw)
+            data = b.getvalue()
+            assert data[2:].find(b"\xff\xc2") >= 0  # SOF2
+            out[f"prog_{name}_jpeg"] = np.frombuffer(data, np.uint8)
+            out[f"prog_{name}_rgb"] = np.array(Image.open(io.BytesIO(data)).convert("RGB"))
     path = Path(__file__).parent / "jpeg_reference.npz"
     np.savez_compressed(path, **out)
-    print(f"{len(CASES)} cases -> {path}")
+    print(f"{len(CASES) + len(PROGRESSIVE)} cases -> {path}")
 
 
 if __name__ == "__main__":

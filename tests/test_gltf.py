@@ -149,11 +149,12 @@ def test_jpeg_textures_match_libjpeg(tmp_path):
     """JPEG base-colour textures (the reference decodes them with stb_image)
     against Pillow's libjpeg decode of the same files
     (tests/golden/make_jpeg_golden.py): 4:4:4 / 4:2:2 / 4:2:0 sampling,
-    restart markers, greyscale, partial MCUs.  Both use exact-enough inverse
-    DCTs and the same chroma filter, so pixels differ by at most 2 levels."""
+    restart markers, greyscale, partial MCUs, sequential and progressive
+    files.  Both use exact-enough inverse DCTs and the same chroma filter, so
+    pixels differ by at most 2 levels."""
     ref = np.load(Path(__file__).parent / "golden" / "jpeg_reference.npz")
     names = sorted({k[:-5] for k in ref.files if k.endswith("_jpeg")})
-    assert len(names) == 8
+    assert len(names) == 14
     pos, nrm, uv, idx = quad()
     for n in names:
         b = GltfBuilder()
@@ -169,15 +170,52 @@ def test_jpeg_textures_match_libjpeg(tmp_path):
         assert diff.max() <= 2 and diff.mean() <= 0.5, (n, diff.max(), diff.mean())
 
 
-def test_progressive_jpeg_is_rejected(tmp_path):
-    # SOF2 marker right after SOI: the loader names the unsupported coding
-    data = bytes([0xFF, 0xD8, 0xFF, 0xC2, 0x00, 0x0B, 8, 0, 1, 0, 1, 1, 1, 0x11, 0, 0xFF, 0xD9])
+def load_texture(tmp_path, data, name):
     pos, nrm, uv, idx = quad()
     b = GltfBuilder()
     b.material(texture_png=data)
     b.node(mesh=b.mesh([b.primitive(pos, nrm, uv, idx=idx, material=0)]))
     err = []
-    assert api.LoadScene(b.write(tmp_path / "p.gltf"), err) is None and "sequential" in err[0]
+    sc = api.LoadScene(b.write(tmp_path / f"{name}.gltf"), err)
+    return (sc.materials[0].albedo if sc is not None else None), err
+
+
+def test_progressive_jpeg_equals_its_sequential_twin(tmp_path):
+    """A progressive file (T.81 annex G: DC and AC first and refinement
+    scans, end-of-band runs) holds the same quantised coefficients as the
+    sequential file of the same image and settings, so the two decode to
+    the same bytes."""
+    ref = np.load(Path(__file__).parent / "golden" / "jpeg_reference.npz")
+    twins = sorted(k[5:-5] for k in ref.files if k.startswith("prog_") and k.endswith("_jpeg"))
+    assert len(twins) == 6
+    for n in twins:
+        seq, err = load_texture(tmp_path, ref[n + "_jpeg"].tobytes(), n)
+        assert seq is not None, (n, err)
+        prog, err = load_texture(tmp_path, ref["prog_" + n + "_jpeg"].tobytes(), "prog_" + n)
+        assert prog is not None, (n, err)
+        assert (prog.width, prog.height) == (seq.width, seq.height)
+        np.testing.assert_array_equal(prog.pixel_data, seq.pixel_data, err_msg=n)
+
+
+def test_bad_progressive_scans_are_rejected(tmp_path):
+    # SOF2 with no scan before EOI
+    data = bytes([0xFF, 0xD8, 0xFF, 0xC2, 0x00, 0x0B, 8, 0, 1, 0, 1, 1, 1, 0x11, 0, 0xFF, 0xD9])
+    tex, err = load_texture(tmp_path, data, "p")
+    assert tex is None and "no image data" in err[0], err
+    # an AC scan with its Ss set to 0: a DC scan (Ss = 0) must have Se = 0
+    good = np.load(Path(__file__).parent / "golden" / "jpeg_reference.npz")["prog_s420_q90_jpeg"].tobytes()
+    k = 2
+    while True:
+        k = good.index(b"\xff\xda", k)
+        ns = good[k + 4]
+        ss = good[k + 5 + 2 * ns]
+        if ss > 0:
+            break
+        k += 2
+    bad = bytearray(good)
+    bad[k + 5 + 2 * ns] = 0  # Ss = 0 with Se > 0
+    tex, err = load_texture(tmp_path, bytes(bad), "q")
+    assert tex is None and "progressive scan parameters" in err[0], err
 
 
 def test_defaults_and_errors(tmp_path):
