@@ -276,8 +276,18 @@ struct Parser {
 
 uint32_t be32(const uint8_t* b) { return (uint32_t)b[0] << 24 | (uint32_t)b[1] << 16 | (uint32_t)b[2] << 8 | b[3]; }
 
-// 8/16-bit, non-interlaced PNG of any colour type -> 3 (RGB) or 4 (RGBA)
-// 8-bit channels; 16-bit samples keep their high byte.
+// PNG of any colour type, bit depth and interlace -> 3 (RGB) or 4 (RGBA)
+// 8-bit channels.  The reference's textures come from tinygltf's image
+// loader over stb_image (src/loader.cpp:415-432), whose 8-bit conversions
+// are these: 1/2/4-bit grey is scaled to 0..255 (x255, x85, x17), palette
+// indices are not; a tRNS colour key on a grey or RGB image adds an alpha
+// channel that is 0 where the pixel's samples equal the key; a palette with
+// tRNS gives its alphas.  An image without alpha has 3 channels here and 4
+// (alpha 255) there: either way the bake sees alpha 1.  16-bit samples keep
+// their high byte, stb_image's 8-bit conversion; tinygltf may instead keep
+// 16-bit samples, which the reference's albedo lookup would read as bytes.
+// Adam7-interlaced images are decoded pass by pass (each pass a filtered
+// sub-image) and scattered to their pixels.
 bool decode_png(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint32_t& W, uint32_t& H, uint32_t& C,
                 std::string& err) {
   static const uint8_t sig[8] = {137, 80, 78, 71, 13, 10, 26, 10};
@@ -314,70 +324,112 @@ bool decode_png(const std::vector<uint8_t>& f, std::vector<uint8_t>& out, uint32
     err = "bad PNG header";
     return false;
   }
-  if (interlace || (depth != 8 && depth != 16) || (ctype == 3 && depth != 8)) {
-    err = "unsupported PNG (interlaced or bit depth other than 8/16)";
-    return false;
-  }
   const int ch = ctype == 0 ? 1 : ctype == 2 ? 3 : ctype == 3 ? 1 : ctype == 4 ? 2 : ctype == 6 ? 4 : 0;
   if (!ch) {
     err = "bad PNG colour type";
     return false;
   }
-  const size_t bpp = (size_t)ch * (depth / 8), stride = bpp * W;
-  std::vector<uint8_t> raw((stride + 1) * H);
+  // PNG 1.2 table 11.1: the bit depths each colour type allows
+  const bool depth_ok = ctype == 0 ? (depth == 1 || depth == 2 || depth == 4 || depth == 8 || depth == 16)
+                        : ctype == 3 ? (depth == 1 || depth == 2 || depth == 4 || depth == 8)
+                                     : (depth == 8 || depth == 16);
+  if (!depth_ok || interlace > 1) {
+    err = "unsupported PNG (bad bit depth for its colour type, or unknown interlace method)";
+    return false;
+  }
+  // colour key (grey: one 16-bit sample, RGB: three) and the output channels
+  const bool key = (ctype == 0 && trns.size() >= 2) || (ctype == 2 && trns.size() >= 6);
+  uint16_t keyv[3] = {0, 0, 0};
+  if (key)
+    for (int k = 0; k < (ctype == 0 ? 1 : 3); ++k) keyv[k] = (uint16_t)(trns[2 * k] << 8 | trns[2 * k + 1]);
+  const bool alpha = ctype == 4 || ctype == 6 || (ctype == 3 && !trns.empty()) || key;
+  C = alpha ? 4 : 3;
+  // passes: (x0, y0, dx, dy); one pass covering every pixel when not interlaced
+  static const int adam7[7][4] = {{0, 0, 8, 8}, {4, 0, 8, 8}, {0, 4, 4, 8}, {2, 0, 4, 4},
+                                  {0, 2, 2, 4}, {1, 0, 2, 2}, {0, 1, 1, 2}};
+  static const int whole[1][4] = {{0, 0, 1, 1}};
+  const int npass = interlace ? 7 : 1;
+  const int(*pass)[4] = interlace ? adam7 : whole;
+  const size_t bitspp = (size_t)ch * depth, bpp = std::max<size_t>(1, bitspp / 8);
+  auto pass_w = [&](int p) { return (W > (uint32_t)pass[p][0]) ? (W - pass[p][0] + pass[p][2] - 1) / pass[p][2] : 0u; };
+  auto pass_h = [&](int p) { return (H > (uint32_t)pass[p][1]) ? (H - pass[p][1] + pass[p][3] - 1) / pass[p][3] : 0u; };
+  size_t total = 0;
+  for (int p = 0; p < npass; ++p)
+    if (pass_w(p) && pass_h(p)) total += ((pass_w(p) * bitspp + 7) / 8 + 1) * pass_h(p);
+  // a zlib stream inflates by at most about 1032:1: refuse a size the IDAT
+  // data cannot hold before allocating it
+  if (total > 1100 * (uint64_t)idat.size() + 1024) {
+    err = "PNG inflate failed";
+    return false;
+  }
+  std::vector<uint8_t> raw(total);
   uLongf rl = (uLongf)raw.size();
   if (uncompress(raw.data(), &rl, idat.data(), (uLong)idat.size()) != Z_OK || rl != raw.size()) {
     err = "PNG inflate failed";
     return false;
   }
-  std::vector<uint8_t> img(stride * H);
-  for (uint32_t y = 0; y < H; ++y) {
-    const uint8_t ft = raw[y * (stride + 1)];
-    const uint8_t* s = &raw[y * (stride + 1) + 1];
-    uint8_t* o = &img[y * stride];
-    const uint8_t* up = y ? &img[(y - 1) * stride] : nullptr;
-    for (size_t x = 0; x < stride; ++x) {
-      int a = x >= bpp ? o[x - bpp] : 0, b = up ? up[x] : 0, c = (up && x >= bpp) ? up[x - bpp] : 0;
-      int v = s[x];
-      switch (ft) {
-        case 0: break;
-        case 1: v += a; break;
-        case 2: v += b; break;
-        case 3: v += (a + b) / 2; break;
-        case 4: {
-          int pp = a + b - c, pa = std::abs(pp - a), pb = std::abs(pp - b), pc = std::abs(pp - c);
-          v += (pa <= pb && pa <= pc) ? a : (pb <= pc ? b : c);
-          break;
-        }
-        default:
-          err = "bad PNG filter";
-          return false;
-      }
-      o[x] = (uint8_t)v;
-    }
-  }
-  const bool alpha = ctype == 4 || ctype == 6 || (ctype == 3 && !trns.empty());
-  C = alpha ? 4 : 3;
   out.assign((size_t)W * H * C, 255);
-  const int step = depth / 8;
-  for (size_t p = 0; p < (size_t)W * H; ++p) {
-    const uint8_t* s = &img[p * bpp];
-    uint8_t* o = &out[p * C];
-    auto smp = [&](int k) { return s[k * step]; };
-    if (ctype == 0 || ctype == 4) {
-      o[0] = o[1] = o[2] = smp(0);
-      if (ctype == 4) o[3] = smp(1);
-    } else if (ctype == 2 || ctype == 6) {
-      for (int k = 0; k < 3; ++k) o[k] = smp(k);
-      if (ctype == 6) o[3] = smp(3);
-    } else {
-      const uint32_t e = s[0];
-      if (3 * e + 2 >= plte.size()) {
-        err = "PNG palette index out of range";
-        return false;
+  const int scale = ctype == 0 && depth < 8 ? 255 / ((1 << depth) - 1) : 1;
+  auto b8 = [&](uint32_t v) { return (uint8_t)(depth == 16 ? v >> 8 : v * scale); };
+  size_t off = 0;
+  std::vector<uint8_t> cur, prev;
+  for (int p = 0; p < npass; ++p) {
+    const uint32_t pw = pass_w(p), ph = pass_h(p);
+    if (!pw || !ph) continue;
+    const size_t stride = (pw * bitspp + 7) / 8;
+    cur.assign(stride, 0);
+    prev.assign(stride, 0);  // the line above the first one is zero
+    for (uint32_t y = 0; y < ph; ++y) {
+      const uint8_t ft = raw[off];
+      const uint8_t* s = &raw[off + 1];
+      off += stride + 1;
+      for (size_t x = 0; x < stride; ++x) {
+        const int a = x >= bpp ? cur[x - bpp] : 0, b = prev[x], c = x >= bpp ? prev[x - bpp] : 0;
+        int v = s[x];
+        switch (ft) {
+          case 0: break;
+          case 1: v += a; break;
+          case 2: v += b; break;
+          case 3: v += (a + b) / 2; break;
+          case 4: {
+            const int pp = a + b - c, pa = std::abs(pp - a), pb = std::abs(pp - b), pc = std::abs(pp - c);
+            v += (pa <= pb && pa <= pc) ? a : (pb <= pc ? b : c);
+            break;
+          }
+          default:
+            err = "bad PNG filter";
+            return false;
+        }
+        cur[x] = (uint8_t)v;
       }
-      for (int k = 0; k < 3; ++k) o[k] = plte[3 * e + k];
-      if (alpha) o[3] = e < trns.size() ? trns[e] : 255;
+      for (uint32_t x = 0; x < pw; ++x) {
+        uint32_t v[4] = {0, 0, 0, 0};
+        for (int k = 0; k < ch; ++k) {
+          const size_t bit = ((size_t)x * ch + k) * depth;
+          if (depth == 16) v[k] = (uint32_t)cur[bit / 8] << 8 | cur[bit / 8 + 1];
+          else if (depth == 8) v[k] = cur[bit / 8];
+          else v[k] = (cur[bit / 8] >> (8 - depth - (bit & 7))) & ((1u << depth) - 1);
+        }
+        const size_t X = pass[p][0] + (size_t)x * pass[p][2], Y = pass[p][1] + (size_t)y * pass[p][3];
+        uint8_t* o = &out[(Y * W + X) * C];
+        if (ctype == 3) {
+          if (3 * (size_t)v[0] + 2 >= plte.size()) {
+            err = "PNG palette index out of range";
+            return false;
+          }
+          for (int k = 0; k < 3; ++k) o[k] = plte[3 * v[0] + k];
+          if (alpha) o[3] = v[0] < trns.size() ? trns[v[0]] : 255;
+        } else if (ctype == 0 || ctype == 4) {
+          o[0] = o[1] = o[2] = b8(v[0]);
+          if (ctype == 4) o[3] = b8(v[1]);
+          else if (key) o[3] = v[0] == keyv[0] ? 0 : 255;
+        } else {
+          for (int k = 0; k < 3; ++k) o[k] = b8(v[k]);
+          if (ctype == 6) o[3] = b8(v[3]);
+          else if (key) o[3] = v[0] == keyv[0] && v[1] == keyv[1] && v[2] == keyv[2] ? 0 : 255;
+        }
+      }
+      cur.swap(prev);
     }
   }
   return true;

@@ -1,8 +1,9 @@
 // jpeg.cpp - JPEG base-colour textures for the glTF loader.  The reference
-// loads every image through stb_image (src/loader.cpp:687-704, tinygltf's
-// image callback); this is an own decoder of Huffman-coded JPEG (ITU-T
-// T.81 baseline, extended 8-bit and progressive, SOF0 / SOF1 / SOF2) with restart
-// intervals, 1 or 3 components and any sampling factors up to 4x4:
+// reads every texture through tinygltf's image loader over stb_image
+// (src/loader.cpp:415-432); this is an own decoder of Huffman-coded JPEG
+// (ITU-T T.81 baseline, extended 8-bit and progressive: SOF0 / SOF1 / SOF2)
+// with restart intervals, 1 or 3 components and any sampling factors up to
+// 4x4:
 //   - Huffman tables as canonical codes (T.81 annex C), DC prediction per
 //     component, AC run/size symbols with EOB and ZRL (annex F.2.2);
 //   - dequantisation, a separable floating-point inverse DCT (the

@@ -174,3 +174,65 @@ def quad(size=1.0):
     uv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float32)
     idx = np.array([0, 1, 2, 0, 2, 3], np.uint32)
     return pos, nrm, uv, idx
+
+
+ADAM7 = [(0, 0, 8, 8), (4, 0, 8, 8), (0, 4, 4, 8), (2, 0, 4, 4), (0, 2, 2, 4), (1, 0, 2, 2), (0, 1, 1, 2)]
+
+
+def png_encode(samples: np.ndarray, color_type: int, depth: int, interlace: bool = False, palette=None,
+               trns: bytes = None) -> bytes:
+    """PNG of raw samples (H, W, channels) in [0, 2^depth) at any bit depth
+    PNG allows (sub-byte rows packed most significant bit first), optionally
+    Adam7-interlaced; each pass is filtered with types 0..4 in turn."""
+    samples = np.asarray(samples, np.uint32)
+    H, W, ch = samples.shape
+    bpp = max(1, ch * depth // 8)
+
+    def pack(row):  # one row of (w, ch) samples -> bytes
+        flat = row.reshape(-1)
+        if depth == 16:
+            return b"".join(int(v).to_bytes(2, "big") for v in flat)
+        if depth == 8:
+            return bytes(int(v) for v in flat)
+        bits = "".join(format(int(v), f"0{depth}b") for v in flat)
+        bits += "0" * (-len(bits) % 8)
+        return bytes(int(bits[i:i + 8], 2) for i in range(0, len(bits), 8))
+
+    raw = bytearray()
+    for x0, y0, dx, dy in (ADAM7 if interlace else [(0, 0, 1, 1)]):
+        sub = samples[y0::dy, x0::dx]
+        if sub.size == 0:
+            continue
+        prev = None
+        for y, row in enumerate(sub):
+            cur = np.frombuffer(pack(row), np.uint8).astype(np.int32)
+            up = prev if prev is not None else np.zeros_like(cur)
+            left = np.concatenate([np.zeros(bpp, np.int32), cur[:-bpp]])
+            upleft = np.concatenate([np.zeros(bpp, np.int32), up[:-bpp]])
+            ft = y % 5
+            if ft == 0:
+                f = cur
+            elif ft == 1:
+                f = cur - left
+            elif ft == 2:
+                f = cur - up
+            elif ft == 3:
+                f = cur - (left + up) // 2
+            else:
+                p = left + up - upleft
+                pa, pb, pc = np.abs(p - left), np.abs(p - up), np.abs(p - upleft)
+                f = cur - np.where((pa <= pb) & (pa <= pc), left, np.where(pb <= pc, up, upleft))
+            raw.append(ft)
+            raw += (f & 0xFF).astype(np.uint8).tobytes()
+            prev = cur
+
+    def chunk(t, d):
+        return struct.pack(">I", len(d)) + t + d + struct.pack(">I", zlib.crc32(t + d) & 0xFFFFFFFF)
+
+    out = b"\x89PNG\r\n\x1a\n" + chunk(b"IHDR", struct.pack(">IIBBBBB", W, H, depth, color_type, 0, 0,
+                                                            1 if interlace else 0))
+    if palette is not None:
+        out += chunk(b"PLTE", np.asarray(palette, np.uint8).tobytes())
+    if trns is not None:
+        out += chunk(b"tRNS", bytes(trns))
+    return out + chunk(b"IDAT", zlib.compress(bytes(raw), 9)) + chunk(b"IEND", b"")
