@@ -197,7 +197,9 @@ int main(int argc, char** argv) {
 
   shb_options o{};
   const char* dev = std::getenv("SHB_DEVICE");
-  o.device = dev ? std::atoi(dev) : 0;
+  // an ordinal outside int32 becomes -1, which context creation refuses
+  const long dv = dev ? std::strtol(dev, nullptr, 10) : 0;
+  o.device = dv < INT32_MIN || dv > INT32_MAX ? -1 : (int)dv;
   shb_context* ctx = nullptr;
   if (shb_context_create(&o, &ctx) != SHB_OK) return fail("no CUDA context");
   shb_scene* scene = nullptr;

@@ -7,6 +7,7 @@
 #include <sys/stat.h>
 
 #include <algorithm>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <string>
@@ -123,7 +124,9 @@ int main(int argc, char** argv) {
   std::sort(files.begin(), files.end());
   shb_options o{};
   const char* dev = std::getenv("SHB_DEVICE");
-  o.device = dev ? std::atoi(dev) : 0;
+  // an ordinal outside int32 becomes -1, which context creation refuses
+  const long dv = dev ? std::strtol(dev, nullptr, 10) : 0;
+  o.device = dv < INT32_MIN || dv > INT32_MAX ? -1 : (int)dv;
   shb_context* ctx = nullptr;
   if (shb_context_create(&o, &ctx) != SHB_OK) {
     std::fprintf(stderr, "E no CUDA context: %s\n", shb_last_error());
