@@ -450,7 +450,14 @@ def LoadScene(path, error: Optional[list] = None) -> Optional[Scene]:
             error.append(lib.shb_last_error().decode())
         return None
     try:
-        return unpack_scene(lib.shb_host_scene_desc(h).contents)
+        scene = unpack_scene(lib.shb_host_scene_desc(h).contents)
+        # names and albedo image paths (src/loader.cpp:428-432,470)
+        for i, m in enumerate(scene.materials):
+            name, path = C.c_char_p(), C.c_char_p()
+            A.check(lib.shb_host_scene_material_info(h, i, C.byref(name), C.byref(path)))
+            m.name = (name.value or b"").decode()
+            m.albedo.file_path = path.value.decode() if path.value else None
+        return scene
     finally:
         lib.shb_host_scene_destroy(h)
 
@@ -516,10 +523,16 @@ def CreateAtlasGeometries(scene: Scene, target_resolution: int, padding: int, de
 
 def SaveScene(scene: Scene, path, material_names=None, albedo_files=None) -> bool:
     """src/saver.h:50-53 SaveScene: glTF + <stem>.bin (host only).  False
-    on failure, like the reference."""
+    on failure, like the reference.  Material names and albedo image files
+    default to the materials' own (Material.name, albedo.file_path), as the
+    reference reads them."""
     lib = A.load()
     desc, keep = pack_scene(scene)
     n = len(scene.materials)
+    if material_names is None:
+        material_names = [m.name for m in scene.materials]
+    if albedo_files is None:
+        albedo_files = [getattr(m.albedo, "file_path", None) for m in scene.materials]
 
     def strs(v):
         if v is None:

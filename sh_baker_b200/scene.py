@@ -28,6 +28,7 @@ class Texture:
     height: int = 0
     channels: int = 0
     pixel_data: np.ndarray = field(default_factory=lambda: np.zeros(0, np.uint8))
+    file_path: Optional[str] = None  # the image file it was read from, absolute (src/scene.h:19-22)
 
 
 @dataclass
