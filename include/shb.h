@@ -299,9 +299,9 @@ SHB_API shb_status shb_bake(shb_scene* scene, const shb_gbuffer* g,
  * texels are cut into (bake, texel tile) work items that the host packs into
  * waves, small bakes sharing a wave, and each wave runs its per-depth
  * traversal and shading launches once for all of its paths; with use_graph
- * the whole launch sequence is captured in one CUDA graph.  Results are bit-identical to one shb_bake
- * call per item.  All scenes must belong to `ctx`; outputs are device
- * pointers of W*s x H*s texels. */
+ * the whole launch sequence is captured in one CUDA graph.  Results are
+ * bit-identical to one shb_bake call per item.  All scenes must belong to
+ * `ctx`; outputs are device pointers of W*s x H*s texels. */
 typedef struct shb_batch_item {
   shb_scene* scene;
   const shb_gbuffer* gbuffer;
