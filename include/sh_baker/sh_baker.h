@@ -345,6 +345,118 @@ inline std::optional<AtlasResult> CreateAtlasGeometries(const Scene& scene, unsi
   return r;
 }
 
+// ---- src/loader.h:13, src/saver.h:50-53 ------------------------------------
+
+namespace detail {
+
+inline Affine3f affine_from_rows(const float r[12]) {
+#ifdef SH_BAKER_HAS_EIGEN
+  Affine3f a = Affine3f::Identity();
+  for (int i = 0; i < 3; ++i)
+    for (int c = 0; c < 4; ++c) a.matrix()(i, c) = r[i * 4 + c];
+  return a;
+#else
+  Affine3f a;
+  std::memcpy(a.m, r, sizeof(a.m));
+  return a;
+#endif
+}
+
+// A geometry description as a Geometry; absent attributes stay empty.
+inline Geometry geometry_from(const shb_geometry_desc& d) {
+  Geometry G;
+  G.material_id = d.material_id;
+  G.transform = affine_from_rows(d.transform);
+  for (uint32_t v = 0; v < d.vertex_count; ++v) {
+    if (d.vertices) G.vertices.push_back(Vector3f(d.vertices[3 * v], d.vertices[3 * v + 1], d.vertices[3 * v + 2]));
+    if (d.normals) G.normals.push_back(Vector3f(d.normals[3 * v], d.normals[3 * v + 1], d.normals[3 * v + 2]));
+    if (d.texture_uvs) G.texture_uvs.push_back(Vector2f(d.texture_uvs[2 * v], d.texture_uvs[2 * v + 1]));
+    if (d.lightmap_uvs) G.lightmap_uvs.push_back(Vector2f(d.lightmap_uvs[2 * v], d.lightmap_uvs[2 * v + 1]));
+    if (d.tangents)
+      G.tangents.push_back(
+          Vector4f(d.tangents[4 * v], d.tangents[4 * v + 1], d.tangents[4 * v + 2], d.tangents[4 * v + 3]));
+  }
+  if (d.indices) G.indices.assign(d.indices, d.indices + d.index_count);
+  return G;
+}
+
+}  // namespace detail
+
+// A .gltf / .glb file through shb_load_gltf (host code, no GPU); nullopt
+// on failure, like the reference, with the reason in shb_last_error().
+// Each area light points at its material and geometry in the returned
+// scene, as the reference fixes them up after loading
+// (src/loader.cpp:835-839); moving the Scene keeps them valid, copying it
+// does not.
+inline std::optional<Scene> LoadScene(const std::filesystem::path& path) {
+  shb_host_scene* hs = nullptr;
+  if (shb_load_gltf(path.string().c_str(), &hs) != SHB_OK) return std::nullopt;
+  struct Owned {
+    shb_host_scene* h;
+    ~Owned() { shb_host_scene_destroy(h); }
+  } owned{hs};
+  const shb_scene_desc* d = shb_host_scene_desc(hs);
+  Scene scene;
+  for (uint32_t g = 0; g < d->geometry_count; ++g) scene.geometries.push_back(detail::geometry_from(d->geometries[g]));
+  for (uint32_t m = 0; m < d->material_count; ++m) {
+    const shb_material_desc& md = d->materials[m];
+    Material M;
+    const char* name = nullptr;
+    const char* file = nullptr;
+    check(shb_host_scene_material_info(hs, (int32_t)m, &name, &file));
+    M.name = name ? name : "";
+    if (file) M.albedo.file_path = std::filesystem::path(file);
+    M.albedo.width = md.albedo_width;
+    M.albedo.height = md.albedo_height;
+    M.albedo.channels = md.albedo_channels;
+    if (md.albedo_pixels)
+      M.albedo.pixel_data.assign(md.albedo_pixels,
+                                 md.albedo_pixels + (size_t)md.albedo_width * md.albedo_height * md.albedo_channels);
+    M.emission_intensity = md.emission_intensity;
+    scene.materials.push_back(std::move(M));
+  }
+  for (uint32_t l = 0; l < d->light_count; ++l) {
+    const shb_light_desc& ld = d->lights[l];
+    Light L;
+    L.type = static_cast<Light::Type>(ld.type);
+    L.position = Vector3f(ld.position[0], ld.position[1], ld.position[2]);
+    L.direction = Vector3f(ld.direction[0], ld.direction[1], ld.direction[2]);
+    L.color = Vector3f(ld.color[0], ld.color[1], ld.color[2]);
+    L.intensity = ld.intensity;
+    L.cos_inner_cone = ld.cos_inner_cone;
+    L.cos_outer_cone = ld.cos_outer_cone;
+    L.area = ld.area;
+    L.geometry_index = ld.geometry_index;
+    scene.lights.push_back(L);
+  }
+  for (size_t l = 0; l < scene.lights.size(); ++l) {
+    const shb_light_desc& ld = d->lights[l];
+    if (ld.material_index >= 0 && (size_t)ld.material_index < scene.materials.size())
+      scene.lights[l].material = &scene.materials[(size_t)ld.material_index];
+    if (ld.geometry_index >= 0 && (size_t)ld.geometry_index < scene.geometries.size())
+      scene.lights[l].geometry = &scene.geometries[(size_t)ld.geometry_index];
+  }
+  return std::optional<Scene>(std::move(scene));
+}
+
+// glTF + <stem>.bin through shb_save_gltf, with each material's name and
+// albedo image file (copied beside the output); false on failure, like
+// the reference.
+inline bool SaveScene(const Scene& scene, const std::filesystem::path& path) {
+  detail::Desc D;
+  detail::describe(scene, &D);
+  const size_t n = scene.materials.size();
+  std::vector<std::string> files(n);
+  std::vector<const char*> names(n), paths(n);
+  for (size_t i = 0; i < n; ++i) {
+    names[i] = scene.materials[i].name.c_str();
+    if (scene.materials[i].albedo.file_path) files[i] = scene.materials[i].albedo.file_path->string();
+    paths[i] = files[i].empty() ? nullptr : files[i].c_str();
+  }
+  return shb_save_gltf(&D.d, n ? names.data() : nullptr, n ? paths.data() : nullptr, path.string().c_str()) ==
+         SHB_OK;
+}
+
 // ---- src/rasterizer.h:27-39 ------------------------------------------------
 
 inline std::vector<SurfacePoint> RasterizeScene(const Scene& scene, const RasterConfig& config) {
