@@ -621,7 +621,7 @@ def roofline_of(stats, steps, scene, w, ms, clk):
     bytes), so the bound reported is issue: warp instructions per ray (ncu,
     small case of the same scene) x rays traced / kernel time, against the
     SMs' issue slots (SMs x 4 schedulers x median SM clock under load).  The
-    model-byte HBM figure (SURVEY-style algorithmic bytes per ray over the
+    model-byte HBM figure (the algorithmic bytes of bytes_per_ray over the
     measured copy bandwidth) is kept beside it as `hbm_model`."""
     import torch
     ext_ms = sum(s.extend_kernel_ms for s in stats)
