@@ -12,6 +12,8 @@
 //   Dilate<T> for SHCoeffs, float, uint8_t                  (src/dilation.h:14-16)
 //   SaveMode, SaveSHLightMap                                (src/saver.h:21-48)
 //   CreateAtlasGeometries, atlas_internal::CalculateGeometryScales (src/atlas.h:10-53)
+//   LoadScene, SaveScene                                    (src/loader.h:13, src/saver.h:50-53)
+//   TransformedVertices / Normals / Tangents, SurfaceArea   (src/scene.h:117-123)
 // Where the reference CHECK-fails these throw sh_baker::Error.  With Eigen
 // available the vector types are Eigen's; otherwise small POD stand-ins with
 // the same memory layout and accessors are used.
@@ -19,6 +21,7 @@
 #define SH_BAKER_B200_SH_BAKER_H_
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
@@ -199,7 +202,8 @@ inline shb_context* context() {
   if (!h.ctx) {
     shb_options o{};
     const char* d = std::getenv("SHB_DEVICE");
-    o.device = d ? std::atoi(d) : 0;
+    const long dv = d ? std::strtol(d, nullptr, 10) : 0;  // outside int32: -1, refused
+    o.device = dv < INT32_MIN || dv > INT32_MAX ? -1 : (int)dv;
     check(shb_context_create(&o, &h.ctx));
   }
   return h.ctx;
@@ -455,6 +459,79 @@ inline bool SaveScene(const Scene& scene, const std::filesystem::path& path) {
   }
   return shb_save_gltf(&D.d, n ? names.data() : nullptr, n ? paths.data() : nullptr, path.string().c_str()) ==
          SHB_OK;
+}
+
+// ---- src/scene.h:117-123 ---------------------------------------------------
+// World-space attributes (src/scene.cpp:162-207), with the float products
+// in the order the library's upload uses: v' = L v + t, n' = normalize(R n),
+// t' = (normalize(R t.xyz), t.w), R the rotation part of L
+// (shb_rotation_part).
+
+namespace detail {
+
+inline Vector3f mat_vec(const float* m, int stride, float x, float y, float z) {
+  return Vector3f(m[0] * x + (m[1] * y + m[2] * z), m[stride] * x + (m[stride + 1] * y + m[stride + 2] * z),
+                  m[2 * stride] * x + (m[2 * stride + 1] * y + m[2 * stride + 2] * z));
+}
+
+inline Vector3f normalized(const Vector3f& v) {
+  const float n = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  return Vector3f(v[0] / n, v[1] / n, v[2] / n);
+}
+
+inline void rotation_of(const Affine3f& a, float R[9]) {
+  float rows[12];
+  affine_rows(a, rows);
+  check(shb_rotation_part(rows, R));
+}
+
+}  // namespace detail
+
+inline std::vector<Vector3f> TransformedVertices(const Geometry& geometry) {
+  float rows[12];
+  affine_rows(geometry.transform, rows);
+  std::vector<Vector3f> out;
+  out.reserve(geometry.vertices.size());
+  for (const Vector3f& v : geometry.vertices) {
+    const Vector3f m = detail::mat_vec(rows, 4, v[0], v[1], v[2]);
+    out.push_back(Vector3f(m[0] + rows[3], m[1] + rows[7], m[2] + rows[11]));
+  }
+  return out;
+}
+
+inline std::vector<Vector3f> TransformedNormals(const Geometry& geometry) {
+  float R[9];
+  detail::rotation_of(geometry.transform, R);
+  std::vector<Vector3f> out;
+  out.reserve(geometry.normals.size());
+  for (const Vector3f& n : geometry.normals) out.push_back(detail::normalized(detail::mat_vec(R, 3, n[0], n[1], n[2])));
+  return out;
+}
+
+inline std::vector<Vector4f> TransformedTangents(const Geometry& geometry) {
+  float R[9];
+  detail::rotation_of(geometry.transform, R);
+  std::vector<Vector4f> out;
+  out.reserve(geometry.tangents.size());
+  for (const Vector4f& t : geometry.tangents) {
+    const Vector3f r = detail::normalized(detail::mat_vec(R, 3, t[0], t[1], t[2]));
+    out.push_back(Vector4f(r[0], r[1], r[2], t[3]));
+  }
+  return out;
+}
+
+// Object-space area: the sum of 0.5 |(v1 - v0) x (v2 - v0)| over triangles.
+inline float SurfaceArea(const Geometry& geometry) {
+  float total = 0.0f;
+  for (size_t i = 0; i + 2 < geometry.indices.size(); i += 3) {
+    const Vector3f& a = geometry.vertices[geometry.indices[i]];
+    const Vector3f& b = geometry.vertices[geometry.indices[i + 1]];
+    const Vector3f& c = geometry.vertices[geometry.indices[i + 2]];
+    const float e1[3] = {b[0] - a[0], b[1] - a[1], b[2] - a[2]}, e2[3] = {c[0] - a[0], c[1] - a[1], c[2] - a[2]};
+    const float x = e1[1] * e2[2] - e1[2] * e2[1], y = e1[2] * e2[0] - e1[0] * e2[2], z = e1[0] * e2[1] - e1[1] * e2[0];
+    total += 0.5f * std::sqrt(x * x + y * y + z * z);
+  }
+  return total;
 }
 
 // ---- src/rasterizer.h:27-39 ------------------------------------------------

@@ -256,6 +256,15 @@ SHB_API shb_status shb_scene_rebuild_bvh(shb_scene* scene);
 SHB_API shb_status shb_scene_bvh_info(const shb_scene* scene, uint32_t* wide_nodes,
                                       uint32_t* triangles, uint32_t* depth);
 
+/* The rotation that TransformedNormals / TransformedTangents
+ * (src/scene.cpp:171-195) apply: the rotation part of a geometry's
+ * transform (row-major 3x4 [L | t], as in shb_geometry_desc), that is
+ * Eigen's Transform::rotation(), the orthogonal factor of L's polar
+ * decomposition with a positive determinant; row-major 3x3 out.  The same
+ * rotation the library applies to normals and tangents on upload.  Host
+ * code only. */
+SHB_API shb_status shb_rotation_part(const float transform[12], float rotation[9]);
+
 /* ---- RasterizeScene (src/rasterizer.cpp:68-211) ----------------------- */
 
 /* Rasterises every triangle's lightmap UVs into a (W*s) x (H*s) texel

@@ -163,6 +163,7 @@ SIGNATURES = {
     "shb_load_gltf": (C.c_int, [C.c_char_p, C.POINTER(vp)]),
     "shb_host_scene_desc": (C.POINTER(SceneDesc), [vp]),
     "shb_host_scene_destroy": (C.c_int, [vp]),
+    "shb_rotation_part": (C.c_int, [vp, vp]),
     "shb_host_scene_material_info": (C.c_int, [vp, C.c_int32, C.POINTER(C.c_char_p), C.POINTER(C.c_char_p)]),
     "shb_save_gltf": (C.c_int, [C.POINTER(SceneDesc), vp, vp, C.c_char_p]),
     "shb_atlas_geometry_scales": (C.c_int, [C.POINTER(SceneDesc), C.c_float, vp]),

@@ -444,6 +444,16 @@ shb_status shb_context_synchronize(shb_context* ctx) {
 
 uint64_t shb_context_kernel_launches(const shb_context* ctx) { return ctx ? ctx->launches : 0; }
 
+shb_status shb_rotation_part(const float transform[12], float rotation[9]) {
+  return ::shb::guarded("shb_rotation_part", [&]() -> shb_status {
+    if (!transform || !rotation) return bad("NULL argument");
+    const float L[9] = {transform[0], transform[1], transform[2], transform[4], transform[5],
+                        transform[6], transform[8], transform[9], transform[10]};
+    polar_rotation(L, rotation);
+    return SHB_OK;
+  });
+}
+
 shb_status shb_scene_upload(shb_context* ctx, const shb_scene_desc* d, shb_scene** out) {
   return ::shb::guarded("shb_scene_upload", [&]() -> shb_status {
     if (!d || !out) return bad("NULL argument");

@@ -4,6 +4,8 @@
 //   scene_io_test roundtrip <dir>   save a scene, load it back, compare
 //   scene_io_test emissive <file>   load a scene with one emissive primitive
 //   scene_io_test missing <file>    a missing file gives nullopt
+//   scene_io_test transforms -      TransformedVertices / Normals / Tangents
+//                                   and SurfaceArea (src/scene_test.cpp:42-94)
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -86,12 +88,52 @@ static int emissive(const std::string& file) {
   return 0;
 }
 
+static bool approx3(const Vector3f& a, float x, float y, float z) {
+  return std::fabs(a[0] - x) <= 1e-5f && std::fabs(a[1] - y) <= 1e-5f && std::fabs(a[2] - z) <= 1e-5f;
+}
+
+static int transforms() {
+  const float pi = 3.14159265358979323846f;
+  const float c = std::cos(pi / 2.0f), s = std::sin(pi / 2.0f);
+  // src/scene_test.cpp:42-57 (TransformedVertices): translation by (1, 2, 3)
+  Geometry g;
+  g.vertices = {Vector3f(1.f, 0.f, 0.f), Vector3f(0.f, 1.f, 0.f)};
+  const float trans[12] = {1, 0, 0, 1, 0, 1, 0, 2, 0, 0, 1, 3};
+  g.transform = detail::affine_from_rows(trans);
+  std::vector<Vector3f> v = TransformedVertices(g);
+  EXPECT(v.size() == 2 && approx3(v[0], 2.f, 2.f, 3.f) && approx3(v[1], 1.f, 3.f, 3.f));
+  // src/scene_test.cpp:59-75 (TransformedNormals): 90 degrees about Z
+  const float rot[12] = {c, -s, 0, 0, s, c, 0, 0, 0, 0, 1, 0};
+  g.transform = detail::affine_from_rows(rot);
+  g.normals = {Vector3f(1.f, 0.f, 0.f), Vector3f(0.f, 1.f, 0.f)};
+  std::vector<Vector3f> n = TransformedNormals(g);
+  EXPECT(n.size() == 2 && approx3(n[0], 0.f, 1.f, 0.f) && approx3(n[1], -1.f, 0.f, 0.f));
+  // src/scene_test.cpp:77-94 (TransformedTangents): rotated, sign kept
+  g.tangents = {Vector4f(1.f, 0.f, 0.f, 1.f)};
+  std::vector<Vector4f> t = TransformedTangents(g);
+  EXPECT(t.size() == 1 && approx3(Vector3f(t[0][0], t[0][1], t[0][2]), 0.f, 1.f, 0.f) && t[0][3] == 1.0f);
+  // the rotation part strips a non-uniform scale: L = Rz(90) diag(2, 3, 4)
+  const float rs[12] = {2 * c, -3 * s, 0, 5, 2 * s, 3 * c, 0, 6, 0, 0, 4, 7};
+  g.transform = detail::affine_from_rows(rs);
+  g.vertices = {Vector3f(1.f, 1.f, 1.f)};
+  v = TransformedVertices(g);
+  EXPECT(approx3(v[0], 2 * c - 3 * s + 5, 2 * s + 3 * c + 6, 11.f));
+  n = TransformedNormals(g);
+  EXPECT(approx3(n[0], 0.f, 1.f, 0.f) && approx3(n[1], -1.f, 0.f, 0.f));
+  // SurfaceArea (src/scene.cpp:197-207): object space, transform ignored
+  g.vertices = {Vector3f(0.f, 0.f, 0.f), Vector3f(1.f, 0.f, 0.f), Vector3f(0.f, 1.f, 0.f), Vector3f(0.f, 0.f, 4.f)};
+  g.indices = {0, 1, 2, 0, 1, 3};
+  EXPECT(std::fabs(SurfaceArea(g) - 2.5f) <= 1e-6f);
+  return 0;
+}
+
 int main(int argc, char** argv) {
   if (argc < 3) return 2;
   const std::string mode = argv[1], arg = argv[2];
   if (mode == "roundtrip") roundtrip(arg);
   else if (mode == "emissive") emissive(arg);
   else if (mode == "missing") EXPECT(!LoadScene(arg).has_value());
+  else if (mode == "transforms") transforms();
   else return 2;
   std::printf(failures ? "scene io test failed\n" : "scene io test passed\n");
   return failures ? 1 : 0;

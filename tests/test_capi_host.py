@@ -216,4 +216,4 @@ def test_entry_point_guard_maps_exceptions(tmp_path):
                     j += 1
                 assert f'guarded("{m.group(3)}"' in lines[j + 1], (f.name, m.group(3))
                 defs += 1
-    assert defs == 34, defs
+    assert defs == 35, defs

@@ -36,10 +36,13 @@ def test_mirror_runs_reference_unit_tests(tmp_path):
 
 
 def test_mirror_load_and_save_scene(tmp_path):
-    """sh_baker::LoadScene / SaveScene (tests/cpp/scene_io_test.cpp, host
-    code): a save and load round trip keeps names, lightmap UVs, tangents
-    and lights; an emissive primitive's area light points at its material
-    and geometry in the returned scene; a missing file is nullopt."""
+    """sh_baker::LoadScene / SaveScene and the scene.h helpers
+    (tests/cpp/scene_io_test.cpp, host code): a save and load round trip
+    keeps names, lightmap UVs, tangents and lights; an emissive primitive's
+    area light points at its material and geometry in the returned scene; a
+    missing file is nullopt; the reference's TransformedVertices / Normals /
+    Tangents tests hold, the rotation part strips a non-uniform scale, and
+    SurfaceArea sums object-space triangle areas."""
     import numpy as np
 
     from tests.gltf_fixture import GltfBuilder, quad
@@ -62,3 +65,4 @@ def test_mirror_load_and_save_scene(tmp_path):
     b.node(mesh=b.mesh([b.primitive(pos + np.float32(1), nrm, uv, idx=idx, material=glow)]))
     run("emissive", b.write(tmp_path / "glow.gltf"))
     run("missing", tmp_path / "no_such.gltf")
+    run("transforms", "-")
