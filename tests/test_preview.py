@@ -44,6 +44,11 @@ def test_write_png_round_trip(tmp_path):
         p = tmp_path / f"t{ch}.png"
         A.check(lib.shb_write_png(str(p).encode(), 5, 7, ch, px.ctypes.data))
         np.testing.assert_array_equal(read_png(p), px)
+        # and an independent decoder (Pillow's) reads the same pixels
+        from PIL import Image
+        im = Image.open(p)
+        assert im.mode == {1: "L", 2: "LA", 3: "RGB", 4: "RGBA"}[ch]
+        np.testing.assert_array_equal(np.asarray(im).reshape(7, 5, ch), px)
     assert lib.shb_write_png(str(tmp_path / "bad.png").encode(), 0, 7, 3, px.ctypes.data) == 1
 
 
